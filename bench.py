@@ -1,0 +1,603 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the rope kd-tree ray-query path on B200.
+
+Default workload (one "step" = one frame): the 1024x1024-cell fBm heightfield
+(2,097,152 triangles, SAH kd-tree with ropes built once on the host and
+resident in HBM), 1920x1080 primary rays + one shadow ray and four
+cosine-weighted AO rays (length 1) per primary hit.  Metric: Mrays/s over all
+rays traced in the frame.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config heightfield_ao|soup|soup1m|terrain_sdf]
+
+Under torchrun (N > 1) every rank holds a replica of the scene and renders
+its own frame (rays are independent, nothing is exchanged): weak scaling,
+value = rays of all ranks / the slowest rank's time.  Rank 0 prints one JSON
+line.  `--impl reference` times the reference's own CPU path (its compiled
+kd-tree builder, which ships as a single leaf, plus its traversal restated on
+the host: brute-force Moller-Trumbore) on all host cores over a bounded pixel
+sample of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+SCENE_CACHE = os.path.join(ROOT, "_build")
+
+
+# ------------------------------------------------------------- plumbing
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world: int, backend: str = "nccl"):
+    import datetime
+
+    import torch.distributed as dist
+
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Slowest rank's time (the only cross-rank exchange of the benchmark)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic(key: str):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get(key)
+
+
+# ------------------------------------------------------------ workloads
+class HeightfieldAO:
+    """Primary + shadow + 4 AO rays over the 2.1M-triangle heightfield."""
+
+    name = "heightfield_ao"
+
+    def __init__(self, torch):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.cfg = cfg = rb.configs.HeightfieldConfig()
+        self.verts, self.faces = cfg.mesh_on_device()
+        t0 = time.time()
+        self.scene = rb.KDScene.from_mesh(self.verts, self.faces)
+        self.build_s = time.time() - t0
+        self.cam = cfg.camera()
+        self.params = rb.ao_params(cfg.light_dir, cfg.ao_length, cfg.bias, cfg.ao_seed)
+        W, H = cfg.width, cfg.height
+        self.primary = torch.empty((H * W, 4), dtype=torch.int32, device="cuda")
+        self.mask = torch.empty(H * W, dtype=torch.int32, device="cuda")
+        self.nsec = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.counts = self.scene.render_ao_counts(self.cam, W, H, self.params)
+        self.rays_per_step = self.counts["primary"]["rays"] + self.counts["secondary"]["rays"]
+        self.kernels_per_step = 2
+
+    def config(self):
+        st = self.scene.stats()
+        c = self.cfg
+        return {"workload": "heightfield 1024x1024 cells (2,097,152 tris) rope kd-tree; 1920x1080 "
+                            "primary + 1 shadow + 4 AO rays per hit",
+                "triangles": st["num_tris"], "kd_nodes": st["num_nodes"],
+                "kd_leaves": st["num_leaves"], "kd_refs": st["num_refs"],
+                "kd_build_s": round(self.build_s, 3), "image": [c.width, c.height],
+                "rays_per_step": self.rays_per_step,
+                "secondary_rays_per_step": self.counts["secondary"]["rays"],
+                "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        W, H = self.cfg.width, self.cfg.height
+        return [
+            ("ao_primary", lambda: self.scene.render_ao_primary(self.cam, W, H, self.params,
+                                                                self.primary, self.mask, stream)),
+            ("ao_secondary", lambda: self.scene.render_ao_secondary(self.mask, self.nsec, stream)),
+        ]
+
+    def alg_bytes(self):
+        """Algorithmic bytes per launch of each kernel:
+        8 B per inner-node step, 36 B per leaf visit (32 B box+range, 4 B
+        rope), 48 B per triangle test, 16 B hit + 4 B mask per primary ray,
+        32 B per queued secondary ray (written by the primary pass, read by
+        the secondary pass)."""
+        p, s = self.counts["primary"], self.counts["secondary"]
+        prim = 20 * p["rays"] + 8 * p["inner"] + 36 * p["leaf"] + 48 * p["tests"] + 32 * s["rays"]
+        sec = 32 * s["rays"] + 8 * s["inner"] + 36 * s["leaf"] + 48 * s["tests"]
+        return {"ao_primary": prim, "ao_secondary": sec}
+
+    def e2e_step(self, torch, stream, host_primary, host_mask):
+        W, H = self.cfg.width, self.cfg.height
+        self.scene.render_ao(self.cam, W, H, self.cfg.light_dir, self.cfg.ao_length,
+                             self.cfg.bias, self.cfg.ao_seed, self.primary, self.mask, self.nsec,
+                             stream)
+        host_primary.copy_(self.primary, non_blocking=True)
+        host_mask.copy_(self.mask, non_blocking=True)
+
+    def e2e_bytes(self):
+        W, H = self.cfg.width, self.cfg.height
+        import ctypes
+
+        h2d = ctypes.sizeof(self.rb.RCamera) + ctypes.sizeof(self.params)
+        return h2d, W * H * 16 + W * H * 4
+
+    def host_buffers(self, torch):
+        W, H = self.cfg.width, self.cfg.height
+        return (torch.empty((H * W, 4), dtype=torch.int32, pin_memory=True),
+                torch.empty(H * W, dtype=torch.int32, pin_memory=True))
+
+    def cpu_baseline(self, budget_s=12.0):
+        """The oracle's rope traversal of the same tree on the host cores."""
+        from oracle import pyoracle as po
+
+        st = self.scene.stats()
+        nodes, leaves, tris = self.scene.export()
+        kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+        packed = self.rb.pack_triangles(self.verts, self.faces)
+        W, H = self.cfg.width, self.cfg.height
+        rng = np.random.default_rng(0)
+        light = self.rb.unit(self.cfg.light_dir)
+        n = 20000
+        while True:
+            pix = rng.choice(W * H, n, replace=False).astype(np.uint32)
+            t0 = time.perf_counter()
+            _, _, nsec = po.frame_ao(kd, packed, self.cam, W, H, light, self.cfg.ao_length,
+                                     self.cfg.bias, self.cfg.ao_seed, pixels=pix)
+            dt = time.perf_counter() - t0
+            if dt > budget_s / 4 or n >= W * H:
+                break
+            n = min(W * H, int(n * min(8.0, budget_s / max(dt, 1e-3))))
+        return {"value": round((n + nsec) / dt / 1e6, 4), "unit": "Mrays/s", "cores": po.threads(),
+                "kind": "port",
+                "sample": f"{n} seeded-random pixels of the 1920x1080 frame with their shadow+AO "
+                          f"rays ({n + nsec} rays); oracle rope traversal over the same SAH tree, "
+                          "OpenMP schedule(dynamic) over pixels"}
+
+    def reference_step_fn(self):
+        """The reference's own path on the host: RKDTreeCPU as shipped (one
+        leaf) from oracle/_ref when present, traced by the restated traversal,
+        i.e. brute-force MT over every triangle per ray."""
+        from oracle import pyoracle as po
+
+        packed = self.rb.pack_triangles(self.verts, self.faces)
+        W, H = self.cfg.width, self.cfg.height
+        built_by = "restated single-leaf build"
+        bmin, bmax = packed_bounds(self.verts, self.faces)
+        if po.ref_lib() is not None:
+            nodes, idx, root, _, _ = po.ref_build(self.verts, self.faces)
+            rn = po.ref_node_fields(nodes[root])
+            assert rn["is_leaf"] and np.array_equal(idx, np.arange(len(idx)))
+            bmin, bmax = rn["min"], rn["max"]
+            built_by = "reference RKDTreeCPU/RKDThreeGPU (oracle/_ref, one leaf)"
+        light = self.rb.unit(self.cfg.light_dir)
+        rng = np.random.default_rng(1)
+        return built_by, lambda npix: po.frame_ao_bruteforce(
+            packed, bmin, bmax, self.cam, W, H, light, self.cfg.ao_length, self.cfg.bias,
+            self.cfg.ao_seed, rng.choice(W * H, npix, replace=False).astype(np.uint32))
+
+
+def packed_bounds(verts, faces):
+    v = verts[faces.reshape(-1)]
+    return v.min(0), v.max(0)
+
+
+class SoupPrimary:
+    name = "soup"
+
+    def __init__(self, torch, num_tris=65536):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.cfg = cfg = rb.configs.SoupConfig(num_tris=num_tris)
+        self.packed = cfg.packed()
+        t0 = time.time()
+        self.scene = rb.KDScene.from_packed(self.packed)
+        self.build_s = time.time() - t0
+        self.cam = cfg.camera()
+        W, H = cfg.width, cfg.height
+        self.out = torch.empty((H * W, 4), dtype=torch.int32, device="cuda")
+        c = self.scene.count_primary(self.cam, W, H).cpu().numpy().astype(np.int64)
+        self.tot = {"inner": int(c[:, 0].sum()), "leaf": int(c[:, 1].sum()),
+                    "tests": int(c[:, 2].sum()), "rays": W * H}
+        self.rays_per_step = W * H
+        self.kernels_per_step = 1
+
+    def config(self):
+        st = self.scene.stats()
+        return {"workload": f"triangle soup {st['num_tris']} tris rope kd-tree; "
+                            f"{self.cfg.width}x{self.cfg.height} primary rays",
+                "triangles": st["num_tris"], "kd_nodes": st["num_nodes"],
+                "kd_refs": st["num_refs"], "kd_build_s": round(self.build_s, 3),
+                "rays_per_step": self.rays_per_step, "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        W, H = self.cfg.width, self.cfg.height
+        return [("primary", lambda: self.scene.trace_primary(self.cam, W, H, 0, self.out, stream))]
+
+    def alg_bytes(self):
+        t = self.tot
+        return {"primary": 16 * t["rays"] + 8 * t["inner"] + 36 * t["leaf"] + 48 * t["tests"]}
+
+    def host_buffers(self, torch):
+        W, H = self.cfg.width, self.cfg.height
+        return (torch.empty((H * W, 4), dtype=torch.int32, pin_memory=True), None)
+
+    def e2e_step(self, torch, stream, host_out, _):
+        W, H = self.cfg.width, self.cfg.height
+        self.scene.trace_primary(self.cam, W, H, 0, self.out, stream)
+        host_out.copy_(self.out, non_blocking=True)
+
+    def e2e_bytes(self):
+        import ctypes
+
+        return ctypes.sizeof(self.rb.RCamera), self.cfg.width * self.cfg.height * 16
+
+    def cpu_baseline(self, budget_s=12.0):
+        from oracle import pyoracle as po
+
+        st = self.scene.stats()
+        nodes, leaves, tris = self.scene.export()
+        kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+        W, H = self.cfg.width, self.cfg.height
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < budget_s / 2:
+            po.primary_kd(kd, self.cam, W, H)
+            reps += 1
+        dt = time.perf_counter() - t0
+        return {"value": round(reps * W * H / dt / 1e6, 4), "unit": "Mrays/s", "cores": po.threads(),
+                "kind": "port", "sample": f"{reps} full {W}x{H} frames; oracle rope traversal over "
+                                          "the same SAH tree, OpenMP"}
+
+    def reference_step_fn(self):
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        v = self.packed
+        verts = np.stack([v[:, 0:3], v[:, 0:3] + v[:, 4:7], v[:, 0:3] + v[:, 8:11]], 1).reshape(-1, 3)
+        bmin, bmax = verts.min(0), verts.max(0)
+        rng = np.random.default_rng(1)
+        return "restated single-leaf build", lambda npix: (
+            po.primary_bruteforce(self.packed, bmin, bmax, self.cam, W, H,
+                                  pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32)),
+            npix)[1]
+
+
+class TerrainSDF:
+    name = "terrain_sdf"
+
+    def __init__(self, torch):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.cfg = cfg = rb.configs.TerrainConfig()
+        self.cam = cfg.camera()
+        self.params = cfg.params()
+        W, H = cfg.width, cfg.height
+        self.out = torch.empty((H * W, 8), dtype=torch.int32, device="cuda")
+        rb.sphere_trace(self.params, self.cam, W, H, self.out)
+        o = self.out.cpu().numpy()
+        self.steps = int(o[:, 6].astype(np.int64).sum())
+        self.hits = int((o[:, 7] == 1).sum())
+        self.rays_per_step = W * H
+        self.kernels_per_step = 1
+
+    def config(self):
+        return {"workload": "exact-SDF sphere tracing of d(p)=p.y-3fBm(0.25p), 8 octaves, "
+                            "1920x1080, step 0.6d, eps 1e-4, tmax 200, <=512 steps",
+                "field_evals_per_step": self.steps + 6 * self.hits,
+                "rays_per_step": self.rays_per_step, "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        W, H = self.cfg.width, self.cfg.height
+        return [("sdf", lambda: self.rb.sphere_trace(self.params, self.cam, W, H, self.out, stream))]
+
+    def alg_bytes(self):
+        return {"sdf": 32 * self.rays_per_step}
+
+    def host_buffers(self, torch):
+        W, H = self.cfg.width, self.cfg.height
+        return (torch.empty((H * W, 8), dtype=torch.int32, pin_memory=True), None)
+
+    def e2e_step(self, torch, stream, host_out, _):
+        W, H = self.cfg.width, self.cfg.height
+        self.rb.sphere_trace(self.params, self.cam, W, H, self.out, stream)
+        host_out.copy_(self.out, non_blocking=True)
+
+    def e2e_bytes(self):
+        import ctypes
+
+        return (ctypes.sizeof(self.rb.RCamera) + ctypes.sizeof(self.params),
+                self.cfg.width * self.cfg.height * 32)
+
+    def cpu_baseline(self, budget_s=12.0):
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        rng = np.random.default_rng(0)
+        n = 4000
+        P = po.perm(self.cfg.seed)
+        while True:
+            pix = rng.choice(W * H, n, replace=False).astype(np.uint32)
+            t0 = time.perf_counter()
+            po.sdf_image(P, self.cam, W, H, pixels=pix)
+            dt = time.perf_counter() - t0
+            if dt > budget_s / 4 or n >= W * H:
+                break
+            n = min(W * H, int(n * min(8.0, budget_s / max(dt, 1e-3))))
+        return {"value": round(n / dt / 1e6, 4), "unit": "Mrays/s", "cores": po.threads(),
+                "kind": "port", "sample": f"{n} seeded-random pixels; oracle exact-SDF march, OpenMP"}
+
+    def reference_step_fn(self):
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        P = po.perm(self.cfg.seed)
+        rng = np.random.default_rng(1)
+        return "restated exact-SDF march", lambda npix: (
+            po.sdf_image(P, self.cam, W, H,
+                         pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32)), npix)[1]
+
+
+WORKLOADS = {
+    "heightfield_ao": HeightfieldAO,
+    "soup": SoupPrimary,
+    "soup1m": lambda torch: SoupPrimary(torch, num_tris=1 << 20),
+    "terrain_sdf": TerrainSDF,
+}
+
+METRIC = "Mrays/s on 1 B200: plain rope-kd/exact-SDF vs wavefront+neural SDF @<=1e-3 err"
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args):
+    """--impl reference: rank 0 times the reference's CPU path; others exit."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.config](torch)
+    built_by, step = wl.reference_step_fn()
+    from oracle import pyoracle as po
+
+    # size one step to roughly one second of work on all host cores
+    npix = 4
+    t0 = time.perf_counter()
+    r = step(npix)
+    dt = time.perf_counter() - t0
+    npix = max(4, min(200000, int(npix * 1.0 / max(dt, 1e-4))))
+    for _ in range(args.warmup):
+        step(npix)
+    rays = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rays += step(npix)
+    dt = time.perf_counter() - t0
+    value = rays / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": wl.config(),
+        "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": po.threads(),
+                         "kind": "port",
+                         "sample": f"{npix} seeded-random pixels per step ({rays // args.steps} "
+                                   f"rays with their shadow/AO rays); tree: {built_by}; "
+                                   "traversal restated from ray_functions.cuh:231-360, "
+                                   "i.e. Moller-Trumbore over every triangle per ray"},
+        "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    init_dist(world)
+    dev = torch.device("cuda", local)
+    wl = WORKLOADS[args.config](torch)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    phases = wl.phases(stream)
+
+    def step():
+        for _, fn in phases:
+            fn()
+
+    for i in range(args.warmup):
+        flush.fill_(i & 0xFF)
+        step()
+    torch.cuda.synchronize()
+
+    n_ph = len(phases)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(n_ph + 1)] for _ in range(args.steps)]
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    clocks = ClockSampler(cvd.split(",")[local] if cvd else str(local))
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        for j, (_, fn) in enumerate(phases):
+            fn()
+            ev[k][j + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    step_ms = [ev[k][0].elapsed_time(ev[k][n_ph]) for k in range(args.steps)]
+    phase_ms = {name: statistics.mean(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(args.steps))
+                for j, (name, _) in enumerate(phases)}
+    ms = statistics.mean(step_ms)
+    ms_max = max_over_ranks(ms, world, dev)
+    value = world * wl.rays_per_step / (ms_max / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers (results copied to pinned memory)
+    hp, hm = wl.host_buffers(torch)
+    for i in range(2):
+        flush.fill_(i)
+        wl.e2e_step(torch, stream, hp, hm)
+    torch.cuda.synchronize()
+    e_ms = []
+    barrier(world)
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        wl.e2e_step(torch, stream, hp, hm)
+        torch.cuda.synchronize()
+        e_ms.append((time.perf_counter() - t0) * 1e3)
+    barrier(world)
+    e_ms_max = max_over_ranks(statistics.mean(e_ms), world, dev)
+    h2d, d2h = wl.e2e_bytes()
+
+    peaks = measured_peaks()
+    ab = wl.alg_bytes()
+    dom = max(phase_ms, key=phase_ms.get)
+    achieved = ab[dom] / (phase_ms[dom] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)", "config": dict(wl.config(), parallelism=f"replica x{world}"),
+        "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4),
+                     "peak_source": peaks["source"], "alg_bytes_per_launch": ab[dom],
+                     "traffic": ncu_traffic(f"{wl.name}:{dom}")},
+        "e2e": {"value": round(world * wl.rays_per_step / (e_ms_max / 1e3) / 1e6, 3),
+                "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": round(e_ms_max, 4)},
+        "gpu_launches": wl.kernels_per_step * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = wl.cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(WORKLOADS), default="heightfield_ao")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

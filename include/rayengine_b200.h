@@ -1,0 +1,244 @@
+/*
+ * rayengine_b200.h -- C ABI of the B200-native RayEngine ray-query path.
+ *
+ * Plain C types only (no CUDA or torch types): device buffers are passed as
+ * raw pointers to device memory, streams as an opaque `void*` holding a
+ * cudaStream_t (NULL = legacy default stream).  Every entry point returns a
+ * re_status; nothing calls exit().  The last error message of the calling
+ * thread is available from re_last_error().
+ *
+ * Reference interface each entry replaces (hadalhw17/RayEngine, paths
+ * relative to its repository root, "RE/" = RayEngine/src/):
+ *
+ *   re_scene_create / re_scene_create_packed
+ *       RKDTreeCPU::RKDTreeCPU + RKDThreeGPU::RKDThreeGPU + RTScene
+ *       init_triangles + copy_memory
+ *       (RE/Primitives/KDTree.cpp:117-173, RE/Primitives/KDThreeGPU.cpp:9-54,
+ *        RE/World/RTScene.cpp:210-285, RE/cuda-src/cuda_memory_functions.cuh:58-211)
+ *   re_scene_destroy          free of the copy_memory buffers (no reference free)
+ *   re_trace_primary          trace_primary_rays kernel launch in cuda_render_frame
+ *                             (RE/cuda-src/renderer.cu:390-410, :705-709)
+ *   re_trace_rays             trace_scene / trace_shadow on caller rays
+ *                             (RE/cuda-src/ray_functions.cuh:366-396)
+ *   re_render_ao              primary + shade()/trace_shadow shadow ray + hemisphere
+ *                             rays of trace_secondary_shadow_rays
+ *                             (RE/cuda-src/material_functions.cuh:99-119,
+ *                              RE/cuda-src/renderer.cu:537-613)
+ *   re_perlin_permutation     RPerlinNoise::RPerlinNoise (RE/World/PerlinNoise.h:16-52)
+ *   re_noise_fbm              eval / terrain fBm (RE/cuda-src/sdf_functions.cuh:84-206)
+ *   re_heightfield            generate_noise bake kernel (RE/cuda-src/renderer.cu:106-126,
+ *                             :813-836) producing a height grid
+ *   re_sdf_trace              render_sphere_trace's march
+ *                             (RE/cuda-src/renderer.cu:143-235,
+ *                              RE/cuda-src/sphere_tracing.cuh:183-216)
+ */
+#ifndef RAYENGINE_B200_H
+#define RAYENGINE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RE_API __attribute__((visibility("default")))
+#define RE_ABI_VERSION 1
+
+typedef enum re_status {
+  RE_OK = 0,
+  RE_ERR_INVALID_ARG = 1,   /* null pointer, zero size, bad flag           */
+  RE_ERR_CUDA = 2,          /* a CUDA runtime call or launch failed        */
+  RE_ERR_OUT_OF_MEMORY = 3, /* device or host allocation failed            */
+  RE_ERR_LIMIT = 4,         /* a size exceeds a documented maximum         */
+  RE_ERR_NO_DEVICE = 5,     /* no CUDA device / library built without one  */
+  RE_ERR_INTERNAL = 6
+} re_status;
+
+/* Same field order and size (88 bytes) as the reference's RCamera
+ * (RE/Primitives/Camera.h:7-16).  generate_ray reads campos, view, camdown,
+ * fov (full angles in degrees) and focial_distance. */
+typedef struct re_camera {
+  float campos[3], camdir[3], camright[3], camdown[3], lookat[3], view[3];
+  float fov[2];
+  float focial_distance, apertude_radius;
+} re_camera;
+
+/* Closest-hit record, 16 bytes: triangle index in the caller's face order
+ * (-1 = miss), ray parameter t (1e20 on a miss) and barycentrics u, v. */
+typedef struct re_hit {
+  int32_t id;
+  float t, u, v;
+} re_hit;
+
+/* A ray, 32 bytes: origin, maximum t, unit direction, caller tag. */
+typedef struct re_ray {
+  float o[3];
+  float tmax;
+  float d[3];
+  uint32_t tag;
+} re_ray;
+
+/* kd-tree build parameters (defaults from re_kd_params_default). */
+typedef struct re_kd_params {
+  uint32_t max_depth;      /* 24                                  */
+  uint32_t leaf_size;      /* 8: nodes above this size are split */
+  float cost_traversal;    /* SAH cost of one inner-node step     */
+  float cost_intersect;    /* SAH cost of one triangle test       */
+  float empty_bonus;       /* SAH discount for an empty child     */
+  uint32_t bfs_levels;     /* top levels laid out breadth-first   */
+  uint32_t threads;        /* host build threads, 0 = all         */
+  uint32_t max_leaf_visits;/* per-ray traversal bound             */
+} re_kd_params;
+
+typedef struct re_scene re_scene;
+
+typedef struct re_scene_stats {
+  uint32_t num_tris, num_nodes, num_leaves, num_refs;
+  uint32_t max_depth, max_leaf_size, bfs_nodes, pad;
+  float bmin[3], bmax[3];
+  double build_seconds;
+  uint64_t device_bytes;
+} re_scene_stats;
+
+/* Trace flags. */
+#define RE_TRACE_TWO_SIDED 0u /* KDTree.cpp:909-949 test (default) */
+#define RE_TRACE_ONE_SIDED 1u /* ray_functions.cuh:174-223 test     */
+#define RE_TRACE_ANY_HIT 2u   /* stop at the first hit (shadow)     */
+
+RE_API int re_abi_version(void);
+RE_API const char* re_status_string(re_status s);
+RE_API const char* re_last_error(void);
+RE_API void re_kd_params_default(re_kd_params* p);
+
+/* Indexed mesh: verts = num_verts x 3 floats, faces = num_faces x 3 indices.
+ * Builds the SAH kd-tree with ropes on the host, flattens it and uploads it
+ * to the current device.  The mesh arrays are read only during the call. */
+RE_API re_status re_scene_create(const float* verts, uint32_t num_verts,
+                                 const uint32_t* faces, uint32_t num_faces,
+                                 const re_kd_params* params, re_scene** out);
+/* The reference's packed triangles (RTScene.cpp:239-241): per triangle
+ * 12 floats {v0.xyz,0, e1.xyz,0, e2.xyz,0} with e = v - v0. */
+RE_API re_status re_scene_create_packed(const float* tris, uint32_t num_tris,
+                                        const re_kd_params* params,
+                                        re_scene** out);
+/* Host-only build of the same tree (no device upload): stats and export
+ * work, trace calls return RE_ERR_NO_DEVICE.  Lets a caller without a GPU
+ * inspect or serialise the tree. */
+RE_API re_status re_scene_build_host(const float* tris, uint32_t num_tris,
+                                     const re_kd_params* params, re_scene** out);
+RE_API re_status re_scene_stats_get(const re_scene* s, re_scene_stats* out);
+/* Copies the flattened host arrays (for checking): nodes 2 words each,
+ * leaves 16 words each, triangle references 12 words each.  Any pointer may
+ * be NULL; sizes come from re_scene_stats. */
+RE_API re_status re_scene_export(const re_scene* s, uint32_t* nodes,
+                                 uint32_t* leaves, float* tris);
+RE_API re_status re_scene_destroy(re_scene* s);
+
+/* Primary rays for every pixel of a w x h image (row-major, d_out has w*h
+ * entries).  flags: RE_TRACE_TWO_SIDED or RE_TRACE_ONE_SIDED. */
+RE_API re_status re_trace_primary(re_scene* s, const re_camera* cam,
+                                  uint32_t w, uint32_t h, uint32_t flags,
+                                  re_hit* d_out, void* stream);
+/* Caller rays (device array of n re_ray). */
+RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n,
+                               uint32_t flags, re_hit* d_out, void* stream);
+
+/* Per-pixel work counters of a primary-ray pass (device array of w*h
+ * uint4: inner-node steps, leaf visits, triangle tests, status).  Used to
+ * compute the algorithmic bytes of a pass. */
+RE_API re_status re_count_primary(re_scene* s, const re_camera* cam,
+                                  uint32_t w, uint32_t h, uint32_t flags,
+                                  uint32_t* d_counts, void* stream);
+
+/* Primary + shadow + ambient-occlusion frame.
+ *   d_primary: w*h re_hit (closest hit, two-sided)
+ *   d_mask:    w*h uint32, bit0 primary hit, bit1 shadow ray unoccluded,
+ *              bits 2..5 AO ray j unoccluded.
+ * Secondary rays start at hit + n * bias (n = geometric normal facing the
+ * ray); the shadow ray goes along light_dir without bound, the four
+ * cosine-weighted AO rays are ao_length long.  The secondary-ray queue is
+ * owned by the scene and grown on demand (5 rays per pixel). */
+typedef struct re_ao_params {
+  float light_dir[3]; /* unit vector */
+  float ao_length;
+  float bias;
+  uint32_t seed;
+} re_ao_params;
+RE_API re_status re_render_ao(re_scene* s, const re_camera* cam, uint32_t w,
+                              uint32_t h, const re_ao_params* p,
+                              re_hit* d_primary, uint32_t* d_mask,
+                              uint32_t* d_num_secondary, void* stream);
+/* The two passes of re_render_ao as separate calls (same results), so a
+ * caller can time or overlap them: the primary pass writes d_primary and
+ * d_mask and fills the scene's secondary-ray queue, the secondary pass
+ * traces that queue into d_mask. */
+RE_API re_status re_render_ao_primary(re_scene* s, const re_camera* cam,
+                                      uint32_t w, uint32_t h,
+                                      const re_ao_params* p, re_hit* d_primary,
+                                      uint32_t* d_mask, void* stream);
+RE_API re_status re_render_ao_secondary(re_scene* s, uint32_t* d_mask,
+                                        uint32_t* d_num_secondary,
+                                        void* stream);
+/* Work counters of the same frame (device array of 8 uint64): primary
+ * inner-node steps, leaf visits, triangle tests, rays; then the same four
+ * for the secondary rays.  Used for the algorithmic bytes of each pass. */
+RE_API re_status re_render_ao_counts(re_scene* s, const re_camera* cam,
+                                     uint32_t w, uint32_t h,
+                                     const re_ao_params* p, uint64_t* d_totals,
+                                     void* stream);
+
+/* ---- noise -------------------------------------------------------- */
+/* RPerlinNoise(seed).permutationTable: 512 entries (256 duplicated). */
+RE_API re_status re_perlin_permutation(uint32_t seed, uint32_t* out512);
+
+typedef struct re_fbm_params {
+  uint32_t seed;     /* permutation table seed (RPerlinNoise default 2016) */
+  uint32_t octaves;
+  float lacunarity;  /* 2.0 */
+  float gain;        /* 0.5 */
+  float scale;       /* input scale applied before octave 0 */
+  float amplitude;   /* output scale */
+} re_fbm_params;
+/* d_pts: n x 3 floats; d_out[i] = amplitude * fbm(scale * p_i). */
+RE_API re_status re_noise_fbm(const re_fbm_params* p, const float* d_pts,
+                              uint32_t n, float* d_out, void* stream);
+/* Height grid of (cells+1)^2 vertices over [lo,hi]^2 (x fastest), written as
+ * xyz floats with y = amplitude * fbm(x, 0, z) (lacunarity/gain from p). */
+RE_API re_status re_heightfield(const re_fbm_params* p, uint32_t cells,
+                                float lo, float hi, float* d_verts,
+                                void* stream);
+/* Host helpers that generate the synthetic scenes. */
+RE_API re_status re_gen_soup(uint64_t seed, uint32_t n, float* verts);
+RE_API re_status re_gen_grid_faces(uint32_t cells, uint32_t* faces);
+
+/* ---- exact-SDF sphere tracing ---------------------------------------- */
+typedef struct re_sdf_params {
+  uint32_t seed;       /* permutation table seed                     */
+  uint32_t octaves;    /* 8                                         */
+  float scale;         /* 0.25: d(p) = p.y - amplitude*fbm(scale*p) */
+  float amplitude;     /* 3                                         */
+  float step_factor;   /* 0.6                                       */
+  float eps;           /* 1e-4                                      */
+  float tmax;          /* 200                                       */
+  uint32_t max_steps;  /* 512                                       */
+} re_sdf_params;
+
+/* 32 bytes per pixel: hit position, unit normal (central differences),
+ * number of field evaluations of the march, status (1 hit, 0 left the
+ * [0,tmax] range, 2 step bound reached). */
+typedef struct re_sdf_hit {
+  float pos[3];
+  float normal[3];
+  uint32_t steps;
+  uint32_t status;
+} re_sdf_hit;
+
+RE_API re_status re_sdf_trace(const re_sdf_params* p, const re_camera* cam,
+                              uint32_t w, uint32_t h, re_sdf_hit* d_out,
+                              void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

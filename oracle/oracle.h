@@ -1,0 +1,126 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- the CPU oracle.
+ *
+ * A plain-C restatement of RayEngine's ray-query hot path, used by tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker.
+ * Nothing in the product (rayengine_b200/) links, loads or calls it.
+ *
+ * Parity pin: the Perlin permutation table and the as-shipped kd-tree (a
+ * single leaf => brute-force Moller-Trumbore in index order) are checked
+ * against the reference's own host code compiled from its sources
+ * (oracle/_ref/libre_ref.so, recipe oracle/Makefile.ref) and against the
+ * golden fixtures under tests/golden/ generated from it.
+ *
+ * Floating point: compiled with -ffp-contract=off.  Every fused multiply-add
+ * is an explicit fmaf(), every division and square root is IEEE, so the CUDA
+ * kernels (built with -fmad=false and the same explicit fmaf calls) produce
+ * bit-identical results.
+ */
+#ifndef RE_ORACLE_H
+#define RE_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float x, y, z; } of3;
+
+/* --- camera (RayEngine/src/cuda-src/ray_functions.cuh:14-55) ------------ */
+typedef struct {
+  float campos[3], view[3], camdown[3];
+  float fov[2];
+  float focal;
+} o_camera;
+
+/* per-frame constants the reference recomputes per pixel */
+typedef struct {
+  float campos[3], middle[3], horizontal[3], vertical[3];
+  float focal;
+} o_camera_basis;
+
+void o_camera_setup(const o_camera* cam, o_camera_basis* out);
+void o_generate_ray(const o_camera_basis* b, uint32_t w, uint32_t h,
+                    uint32_t x, uint32_t y, float o[3], float d[3]);
+
+/* --- ray/box and ray/triangle ------------------------------------------ */
+/* ray_functions.cuh:62-92 */
+int o_ray_box(const float bmin[3], const float bmax[3], const float o[3],
+              const float d[3], float* t_near, float* t_far);
+/* mode 0: two-sided (KDTree.cpp:909-949, |a|<1e-5, t>1e-5)
+ * mode 1: one-sided (ray_functions.cuh:174-223, a<1e-4 rejected, t>1e-4) */
+int o_ray_tri(const float o[3], const float d[3], const float v0[3],
+              const float e1[3], const float e2[3], int mode, float* t,
+              float* u, float* v);
+
+typedef struct { int32_t id; float t, u, v; } o_hit;
+
+/* Reference as shipped: RKDTreeCPU with MAX_DEPTH=1 is one leaf holding every
+ * triangle, so stackless_kdtree_traversal (ray_functions.cuh:231-360) is a
+ * root-box test followed by an index-order MT loop keeping t < t_exit.
+ * tris: n x 12 floats {v0.xyz,_, e1.xyz,_, e2.xyz,_}. */
+void o_trace_bruteforce(const float* tris, int32_t n, const float bmin[3],
+                        const float bmax[3], const float o[3], const float d[3],
+                        int mode, o_hit* out);
+
+/* --- the project's flattened kd-tree (same layout the kernels read) ---- */
+typedef struct {
+  const float* nodes;      /* 2 x 32-bit per node: split, meta            */
+  const float* leaves;     /* 16 x 32-bit per leaf                        */
+  const float* tris;       /* 12 floats per reference, leaf order         */
+  float bmin[3], bmax[3];  /* root box                                    */
+} o_kdtree;
+
+typedef struct {
+  uint32_t inner_visits, leaf_visits, tri_tests, status;
+} o_counts;
+
+/* The reference's rope traversal restated over the project's tree, with the
+ * exit face taken from the slab test (not the reference's 1e-4 proximity test).
+ * anyhit != 0: stop at the first hit with t < tmax (shadow/AO rays). */
+void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
+                float tmax, int mode, int anyhit, uint32_t max_leaf_visits,
+                o_hit* out, o_counts* cnt);
+
+/* --- Perlin / fBm (sdf_functions.cuh:26-135, PerlinNoise.h:16-52) ------ */
+void o_perlin_permutation(uint32_t seed, uint32_t perm[512]);
+float o_perlin(const uint32_t perm[512], float x, float y, float z);
+float o_fbm(const uint32_t perm[512], float x, float y, float z, int octaves,
+            float lacunarity, float gain);
+/* heightfield: y = amp * fbm(x, 0, z) */
+float o_height(const uint32_t perm[512], float x, float z, int octaves,
+               float amp);
+/* volumetric terrain d(p) = p.y - amp * fbm(scale * p) */
+float o_terrain_density(const uint32_t perm[512], const float p[3], int octaves,
+                        float scale, float amp);
+
+/* --- scene generators -------------------------------------------------- */
+uint64_t o_mt64_next(uint64_t* state /* 312 + 1 words */);
+void o_gen_soup(uint64_t seed, int32_t n, float* verts /* n*9 */);
+/* grid of (cells+1)^2 vertices over [lo,hi]^2, 2*cells^2 triangles */
+void o_gen_heightfield(const uint32_t perm[512], int32_t cells, float lo,
+                       float hi, int octaves, float amp, float* verts,
+                       uint32_t* faces);
+
+/* --- exact-SDF sphere tracer (sphere_tracing.cuh:183-216) --------------- */
+typedef struct {
+  float pos[3], normal[3];
+  uint32_t steps, status; /* status: 1 hit, 0 miss, 2 step cap */
+  float t, pad;
+} o_sdf_hit;
+
+void o_sdf_trace(const uint32_t perm[512], const float o[3], const float d[3],
+                 int octaves, float scale, float amp, float step_factor,
+                 float eps, float tmax, uint32_t max_steps, o_sdf_hit* out);
+
+/* --- deterministic sampling shared with the kernels -------------------- */
+uint32_t o_hash_u32(uint32_t a, uint32_t b, uint32_t c);
+void o_sincos_2pi(float u, float* s, float* c);
+void o_secondary_rays(const float hitp[3], const float n[3], uint32_t seed,
+                      uint32_t pixel, const float light_dir[3], float bias,
+                      float o_out[5][3], float d_out[5][3], float tmax_out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

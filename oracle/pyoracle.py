@@ -1,0 +1,323 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle (liboracle.so).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
+reference legs, as the checker.  The product (rayengine_b200/) never imports
+it.  Build with `make -f oracle/Makefile`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libre_ref.so")
+
+HIT_DTYPE = np.dtype([("id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+COUNT_DTYPE = np.dtype([("inner", "<u4"), ("leaf", "<u4"), ("tests", "<u4"), ("status", "<u4")])
+SDF_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<f4", 3), ("steps", "<u4"),
+                      ("status", "<u4"), ("t", "<f4"), ("pad", "<f4")])
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `make -f oracle/Makefile`")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.o_ray_tri.restype = ctypes.c_int
+        _lib.o_perlin.restype = ctypes.c_float
+        _lib.o_perlin.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        _lib.o_fbm.restype = ctypes.c_float
+        _lib.o_fbm.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_int, ctypes.c_float, ctypes.c_float]
+        _lib.o_hash_u32.restype = ctypes.c_uint32
+        _lib.o_hash_u32.argtypes = [ctypes.c_uint32] * 3
+        _lib.o_sincos_2pi.argtypes = [ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.o_max_threads.restype = ctypes.c_int
+    return _lib
+
+
+class OCamera(ctypes.Structure):
+    _fields_ = [("campos", ctypes.c_float * 3), ("view", ctypes.c_float * 3),
+                ("camdown", ctypes.c_float * 3), ("fov", ctypes.c_float * 2),
+                ("focal", ctypes.c_float)]
+
+
+class OKdTree(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("leaves", ctypes.c_void_p),
+                ("tris", ctypes.c_void_p), ("bmin", ctypes.c_float * 3),
+                ("bmax", ctypes.c_float * 3)]
+
+
+def camera(re_cam) -> OCamera:
+    """Oracle camera from a product re_camera (same field values)."""
+    c = OCamera()
+    c.campos[:] = list(re_cam.campos)
+    c.view[:] = list(re_cam.view)
+    c.camdown[:] = list(re_cam.camdown)
+    c.fov[:] = list(re_cam.fov)
+    c.focal = re_cam.focial_distance
+    return c
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def threads() -> int:
+    return lib().o_max_threads()
+
+
+def perm(seed: int) -> np.ndarray:
+    out = np.zeros(512, np.uint32)
+    lib().o_perlin_permutation(ctypes.c_uint32(seed), _p(out))
+    return out
+
+
+def soup(seed: int, n: int) -> np.ndarray:
+    v = np.zeros((n, 3, 3), np.float32)
+    lib().o_gen_soup(ctypes.c_uint64(seed), ctypes.c_int32(n), _p(v))
+    return v
+
+
+def heightfield(p: np.ndarray, cells: int, lo: float, hi: float, octaves: int, amp: float):
+    nv = cells + 1
+    verts = np.zeros((nv * nv, 3), np.float32)
+    faces = np.zeros((2 * cells * cells, 3), np.uint32)
+    lib().o_gen_heightfield(_p(p), ctypes.c_int32(cells), ctypes.c_float(lo), ctypes.c_float(hi),
+                            ctypes.c_int(octaves), ctypes.c_float(amp), _p(verts), _p(faces))
+    return verts, faces
+
+
+def fbm_batch(p, pts, octaves, lac=2.0, gain=0.5, scale=1.0, amp=1.0, nthreads=0):
+    pts = np.ascontiguousarray(pts, np.float32)
+    out = np.zeros(pts.shape[0], np.float32)
+    lib().o_batch_fbm(_p(p), _p(pts), ctypes.c_int64(pts.shape[0]), ctypes.c_int(octaves),
+                      ctypes.c_float(lac), ctypes.c_float(gain), ctypes.c_float(scale),
+                      ctypes.c_float(amp), _p(out), ctypes.c_int(nthreads))
+    return out
+
+
+class KdTree:
+    """Oracle view of a flattened tree (arrays from KDScene.export())."""
+
+    def __init__(self, nodes, leaves, tris, bmin, bmax):
+        self.nodes = np.ascontiguousarray(nodes, np.uint32)
+        self.leaves = np.ascontiguousarray(leaves, np.uint32)
+        self.tris = np.ascontiguousarray(tris, np.float32)
+        self.s = OKdTree()
+        self.s.nodes = self.nodes.ctypes.data
+        self.s.leaves = self.leaves.ctypes.data
+        self.s.tris = self.tris.ctypes.data
+        self.s.bmin[:] = [float(x) for x in bmin]
+        self.s.bmax[:] = [float(x) for x in bmax]
+
+
+def primary_kd(kd: KdTree, cam, w, h, mode=0, max_visits=16384, pixels=None, counts=False,
+               nthreads=0):
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, HIT_DTYPE)
+    cnt = np.zeros(n, COUNT_DTYPE) if counts else None
+    oc = camera(cam)
+    lib().o_batch_primary_kd(ctypes.byref(kd.s), ctypes.byref(oc), ctypes.c_uint32(w),
+                             ctypes.c_uint32(h), ctypes.c_int(mode), ctypes.c_uint32(max_visits),
+                             _p(pix), ctypes.c_int64(n), _p(out), _p(cnt), ctypes.c_int(nthreads))
+    return (out, cnt) if counts else out
+
+
+def primary_bruteforce(tris_packed, bmin, bmax, cam, w, h, mode=0, pixels=None, nthreads=0):
+    tris = np.ascontiguousarray(tris_packed, np.float32)
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, HIT_DTYPE)
+    oc = camera(cam)
+    b0 = (ctypes.c_float * 3)(*bmin)
+    b1 = (ctypes.c_float * 3)(*bmax)
+    lib().o_batch_primary_bruteforce(_p(tris), ctypes.c_int32(tris.shape[0]), b0, b1,
+                                     ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                                     ctypes.c_int(mode), _p(pix), ctypes.c_int64(n), _p(out),
+                                     ctypes.c_int(nthreads))
+    return out
+
+
+def rays_kd(kd: KdTree, rays, mode=0, anyhit=False, max_visits=16384, nthreads=0):
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = np.zeros(rays.shape[0], HIT_DTYPE)
+    lib().o_batch_rays_kd(ctypes.byref(kd.s), _p(rays), ctypes.c_int64(rays.shape[0]),
+                          ctypes.c_int(mode), ctypes.c_int(1 if anyhit else 0),
+                          ctypes.c_uint32(max_visits), _p(out), ctypes.c_int(nthreads))
+    return out
+
+
+def frame_ao(kd: KdTree, packed, cam, w, h, light_dir, ao_length, bias, seed, pixels=None,
+             max_visits=16384, nthreads=0, totals=False):
+    packed = np.ascontiguousarray(packed, np.float32)
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, HIT_DTYPE)
+    mask = np.zeros(n, np.uint32)
+    nsec = ctypes.c_uint32(0)
+    tot = np.zeros(8, np.uint64)
+    oc = camera(cam)
+    ld = (ctypes.c_float * 3)(*light_dir)
+    lib().o_batch_frame_ao(ctypes.byref(kd.s), _p(packed), ctypes.byref(oc), ctypes.c_uint32(w),
+                           ctypes.c_uint32(h), ld, ctypes.c_float(ao_length), ctypes.c_float(bias),
+                           ctypes.c_uint32(seed), ctypes.c_uint32(max_visits), _p(pix),
+                           ctypes.c_int64(n), _p(out), _p(mask), ctypes.byref(nsec), _p(tot),
+                           ctypes.c_int(nthreads))
+    if totals:
+        return out, mask, nsec.value, tot
+    return out, mask, nsec.value
+
+
+def sdf_image(p, cam, w, h, octaves=8, scale=0.25, amp=3.0, step_factor=0.6, eps=1e-4,
+              tmax=200.0, max_steps=512, pixels=None, nthreads=0):
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, SDF_DTYPE)
+    oc = camera(cam)
+    lib().o_batch_sdf(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                      ctypes.c_int(octaves), ctypes.c_float(scale), ctypes.c_float(amp),
+                      ctypes.c_float(step_factor), ctypes.c_float(eps), ctypes.c_float(tmax),
+                      ctypes.c_uint32(max_steps), _p(pix), ctypes.c_int64(n), _p(out),
+                      ctypes.c_int(nthreads))
+    return out
+
+
+def sincos_2pi(u: float):
+    s = ctypes.c_float()
+    c = ctypes.c_float()
+    lib().o_sincos_2pi(ctypes.c_float(u), ctypes.byref(s), ctypes.byref(c))
+    return s.value, c.value
+
+
+def hash_u32(a, b, c) -> int:
+    return lib().o_hash_u32(a, b, c)
+
+
+# ---------------------------------------------------------- FP64 judge
+def edge_margin(packed, ids, o, d):
+    """Barycentric margin min(u, v, 1-u-v) of the ray against triangle ids,
+    in float64 (the relative edge distance used to exempt grazing rays)."""
+    packed = np.asarray(packed, np.float64)
+    T = packed[ids]
+    v0, e1, e2 = T[:, 0:3], T[:, 4:7], T[:, 8:11]
+    o = np.asarray(o, np.float64)
+    d = np.asarray(d, np.float64)
+    h = np.cross(d, e2)
+    a = np.einsum("ij,ij->i", e1, h)
+    s = o - v0
+    f = 1.0 / a
+    u = f * np.einsum("ij,ij->i", s, h)
+    q = np.cross(s, e1)
+    v = f * np.einsum("ij,ij->i", d, q)
+    return np.minimum(np.minimum(u, v), 1.0 - u - v)
+
+
+def camera_rays(cam, w, h, pixels):
+    """Float64 ray origins/directions of the given pixels (judge only)."""
+    campos = np.array(cam.campos, np.float64)
+    view = np.array(cam.view, np.float64)
+    view /= np.linalg.norm(view)
+    down = np.array(cam.camdown, np.float64)
+    down /= np.linalg.norm(down)
+    hx = np.cross(view, down)
+    hx /= np.linalg.norm(hx)
+    vx = np.cross(hx, view)
+    vx /= np.linalg.norm(vx)
+    th = np.tan(np.radians(cam.fov[0]) * 0.5)
+    tv = np.tan(np.radians(cam.fov[1]) * 0.5)
+    pixels = np.asarray(pixels)
+    x = (pixels % w).astype(np.float64)
+    y = (pixels // w).astype(np.float64)
+    sx = x / (w - 1.0)
+    sy = 1.0 - y / (h - 1.0)
+    p = campos + view + hx * th * (2 * sx - 1)[:, None] + vx * tv * (2 * sy - 1)[:, None]
+    d = (p - campos) * cam.focial_distance
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.broadcast_to(campos, d.shape).copy(), d
+
+
+# ---------------------------------------------- the reference, compiled
+def ref_lib():
+    """The reference's own host code (oracle/_ref/libre_ref.so), or None."""
+    if not os.path.exists(REF_LIB_PATH):
+        return None
+    L = ctypes.CDLL(REF_LIB_PATH)
+    L.ref_sizeof_node.restype = ctypes.c_int
+    L.ref_build_kdtree.restype = ctypes.c_int
+    return L
+
+
+def ref_build(verts, faces):
+    """Reference RKDTreeCPU + RKDThreeGPU over a mesh -> (raw 128-byte node
+    records, obj_index_list, root, levels, leaves)."""
+    L = ref_lib()
+    if L is None:
+        raise FileNotFoundError(REF_LIB_PATH)
+    verts = np.ascontiguousarray(verts, np.float32)
+    faces = np.ascontiguousarray(faces, np.uint32)
+    max_nodes = 4 * faces.shape[0] + 16
+    nodes = np.zeros((max_nodes, 128), np.uint8)
+    idx = np.zeros(64 * faces.shape[0] + 16, np.int32)
+    root, nidx, levels, leaves = (ctypes.c_int() for _ in range(4))
+    nn = L.ref_build_kdtree(_p(verts), ctypes.c_int(verts.shape[0]), _p(faces),
+                            ctypes.c_int(faces.shape[0]), _p(nodes), ctypes.c_int(max_nodes),
+                            _p(idx), ctypes.c_int(idx.shape[0]), ctypes.byref(root),
+                            ctypes.byref(nidx), ctypes.byref(levels), ctypes.byref(leaves))
+    if nn < 0:
+        raise RuntimeError("reference tree larger than the buffers")
+    return nodes[:nn].copy(), idx[: nidx.value].copy(), root.value, levels.value, leaves.value
+
+
+def ref_perm(seed: int) -> np.ndarray:
+    L = ref_lib()
+    if L is None:
+        raise FileNotFoundError(REF_LIB_PATH)
+    out = np.zeros(512, np.uint32)
+    L.ref_perlin_permutation(ctypes.c_uint32(seed), _p(out))
+    return out
+
+
+def ref_node_fields(raw: np.ndarray) -> dict:
+    """Decode one 128-byte RKDTreeNodeGPU (KDTreeGPUUtills.h:34-46, x86-64
+    layout: box 24 B, axis i32, split f32, 5 x size_t, bool, 6 x size_t)."""
+    b = raw.tobytes()
+    box = np.frombuffer(b[0:24], np.float32)
+    axis = int(np.frombuffer(b[24:28], np.int32)[0])
+    split = float(np.frombuffer(b[28:32], np.float32)[0])
+    left, right, first, num, nnodes = np.frombuffer(b[32:72], np.uint64)
+    is_leaf = bool(b[72])
+    ropes = np.frombuffer(b[80:128], np.int64)
+    return {"min": box[:3].copy(), "max": box[3:].copy(), "axis": axis, "split": split,
+            "left": int(left), "right": int(right), "first": int(first), "num_objs": int(num),
+            "is_leaf": is_leaf, "ropes": ropes.copy()}
+
+
+def frame_ao_bruteforce(packed, bmin, bmax, cam, w, h, light_dir, ao_length, bias, seed, pixels,
+                        nthreads=0, return_results=False):
+    """Reference-as-shipped AO frame on a pixel sample; returns rays traced."""
+    packed = np.ascontiguousarray(packed, np.float32)
+    pix = np.ascontiguousarray(pixels, np.uint32)
+    n = pix.shape[0]
+    out = np.zeros(n, HIT_DTYPE)
+    mask = np.zeros(n, np.uint32)
+    nsec = ctypes.c_uint32(0)
+    oc = camera(cam)
+    b0 = (ctypes.c_float * 3)(*[float(x) for x in bmin])
+    b1 = (ctypes.c_float * 3)(*[float(x) for x in bmax])
+    ld = (ctypes.c_float * 3)(*light_dir)
+    lib().o_batch_frame_ao_bruteforce(_p(packed), ctypes.c_int32(packed.shape[0]), b0, b1,
+                                      ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h), ld,
+                                      ctypes.c_float(ao_length), ctypes.c_float(bias),
+                                      ctypes.c_uint32(seed), _p(pix), ctypes.c_int64(n), _p(out),
+                                      _p(mask), ctypes.byref(nsec), ctypes.c_int(nthreads))
+    if return_results:
+        return out, mask, nsec.value
+    return n + nsec.value

@@ -1,0 +1,157 @@
+"""ctypes binding of librayengine_b200.so (declarations: include/rayengine_b200.h).
+
+The shared library is the product: there is no Python or CPU fallback.  If
+the library is missing this module raises at import time.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librayengine_b200.so")
+
+
+class RayEngineError(RuntimeError):
+    """A C-ABI call returned a non-zero re_status."""
+
+    def __init__(self, status: int, fn: str, message: str):
+        super().__init__(f"{fn} failed with status {status}: {message}")
+        self.status = status
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+        "or `make -f rayengine_b200/csrc/Makefile`"
+    )
+
+lib = ctypes.CDLL(LIB_PATH)
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_u32_p = ctypes.POINTER(ctypes.c_uint32)
+
+
+class re_camera(ctypes.Structure):
+    """Same layout as the reference's RCamera (Camera.h:7-16), 88 bytes."""
+
+    _fields_ = [
+        ("campos", ctypes.c_float * 3),
+        ("camdir", ctypes.c_float * 3),
+        ("camright", ctypes.c_float * 3),
+        ("camdown", ctypes.c_float * 3),
+        ("lookat", ctypes.c_float * 3),
+        ("view", ctypes.c_float * 3),
+        ("fov", ctypes.c_float * 2),
+        ("focial_distance", ctypes.c_float),
+        ("apertude_radius", ctypes.c_float),
+    ]
+
+
+class re_kd_params(ctypes.Structure):
+    _fields_ = [
+        ("max_depth", ctypes.c_uint32),
+        ("leaf_size", ctypes.c_uint32),
+        ("cost_traversal", ctypes.c_float),
+        ("cost_intersect", ctypes.c_float),
+        ("empty_bonus", ctypes.c_float),
+        ("bfs_levels", ctypes.c_uint32),
+        ("threads", ctypes.c_uint32),
+        ("max_leaf_visits", ctypes.c_uint32),
+    ]
+
+
+class re_scene_stats(ctypes.Structure):
+    _fields_ = [
+        ("num_tris", ctypes.c_uint32),
+        ("num_nodes", ctypes.c_uint32),
+        ("num_leaves", ctypes.c_uint32),
+        ("num_refs", ctypes.c_uint32),
+        ("max_depth", ctypes.c_uint32),
+        ("max_leaf_size", ctypes.c_uint32),
+        ("bfs_nodes", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("bmin", ctypes.c_float * 3),
+        ("bmax", ctypes.c_float * 3),
+        ("build_seconds", ctypes.c_double),
+        ("device_bytes", ctypes.c_uint64),
+    ]
+
+
+class re_ao_params(ctypes.Structure):
+    _fields_ = [
+        ("light_dir", ctypes.c_float * 3),
+        ("ao_length", ctypes.c_float),
+        ("bias", ctypes.c_float),
+        ("seed", ctypes.c_uint32),
+    ]
+
+
+class re_fbm_params(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint32),
+        ("octaves", ctypes.c_uint32),
+        ("lacunarity", ctypes.c_float),
+        ("gain", ctypes.c_float),
+        ("scale", ctypes.c_float),
+        ("amplitude", ctypes.c_float),
+    ]
+
+
+class re_sdf_params(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint32),
+        ("octaves", ctypes.c_uint32),
+        ("scale", ctypes.c_float),
+        ("amplitude", ctypes.c_float),
+        ("step_factor", ctypes.c_float),
+        ("eps", ctypes.c_float),
+        ("tmax", ctypes.c_float),
+        ("max_steps", ctypes.c_uint32),
+    ]
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_SIGS = {
+    "re_abi_version": (ctypes.c_int, []),
+    "re_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "re_last_error": (ctypes.c_char_p, []),
+    "re_kd_params_default": (None, [ctypes.POINTER(re_kd_params)]),
+    "re_scene_create": (ctypes.c_int, [_P, _U32, _P, _U32, ctypes.POINTER(re_kd_params), ctypes.POINTER(_P)]),
+    "re_scene_create_packed": (ctypes.c_int, [_P, _U32, ctypes.POINTER(re_kd_params), ctypes.POINTER(_P)]),
+    "re_scene_build_host": (ctypes.c_int, [_P, _U32, ctypes.POINTER(re_kd_params), ctypes.POINTER(_P)]),
+    "re_scene_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(re_scene_stats)]),
+    "re_scene_export": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_scene_destroy": (ctypes.c_int, [_P]),
+    "re_trace_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P]),
+    "re_trace_rays": (ctypes.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "re_count_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P]),
+    "re_render_ao": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
+    "re_render_ao_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P]),
+    "re_render_ao_secondary": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_render_ao_counts": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P]),
+    "re_perlin_permutation": (ctypes.c_int, [_U32, _P]),
+    "re_noise_fbm": (ctypes.c_int, [ctypes.POINTER(re_fbm_params), _P, _U32, _P, _P]),
+    "re_heightfield": (ctypes.c_int, [ctypes.POINTER(re_fbm_params), _U32, ctypes.c_float, ctypes.c_float, _P, _P]),
+    "re_gen_soup": (ctypes.c_int, [ctypes.c_uint64, _U32, _P]),
+    "re_gen_grid_faces": (ctypes.c_int, [_U32, _P]),
+    "re_sdf_trace": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+for _name, (_res, _args) in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def check(status: int, fn: str) -> None:
+    if status != 0:
+        msg = lib.re_last_error()
+        raise RayEngineError(status, fn, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib, name)(*args), name)

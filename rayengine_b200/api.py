@@ -1,0 +1,331 @@
+"""Host-side mirror of RayEngine's ray-query interface over the C ABI.
+
+Names follow the reference (hadalhw17/RayEngine, "RE/" = RayEngine/src/):
+
+* ``RCamera`` / ``build_camera``  -- RE/Primitives/Camera.h:7-16,
+  RE/Objects/MovableCamera.cpp:101-118 (camdown = (0,-1,0), fov in degrees).
+* ``RPerlinNoise``                -- RE/World/PerlinNoise.h:16-52.
+* ``KDScene``                     -- RKDTreeCPU + RKDThreeGPU + RTScene +
+  copy_memory (RE/Primitives/KDTree.cpp:117-173, RE/Primitives/KDThreeGPU.cpp:9-54,
+  RE/World/RTScene.cpp:40-62,179-285, RE/cuda-src/cuda_memory_functions.cuh:58-211),
+  with ``trace_primary`` standing for the trace_primary_rays launch
+  (RE/cuda-src/renderer.cu:390-410,705-709).
+* ``generate_noise`` / ``heightfield`` -- the generate_noise bake
+  (RE/cuda-src/renderer.cu:106-126,813-836).
+* ``sphere_trace``                -- render_sphere_trace's terrain march
+  (RE/cuda-src/renderer.cu:143-235, RE/cuda-src/sphere_tracing.cuh:183-216).
+
+Device buffers are torch CUDA tensors (torch is only the allocator and the
+stream provider); every computation runs in librayengine_b200.so.  Errors
+raise RayEngineError carrying the library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import RayEngineError, call, lib  # noqa: F401
+
+TRACE_TWO_SIDED = 0
+TRACE_ONE_SIDED = 1
+TRACE_ANY_HIT = 2
+
+HIT_DTYPE = np.dtype([("id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+SDF_HIT_DTYPE = np.dtype(
+    [("pos", "<f4", 3), ("normal", "<f4", 3), ("steps", "<u4"), ("status", "<u4")]
+)
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def _dptr(t) -> int:
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+# ---------------------------------------------------------------- camera
+RCamera = _lib.re_camera
+
+
+def build_camera(campos: Sequence[float], lookat: Sequence[float],
+                 fov: Sequence[float] = (60.0, 60.0), focal: float = 1.0) -> RCamera:
+    """RMovableCamera::build_camera with the view pointing at ``lookat``."""
+    c = RCamera()
+    v = np.asarray(lookat, np.float64) - np.asarray(campos, np.float64)
+    v = v / np.linalg.norm(v)
+    c.campos[:] = [float(x) for x in campos]
+    c.view[:] = [float(x) for x in v]
+    c.camdir[:] = [float(x) for x in v]
+    c.lookat[:] = [float(x) for x in lookat]
+    c.camdown[:] = [0.0, -1.0, 0.0]
+    c.fov[:] = [float(fov[0]), float(fov[1])]
+    c.focial_distance = float(focal)
+    c.apertude_radius = 0.0
+    return c
+
+
+def vertical_fov(fov_x_deg: float, width: int, height: int) -> float:
+    """Full vertical angle matching fov_x on a width x height image (the
+    intent of RMovableCamera::set_fovx, MovableCamera.cpp:38-42)."""
+    return math.degrees(2.0 * math.atan(math.tan(math.radians(fov_x_deg) * 0.5) * height / width))
+
+
+# ----------------------------------------------------------------- noise
+class RPerlinNoise:
+    """RPerlinNoise(seed): the 512-entry permutation table."""
+
+    def __init__(self, seed: int = 2016):
+        self.seed = int(seed)
+        tab = np.zeros(512, np.uint32)
+        call("re_perlin_permutation", self.seed, tab.ctypes.data)
+        self.permutationTable = tab
+
+
+def fbm_params(seed=2016, octaves=6, lacunarity=2.0, gain=0.5, scale=1.0, amplitude=1.0):
+    p = _lib.re_fbm_params()
+    p.seed, p.octaves, p.lacunarity, p.gain = seed, octaves, lacunarity, gain
+    p.scale, p.amplitude = scale, amplitude
+    return p
+
+
+def generate_noise(params, pts, out=None, stream=None):
+    """Batch fBm: out[i] = amplitude * fbm(scale * pts[i]); pts (n,3) float32 CUDA."""
+    import torch
+
+    n = pts.shape[0]
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=pts.device)
+    call("re_noise_fbm", ctypes.byref(params), _dptr(pts), n, _dptr(out), _stream_ptr(stream))
+    return out
+
+
+def heightfield(params, cells: int, lo: float, hi: float, out=None, stream=None):
+    """(cells+1)^2 x 3 vertex grid with y = amplitude * fbm(x, 0, z)."""
+    import torch
+
+    nv = (cells + 1) * (cells + 1)
+    if out is None:
+        out = torch.empty((nv, 3), dtype=torch.float32, device="cuda")
+    call("re_heightfield", ctypes.byref(params), cells, lo, hi, _dptr(out), _stream_ptr(stream))
+    return out
+
+
+def grid_faces(cells: int) -> np.ndarray:
+    f = np.empty((2 * cells * cells, 3), np.uint32)
+    call("re_gen_grid_faces", cells, f.ctypes.data)
+    return f
+
+
+def triangle_soup(n: int, seed: int = 0) -> np.ndarray:
+    """(n, 3, 3) float32 vertices of the seeded soup."""
+    v = np.empty((n, 3, 3), np.float32)
+    call("re_gen_soup", seed, n, v.ctypes.data)
+    return v
+
+
+def pack_triangles(verts: np.ndarray, faces: np.ndarray) -> np.ndarray:
+    """RTScene::init_triangles packing: per face {v0,0, v1-v0,0, v2-v0,0}."""
+    v0 = verts[faces[:, 0]]
+    p = np.zeros((faces.shape[0], 12), np.float32)
+    p[:, 0:3] = v0
+    p[:, 4:7] = verts[faces[:, 1]] - v0
+    p[:, 8:11] = verts[faces[:, 2]] - v0
+    return p
+
+
+# ------------------------------------------------------------- kd scene
+def kd_params(**kw):
+    p = _lib.re_kd_params()
+    lib.re_kd_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class KDScene:
+    """A rope kd-tree scene resident on the current CUDA device."""
+
+    def __init__(self, handle: int):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def from_mesh(cls, verts: np.ndarray, faces: np.ndarray, params=None) -> "KDScene":
+        verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        faces = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+        h = ctypes.c_void_p()
+        call("re_scene_create", verts.ctypes.data, verts.shape[0], faces.ctypes.data,
+             faces.shape[0], ctypes.byref(params) if params is not None else None, ctypes.byref(h))
+        return cls(h.value)
+
+    @classmethod
+    def from_packed(cls, tris: np.ndarray, params=None) -> "KDScene":
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 12)
+        h = ctypes.c_void_p()
+        call("re_scene_create_packed", tris.ctypes.data, tris.shape[0],
+             ctypes.byref(params) if params is not None else None, ctypes.byref(h))
+        return cls(h.value)
+
+    @classmethod
+    def build_host(cls, tris: np.ndarray, params=None) -> "KDScene":
+        """Build the tree on the host only (no device); stats/export work."""
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 12)
+        h = ctypes.c_void_p()
+        call("re_scene_build_host", tris.ctypes.data, tris.shape[0],
+             ctypes.byref(params) if params is not None else None, ctypes.byref(h))
+        return cls(h.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib.re_scene_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stats(self) -> dict:
+        s = _lib.re_scene_stats()
+        call("re_scene_stats_get", self._h, ctypes.byref(s))
+        return {
+            "num_tris": s.num_tris, "num_nodes": s.num_nodes, "num_leaves": s.num_leaves,
+            "num_refs": s.num_refs, "max_depth": s.max_depth, "max_leaf_size": s.max_leaf_size,
+            "bfs_nodes": s.bfs_nodes, "bmin": list(s.bmin), "bmax": list(s.bmax),
+            "build_seconds": s.build_seconds, "device_bytes": s.device_bytes,
+        }
+
+    def export(self):
+        """(nodes uint32 (N,2), leaves uint32 (L,16), tris float32 (R,12))."""
+        st = self.stats()
+        nodes = np.empty((st["num_nodes"], 2), np.uint32)
+        leaves = np.empty((st["num_leaves"], 16), np.uint32)
+        tris = np.empty((st["num_refs"], 12), np.float32)
+        call("re_scene_export", self._h, nodes.ctypes.data, leaves.ctypes.data, tris.ctypes.data)
+        return nodes, leaves, tris
+
+    def trace_primary(self, cam: RCamera, w: int, h: int, flags: int = TRACE_TWO_SIDED,
+                      out=None, stream=None):
+        """Closest hits for every pixel -> int32 CUDA tensor (h*w, 4) = re_hit."""
+        import torch
+
+        if out is None:
+            out = torch.empty((h * w, 4), dtype=torch.int32, device="cuda")
+        call("re_trace_primary", self._h, ctypes.byref(cam), w, h, flags, _dptr(out),
+             _stream_ptr(stream))
+        return out
+
+    def count_primary(self, cam: RCamera, w: int, h: int, flags: int = TRACE_TWO_SIDED,
+                      out=None, stream=None):
+        """Per-pixel (inner steps, leaf visits, triangle tests, status)."""
+        import torch
+
+        if out is None:
+            out = torch.empty((h * w, 4), dtype=torch.int32, device="cuda")
+        call("re_count_primary", self._h, ctypes.byref(cam), w, h, flags, _dptr(out),
+             _stream_ptr(stream))
+        return out
+
+    def trace_rays(self, rays, flags: int = TRACE_TWO_SIDED, out=None, stream=None):
+        """rays: float32 CUDA tensor (n, 8) = re_ray {o, tmax, d, tag}."""
+        import torch
+
+        n = rays.shape[0]
+        if out is None:
+            out = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+        call("re_trace_rays", self._h, _dptr(rays), n, flags, _dptr(out), _stream_ptr(stream))
+        return out
+
+    def render_ao(self, cam: RCamera, w: int, h: int, light_dir=(0.3, 1.0, 0.2),
+                  ao_length: float = 1.0, bias: float = 1e-4, seed: int = 0,
+                  primary=None, mask=None, nsec=None, stream=None):
+        """Primary + shadow + 4 AO rays -> (hits (h*w,4) int32, mask (h*w,) int32, n_secondary)."""
+        import torch
+
+        if primary is None:
+            primary = torch.empty((h * w, 4), dtype=torch.int32, device="cuda")
+        if mask is None:
+            mask = torch.empty(h * w, dtype=torch.int32, device="cuda")
+        if nsec is None:
+            nsec = torch.zeros(1, dtype=torch.int32, device="cuda")
+        p = ao_params(light_dir, ao_length, bias, seed)
+        call("re_render_ao", self._h, ctypes.byref(cam), w, h, ctypes.byref(p), _dptr(primary),
+             _dptr(mask), _dptr(nsec), _stream_ptr(stream))
+        return primary, mask, nsec
+
+    def render_ao_primary(self, cam: RCamera, w: int, h: int, params, primary, mask,
+                          stream=None):
+        call("re_render_ao_primary", self._h, ctypes.byref(cam), w, h, ctypes.byref(params),
+             _dptr(primary), _dptr(mask), _stream_ptr(stream))
+
+    def render_ao_secondary(self, mask, nsec=None, stream=None):
+        call("re_render_ao_secondary", self._h, _dptr(mask),
+             _dptr(nsec) if nsec is not None else None, _stream_ptr(stream))
+
+    def render_ao_counts(self, cam: RCamera, w: int, h: int, params, stream=None) -> dict:
+        """Traversal work of the AO frame (sums over all rays of each pass)."""
+        import torch
+
+        t = torch.zeros(8, dtype=torch.int64, device="cuda")
+        call("re_render_ao_counts", self._h, ctypes.byref(cam), w, h, ctypes.byref(params),
+             _dptr(t), _stream_ptr(stream))
+        v = [int(x) for x in t.cpu().tolist()]
+        keys = ("inner", "leaf", "tests", "rays")
+        return {"primary": dict(zip(keys, v[:4])), "secondary": dict(zip(keys, v[4:]))}
+
+
+def unit(v) -> list:
+    """Unit vector as float32 values (light directions)."""
+    v = np.asarray(v, np.float64)
+    return [float(x) for x in (v / np.linalg.norm(v)).astype(np.float32)]
+
+
+def ao_params(light_dir, ao_length=1.0, bias=1e-4, seed=0):
+    p = _lib.re_ao_params()
+    p.light_dir[:] = unit(light_dir)
+    p.ao_length, p.bias, p.seed = ao_length, bias, seed
+    return p
+
+
+# ----------------------------------------------------------- SDF tracing
+def sdf_params(seed=2016, octaves=8, scale=0.25, amplitude=3.0, step_factor=0.6, eps=1e-4,
+               tmax=200.0, max_steps=512):
+    p = _lib.re_sdf_params()
+    p.seed, p.octaves, p.scale, p.amplitude = seed, octaves, scale, amplitude
+    p.step_factor, p.eps, p.tmax, p.max_steps = step_factor, eps, tmax, max_steps
+    return p
+
+
+def sphere_trace(params, cam: RCamera, w: int, h: int, out=None, stream=None):
+    """Exact-SDF march per pixel -> int32 CUDA tensor (h*w, 8) = re_sdf_hit."""
+    import torch
+
+    if out is None:
+        out = torch.empty((h * w, 8), dtype=torch.int32, device="cuda")
+    call("re_sdf_trace", ctypes.byref(params), ctypes.byref(cam), w, h, _dptr(out),
+         _stream_ptr(stream))
+    return out

@@ -1,0 +1,105 @@
+"""The seeded synthetic workloads (no dataset is involved; every input is
+generated from a seed with the shapes and distributions below).
+
+soup:        N triangles, centroid ~ U[-1,1]^3, vertex offsets ~ N(0, 0.02)
+             per axis (mt19937_64 seed 0); camera at (0,0,3) looking at the
+             origin, 60x60 degree field of view, 512x512 primary rays.  The
+             "1M-triangle scene" is the same generator with N = 2^20.
+heightfield: 1024x1024 cells over [-10,10]^2 (2,097,152 triangles), height =
+             2 * fBm(x, 0, z) with RPerlinNoise(2016), 6 octaves, lacunarity 2,
+             gain 0.5; camera at (0,8,-14) looking at the origin, 60 degree
+             horizontal field of view, 1920x1080, plus one shadow ray toward
+             normalize(0.3,1,0.2) and four cosine-weighted AO rays of length 1
+             per primary hit.
+terrain SDF: d(p) = p.y - 3 * fBm(0.25 p), RPerlinNoise(2016), 8 octaves;
+             camera at (0,6,-20) looking at the origin, 60 degree horizontal
+             field of view, 1920x1080, step 0.6 d, eps 1e-4, tmax 200, at most
+             512 steps.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import api
+
+PERLIN_SEED = 2016  # RPerlinNoise's default seed (PerlinNoise.h:16)
+
+
+@dataclass
+class SoupConfig:
+    num_tris: int = 65536
+    seed: int = 0
+    width: int = 512
+    height: int = 512
+    campos: tuple = (0.0, 0.0, 3.0)
+    lookat: tuple = (0.0, 0.0, 0.0)
+    fov: tuple = (60.0, 60.0)
+
+    def camera(self):
+        return api.build_camera(self.campos, self.lookat, self.fov)
+
+    def packed(self) -> np.ndarray:
+        v = api.triangle_soup(self.num_tris, self.seed)
+        p = np.zeros((self.num_tris, 12), np.float32)
+        p[:, 0:3] = v[:, 0]
+        p[:, 4:7] = v[:, 1] - v[:, 0]
+        p[:, 8:11] = v[:, 2] - v[:, 0]
+        return p
+
+
+@dataclass
+class HeightfieldConfig:
+    cells: int = 1024
+    lo: float = -10.0
+    hi: float = 10.0
+    octaves: int = 6
+    amplitude: float = 2.0
+    seed: int = PERLIN_SEED
+    width: int = 1920
+    height: int = 1080
+    campos: tuple = (0.0, 8.0, -14.0)
+    lookat: tuple = (0.0, 0.0, 0.0)
+    fov_x: float = 60.0
+    light_dir: tuple = (0.3, 1.0, 0.2)
+    ao_length: float = 1.0
+    bias: float = 1e-4
+    ao_seed: int = 7
+
+    def camera(self):
+        fy = api.vertical_fov(self.fov_x, self.width, self.height)
+        return api.build_camera(self.campos, self.lookat, (self.fov_x, fy))
+
+    def fbm(self):
+        return api.fbm_params(seed=self.seed, octaves=self.octaves, amplitude=self.amplitude)
+
+    def mesh_on_device(self, stream=None):
+        """(vertices as a host array, faces) with heights computed on the GPU."""
+        verts = api.heightfield(self.fbm(), self.cells, self.lo, self.hi, stream=stream)
+        return verts.cpu().numpy(), api.grid_faces(self.cells)
+
+
+@dataclass
+class TerrainConfig:
+    seed: int = PERLIN_SEED
+    octaves: int = 8
+    scale: float = 0.25
+    amplitude: float = 3.0
+    step_factor: float = 0.6
+    eps: float = 1e-4
+    tmax: float = 200.0
+    max_steps: int = 512
+    width: int = 1920
+    height: int = 1080
+    campos: tuple = (0.0, 6.0, -20.0)
+    lookat: tuple = (0.0, 0.0, 0.0)
+    fov_x: float = 60.0
+
+    def camera(self):
+        fy = api.vertical_fov(self.fov_x, self.width, self.height)
+        return api.build_camera(self.campos, self.lookat, (self.fov_x, fy))
+
+    def params(self):
+        return api.sdf_params(self.seed, self.octaves, self.scale, self.amplitude,
+                              self.step_factor, self.eps, self.tmax, self.max_steps)

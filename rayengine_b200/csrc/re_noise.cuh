@@ -1,0 +1,109 @@
+// Improved-Perlin noise and fBm on the device.
+//
+// Value part of eval() (RayEngine/src/cuda-src/sdf_functions.cuh:84-135):
+// lattice cell from floor & 255, quintic fade (:57-60), 16-case gradient dot
+// (:26-47) and the k0..k7 polynomial form of the trilinear blend.  The
+// reference's hash (:77-81) reads a linearly filtered, normalised-float
+// texture and cannot be reproduced; the lattice hash here is
+// P[P[P[x] + y] + z] over RPerlinNoise's table (PerlinNoise.h:16-52), which
+// the kernels keep in shared memory.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "re_math.cuh"
+
+namespace re {
+
+struct PermTable {
+  uint8_t p[512];
+};
+
+__device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
+  for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) s[i] = t.p[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ float grad_dot(uint32_t h, float x, float y, float z) {
+  switch (h & 15u) {
+    case 0: return x + y;
+    case 1: return -x + y;
+    case 2: return x - y;
+    case 3: return -x - y;
+    case 4: return x + z;
+    case 5: return -x + z;
+    case 6: return x - z;
+    case 7: return -x - z;
+    case 8: return y + z;
+    case 9: return -y + z;
+    case 10: return y - z;
+    case 11: return -y - z;
+    case 12: return y + x;
+    case 13: return -x + y;
+    case 14: return -y + z;
+    default: return -y - z;
+  }
+}
+
+__device__ __forceinline__ float quintic(float t) {
+  float in = __fmaf_rn(t, 6.0f, -15.0f);
+  in = __fmaf_rn(t, in, 10.0f);
+  return ((t * t) * t) * in;
+}
+
+__device__ __forceinline__ float perlin(const uint32_t* __restrict__ P, float x, float y, float z) {
+  float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  int xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
+  int xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
+  float tx = x - fx, ty = y - fy, tz = z - fz;
+  float u = quintic(tx), v = quintic(ty), w = quintic(tz);
+  float x1 = tx - 1.0f, y1 = ty - 1.0f, z1 = tz - 1.0f;
+  uint32_t px0 = P[xi0], px1 = P[xi1];
+  uint32_t p00 = P[px0 + yi0], p10 = P[px1 + yi0];
+  uint32_t p01 = P[px0 + yi1], p11 = P[px1 + yi1];
+  float a = grad_dot(P[p00 + zi0], tx, ty, tz);
+  float b = grad_dot(P[p10 + zi0], x1, ty, tz);
+  float c = grad_dot(P[p01 + zi0], tx, y1, tz);
+  float d = grad_dot(P[p11 + zi0], x1, y1, tz);
+  float e = grad_dot(P[p00 + zi1], tx, ty, z1);
+  float f = grad_dot(P[p10 + zi1], x1, ty, z1);
+  float g = grad_dot(P[p01 + zi1], tx, y1, z1);
+  float h = grad_dot(P[p11 + zi1], x1, y1, z1);
+  float k1 = b - a;
+  float k2 = c - a;
+  float k3 = e - a;
+  float k4 = ((a + d) - b) - c;
+  float k5 = ((a + f) - b) - e;
+  float k6 = ((a + g) - c) - e;
+  float k7 = ((((((b + c) + e) + h) - a) - d) - f) - g;
+  float r = __fmaf_rn(k1, u, a);
+  r = __fmaf_rn(k2, v, r);
+  r = __fmaf_rn(k3, w, r);
+  r = __fmaf_rn(k4, u * v, r);
+  r = __fmaf_rn(k5, u * w, r);
+  r = __fmaf_rn(k6, v * w, r);
+  r = __fmaf_rn(k7, (u * v) * w, r);
+  return r;
+}
+
+__device__ __forceinline__ float fbm(const uint32_t* __restrict__ P, float x, float y, float z,
+                                     uint32_t octaves, float lacunarity, float gain) {
+  float sum = 0.0f, amp = 1.0f;
+  for (uint32_t i = 0; i < octaves; ++i) {
+    sum = __fmaf_rn(amp, perlin(P, x, y, z), sum);
+    x *= lacunarity;
+    y *= lacunarity;
+    z *= lacunarity;
+    amp *= gain;
+  }
+  return sum;
+}
+
+// d(p) = p.y - amp * fbm(scale * p), lacunarity 2, gain 0.5
+__device__ __forceinline__ float terrain_density(const uint32_t* __restrict__ P, V3 p,
+                                                 uint32_t octaves, float scale, float amp) {
+  float f = fbm(P, scale * p.x, scale * p.y, scale * p.z, octaves, 2.0f, 0.5f);
+  return __fmaf_rn(-amp, f, p.y);
+}
+
+}  // namespace re

@@ -1,0 +1,823 @@
+// Rope kd-tree scenes on the device and the traversal kernels.
+//
+// Replaces, in the reference (hadalhw17/RayEngine, "RE/" = RayEngine/src/):
+//   copy_memory            RE/cuda-src/cuda_memory_functions.cuh:58-211
+//   stackless_kdtree_traversal, gpu_ray_box_intersect, gpu_ray_tri_intersect,
+//   is_point_to_the_left_of_split, get_neighboring_node_index
+//                          RE/cuda-src/ray_functions.cuh:62-92,174-360,
+//                          RE/cuda-src/kd_tree_functions.cuh:10-62
+//   trace_primary_rays     RE/cuda-src/renderer.cu:390-410
+//   trace_shadow / shade   RE/cuda-src/ray_functions.cuh:366-374,
+//                          RE/cuda-src/material_functions.cuh:99-119
+//   hemisphere sampling    RE/cuda-src/renderer.cu:537-613,
+//                          RE/cuda-src/cuda_helper_functions.h:197-216
+//
+// Kernel design (sm_100a):
+//   * persistent warps: each warp takes 8x4 pixel tiles (or 32 queued rays)
+//     from a global counter until the frame is done, so long and short rays
+//     are balanced across the 148 SMs;
+//   * the breadth-first top of the node array is staged in shared memory
+//     once per resident block;
+//   * nodes are 8 bytes, leaves 64 bytes, triangle references 48 bytes, all
+//     read with 8/16-byte vector loads through the read-only path;
+//   * secondary rays are appended to a queue with one warp-aggregated atomic
+//     per warp (ballot + popc).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "kd_build.hpp"
+#include "re_common.hpp"
+#include "re_math.cuh"
+
+namespace re {
+
+constexpr float K_INF = 1e20f;  // RE/RayEngine/RayEngine.h:24
+
+struct KdDev {
+  const uint2* __restrict__ nodes;
+  const float4* __restrict__ leaves;
+  const float4* __restrict__ tris;
+  V3 bmin, bmax;
+  uint32_t max_visits;
+  uint32_t stage;  // nodes [0, stage) are read from shared memory
+};
+
+struct Counters {
+  uint32_t inner, leaf, tests, status;
+};
+
+// gpu_ray_box_intersect (ray_functions.cuh:62-92)
+__device__ __forceinline__ bool ray_box(V3 lo, V3 hi, V3 o, V3 inv, float& tn, float& tf) {
+  float t1 = (lo.x - o.x) * inv.x, t2 = (hi.x - o.x) * inv.x;
+  float t3 = (lo.y - o.y) * inv.y, t4 = (hi.y - o.y) * inv.y;
+  float t5 = (lo.z - o.z) * inv.z, t6 = (hi.z - o.z) * inv.z;
+  float tmin = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
+  float tmax = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
+  if (tmax < 0.0f) return false;
+  if (tmin > tmax) return false;
+  tn = tmin >= 0.0f ? tmin : 0.0f;
+  tf = tmax;
+  return true;
+}
+
+// Moller-Trumbore.  MODE 0: two-sided (KDTree.cpp:909-949), MODE 1:
+// back faces culled (ray_functions.cuh:174-223).
+template <int MODE>
+__device__ __forceinline__ bool ray_tri(V3 o, V3 d, float4 T0, float4 T1, float4 T2,
+                                        float& t, float& u, float& v) {
+  V3 v0 = {T0.x, T0.y, T0.z}, e1 = {T1.x, T1.y, T1.z}, e2 = {T2.x, T2.y, T2.z};
+  V3 h = cross(d, e2);
+  float a = dot(e1, h);
+  if (MODE == 0) {
+    if (a > -0.00001f && a < 0.00001f) return false;
+  } else {
+    if (a < 1e-4f) return false;
+  }
+  float f = 1.0f / a;
+  V3 s = sub(o, v0);
+  float uu = f * dot(s, h);
+  if (uu < 0.0f || uu > 1.0f) return false;
+  V3 q = cross(s, e1);
+  float vv = f * dot(d, q);
+  if (vv < 0.0f || uu + vv > 1.0f) return false;
+  float tt = f * dot(e2, q);
+  if (!(tt > (MODE == 0 ? 0.00001f : 1e-4f))) return false;
+  t = tt;
+  u = uu;
+  v = vv;
+  return true;
+}
+
+struct HitState {
+  float t, u, v;
+  int32_t id;
+  uint32_t ref;  // leaf-order triangle slot of the best hit
+};
+
+__device__ __forceinline__ uint2 load_node(const KdDev& kd, const uint2* snodes, uint32_t i) {
+  return i < kd.stage ? snodes[i] : __ldg(&kd.nodes[i]);
+}
+
+// Stackless rope traversal (stackless_kdtree_traversal,
+// ray_functions.cuh:231-360) with the exit face taken from the slab test and
+// split decisions made on the ray parameter so that a point on a split plane
+// goes to the side the ray moves into.  Returns false when the ray misses the
+// root box.
+template <int MODE, bool ANYHIT, bool COUNT>
+__device__ __forceinline__ void traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
+                                         float tmax, HitState& hs, Counters& c) {
+  hs.t = K_INF;
+  hs.u = 0.f;
+  hs.v = 0.f;
+  hs.id = -1;
+  hs.ref = 0xFFFFFFFFu;
+  V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  float t_entry, t_root_exit;
+  if (!ray_box(kd.bmin, kd.bmax, o, inv, t_entry, t_root_exit)) return;
+  float best_t = fminf(t_root_exit, tmax);
+  int32_t best_id = -1;
+  float best_u = 0.f, best_v = 0.f;
+  uint32_t best_ref = 0xFFFFFFFFu;
+  uint32_t node = 0, visits = 0;
+  bool done = false;
+  while (!done && t_entry < best_t) {
+    uint2 nd = load_node(kd, snodes, node);
+    while ((nd.y & 3u) != 3u) {
+      uint32_t k = nd.y & 3u;
+      float split = __uint_as_float(nd.x);
+      float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
+      bool left;
+      if (dk > 0.0f)
+        left = t_entry < (split - ok) * ik;
+      else if (dk < 0.0f)
+        left = t_entry >= (split - ok) * ik;
+      else
+        left = ok < split;
+      node = (nd.y >> 2) + (left ? 0u : 1u);
+      nd = load_node(kd, snodes, node);
+      if (COUNT) c.inner++;
+    }
+    const float4* L = kd.leaves + 4 * (size_t)(nd.y >> 2);
+    float4 A = __ldg(L), B = __ldg(L + 1);
+    if (COUNT) c.leaf++;
+    uint32_t first = __float_as_uint(B.z), count = __float_as_uint(B.w);
+    for (uint32_t i = first; i < first + count; ++i) {
+      const float4* T = kd.tris + 3 * (size_t)i;
+      float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
+      int32_t id = __float_as_int(T0.w);
+      float t, u, v;
+      if (COUNT) c.tests++;
+      if (ray_tri<MODE>(o, d, T0, T1, T2, t, u, v)) {
+        if (t < best_t || (t == best_t && id < best_id && best_id >= 0)) {
+          best_t = t;
+          best_id = id;
+          best_u = u;
+          best_v = v;
+          best_ref = i;
+          if (ANYHIT) {
+            done = true;
+            break;
+          }
+        }
+      }
+    }
+    if (done) break;
+    float texit = __int_as_float(0x7f800000);
+    int face = -1;
+    {
+      float tk;
+      if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
+      else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
+      if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
+      else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
+      if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
+      else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
+    }
+    if (face < 0) break;
+    t_entry = fmaxf(t_entry, texit);
+    if (!(t_entry < best_t)) break;
+    int32_t rope = __ldg(reinterpret_cast<const int32_t*>(L + 2) + face);
+    if (rope < 0) break;
+    node = (uint32_t)rope;
+    if (++visits >= kd.max_visits) {
+      c.status = 1;
+      break;
+    }
+  }
+  if (best_id >= 0) {
+    hs.t = best_t;
+    hs.u = best_u;
+    hs.v = best_v;
+    hs.id = best_id;
+    hs.ref = best_ref;
+  }
+}
+
+__device__ __forceinline__ void stage_nodes(const KdDev& kd, uint2* snodes) {
+  for (uint32_t i = threadIdx.x; i < kd.stage; i += blockDim.x) snodes[i] = __ldg(&kd.nodes[i]);
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter) {
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t t = 0;
+  if (lane == 0) t = atomicAdd(counter, 1u);
+  return __shfl_sync(0xFFFFFFFFu, t, 0);
+}
+
+__device__ __forceinline__ void store_hit(re_hit* out, size_t i, const HitState& hs) {
+  reinterpret_cast<int4*>(out)[i] =
+      make_int4(hs.id, __float_as_int(hs.t), __float_as_int(hs.u), __float_as_int(hs.v));
+}
+
+// --------------------------------------------------------------- kernels
+// Primary rays, persistent warps over 8x4 pixel tiles.
+template <int MODE, bool COUNT>
+__global__ void __launch_bounds__(256) k_primary(KdDev kd, CamDev cam, uint32_t w, uint32_t h,
+                                                 re_hit* __restrict__ out,
+                                                 uint4* __restrict__ counts,
+                                                 uint32_t* __restrict__ tile_counter) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
+  for (;;) {
+    uint32_t tile = warp_fetch(tile_counter);
+    if (tile >= tiles) break;
+    uint32_t x = (tile % tiles_x) * 8 + (lane & 7u);
+    uint32_t y = (tile / tiles_x) * 4 + (lane >> 3);
+    if (x >= w || y >= h) continue;
+    V3 o, d;
+    generate_ray(cam, w, h, x, y, o, d);
+    HitState hs;
+    Counters c = {0, 0, 0, 0};
+    traverse<MODE, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), hs, c);
+    size_t pix = (size_t)y * w + x;
+    if (COUNT)
+      counts[pix] = make_uint4(c.inner, c.leaf, c.tests, c.status);
+    else
+      store_hit(out, pix, hs);
+  }
+}
+
+// Caller rays (re_ray), persistent warps over 32-ray chunks.
+template <int MODE, bool ANYHIT>
+__global__ void __launch_bounds__(256) k_rays(KdDev kd, const float4* __restrict__ rays,
+                                              uint32_t n, re_hit* __restrict__ out,
+                                              uint32_t* __restrict__ counter) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t chunk = warp_fetch(counter);
+    uint32_t i = chunk * 32 + lane;
+    if (chunk * 32 >= n) break;
+    if (i >= n) continue;
+    float4 R0 = __ldg(&rays[2 * (size_t)i]), R1 = __ldg(&rays[2 * (size_t)i + 1]);
+    V3 o = {R0.x, R0.y, R0.z}, d = {R1.x, R1.y, R1.z};
+    HitState hs;
+    Counters c = {0, 0, 0, 0};
+    traverse<MODE, ANYHIT, false>(kd, snodes, o, d, R0.w, hs, c);
+    store_hit(out, i, hs);
+  }
+}
+
+// Primary + secondary-ray generation for the AO frame.
+struct AoDev {
+  V3 light;
+  float ao_length, bias;
+  uint32_t seed;
+};
+
+// Warp-sum of per-thread work counters, one 64-bit atomic per warp and field.
+__device__ __forceinline__ void flush_counts(const Counters& c, uint32_t rays,
+                                             unsigned long long* totals) {
+  uint32_t v[4] = {c.inner, c.leaf, c.tests, rays};
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    uint32_t x = v[f];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, off);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(&totals[f], (unsigned long long)x);
+  }
+}
+
+// Primary rays of the AO frame: closest hit, pixel mask bit 0, and the five
+// secondary rays of every hit appended to the queue (one warp-aggregated
+// atomic per warp).  COUNT: also sum the traversal work into totals[0..3].
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev ao, uint32_t w,
+                                                    uint32_t h, re_hit* __restrict__ out,
+                                                    uint32_t* __restrict__ mask,
+                                                    float4* __restrict__ queue,
+                                                    uint32_t* __restrict__ counters,
+                                                    unsigned long long* __restrict__ totals) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
+  Counters c = {0, 0, 0, 0};
+  uint32_t rays = 0;
+  for (;;) {
+    uint32_t tile = warp_fetch(&counters[0]);
+    if (tile >= tiles) break;
+    uint32_t x = (tile % tiles_x) * 8 + (lane & 7u);
+    uint32_t y = (tile / tiles_x) * 4 + (lane >> 3);
+    bool valid = x < w && y < h;
+    HitState hs;
+    hs.id = -1;
+    V3 o = {0, 0, 0}, d = {0, 0, 1};
+    if (valid) {
+      generate_ray(cam, w, h, x, y, o, d);
+      traverse<0, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), hs, c);
+      ++rays;
+      size_t pix = (size_t)y * w + x;
+      if (!COUNT) {
+        store_hit(out, pix, hs);
+        mask[pix] = hs.id >= 0 ? 1u : 0u;
+      }
+    }
+    bool hit = valid && hs.id >= 0;
+    uint32_t ballot = __ballot_sync(0xFFFFFFFFu, hit);
+    if (!ballot) continue;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&counters[1], 5u * __popc(ballot));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (!hit) continue;
+    uint32_t slot = base + 5u * __popc(ballot & ((1u << lane) - 1u));
+    // geometric normal of the hit triangle, facing the incoming ray
+    const float4* T = kd.tris + 3 * (size_t)hs.ref;
+    float4 T1 = __ldg(T + 1), T2 = __ldg(T + 2);
+    V3 n = normalize(cross(v3(T1.x, T1.y, T1.z), v3(T2.x, T2.y, T2.z)));
+    if (dot(n, d) > 0.0f) n = v3(-n.x, -n.y, -n.z);
+    V3 p = {__fmaf_rn(hs.t, d.x, o.x), __fmaf_rn(hs.t, d.y, o.y), __fmaf_rn(hs.t, d.z, o.z)};
+    V3 org = {__fmaf_rn(n.x, ao.bias, p.x), __fmaf_rn(n.y, ao.bias, p.y),
+              __fmaf_rn(n.z, ao.bias, p.z)};
+    uint32_t pix = y * w + x;
+    queue[2 * (size_t)slot] = make_float4(org.x, org.y, org.z, K_INF);
+    queue[2 * (size_t)slot + 1] = make_float4(ao.light.x, ao.light.y, ao.light.z,
+                                              __uint_as_float(pix * 8u + 1u));
+    // createCoordinateSystem (cuda_helper_functions.h:197-204)
+    V3 nt;
+    if (fabsf(n.x) > fabsf(n.y)) {
+      float iv = 1.0f / sqrtf(__fmaf_rn(n.z, n.z, n.x * n.x));
+      nt = v3(n.z * iv, 0.0f, -n.x * iv);
+    } else {
+      float iv = 1.0f / sqrtf(__fmaf_rn(n.z, n.z, n.y * n.y));
+      nt = v3(0.0f, -n.z * iv, n.y * iv);
+    }
+    V3 nb = cross(n, nt);
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      uint32_t h1 = hash_u32(ao.seed, pix, 2 * j), h2 = hash_u32(ao.seed, pix, 2 * j + 1);
+      float u1 = (float)(h1 >> 8) * 5.9604644775390625e-08f;
+      float u2 = (float)(h2 >> 8) * 5.9604644775390625e-08f;
+      float r = sqrtf(u1);
+      float sn, cs;
+      sincos_2pi(u2, sn, cs);
+      float lx = r * cs, ly = sqrtf(1.0f - u1), lz = r * sn;
+      V3 dir = {__fmaf_rn(lz, nt.x, __fmaf_rn(ly, n.x, lx * nb.x)),
+                __fmaf_rn(lz, nt.y, __fmaf_rn(ly, n.y, lx * nb.y)),
+                __fmaf_rn(lz, nt.z, __fmaf_rn(ly, n.z, lx * nb.z))};
+      size_t q = slot + 1 + j;
+      queue[2 * q] = make_float4(org.x, org.y, org.z, ao.ao_length);
+      queue[2 * q + 1] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(pix * 8u + 2u + j));
+    }
+  }
+  if (COUNT) flush_counts(c, rays, totals);
+}
+
+// Any-hit pass over the queued secondary rays; unoccluded rays set their
+// bit in the pixel mask.  The ray count is read on the device.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_ao_secondary(KdDev kd, const float4* __restrict__ queue,
+                                                      uint32_t* __restrict__ mask,
+                                                      uint32_t* __restrict__ counters,
+                                                      unsigned long long* __restrict__ totals) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t n = counters[1];
+  Counters c = {0, 0, 0, 0};
+  uint32_t rays = 0;
+  for (;;) {
+    uint32_t chunk = warp_fetch(&counters[2]);
+    if (chunk * 32 >= n) break;
+    uint32_t i = chunk * 32 + lane;
+    if (i >= n) continue;
+    float4 R0 = __ldg(&queue[2 * (size_t)i]), R1 = __ldg(&queue[2 * (size_t)i + 1]);
+    V3 o = {R0.x, R0.y, R0.z}, d = {R1.x, R1.y, R1.z};
+    HitState hs;
+    traverse<0, true, COUNT>(kd, snodes, o, d, R0.w, hs, c);
+    ++rays;
+    if (!COUNT && hs.id < 0) {
+      uint32_t tag = __float_as_uint(R1.w);
+      atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
+    }
+  }
+  if (COUNT) flush_counts(c, rays, totals + 4);
+}
+
+}  // namespace re
+
+// ------------------------------------------------------------------ host
+struct re_scene {
+  int device = 0;
+  re::FlatTree host;
+  uint2* d_nodes = nullptr;
+  float4* d_leaves = nullptr;
+  float4* d_tris = nullptr;
+  uint32_t* d_counters = nullptr;  // [0] tiles, [1] queue size, [2] queue chunks
+  float4* d_queue = nullptr;
+  size_t queue_cap = 0;  // rays
+  uint32_t max_visits = 16384;
+  uint32_t stage = 0;
+  int blocks_per_sm = 0;
+};
+
+namespace re {
+namespace {
+
+constexpr uint32_t kMaxStage = 8192;  // 64 KB of shared memory
+
+KdDev kd_view(const re_scene* s) {
+  KdDev kd;
+  kd.nodes = s->d_nodes;
+  kd.leaves = s->d_leaves;
+  kd.tris = s->d_tris;
+  kd.bmin = {s->host.bmin[0], s->host.bmin[1], s->host.bmin[2]};
+  kd.bmax = {s->host.bmax[0], s->host.bmax[1], s->host.bmax[2]};
+  kd.max_visits = s->max_visits;
+  kd.stage = s->stage;
+  return kd;
+}
+
+CamDev cam_view(const re_camera& c) {
+  CamBasis b;
+  camera_basis(c, b);
+  CamDev d;
+  d.campos = {b.campos[0], b.campos[1], b.campos[2]};
+  d.middle = {b.middle[0], b.middle[1], b.middle[2]};
+  d.horizontal = {b.horizontal[0], b.horizontal[1], b.horizontal[2]};
+  d.vertical = {b.vertical[0], b.vertical[1], b.vertical[2]};
+  d.focal = b.focal;
+  return d;
+}
+
+re_status check_scene(const re_scene* s, const char* fn) {
+  if (!s) return fail(RE_ERR_INVALID_ARG, "%s: null scene", fn);
+  if (s->device < 0) return fail(RE_ERR_NO_DEVICE, "%s: scene was built host-only", fn);
+  int dev = -1;
+  RE_CUDA(cudaGetDevice(&dev));
+  if (dev != s->device)
+    return fail(RE_ERR_INVALID_ARG, "%s: scene lives on device %d, current device is %d", fn,
+                s->device, dev);
+  return RE_OK;
+}
+
+template <typename K>
+int grid_for(K kernel, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return per_sm * sm_count();
+}
+
+re_status upload(re_scene* s) {
+  const FlatTree& h = s->host;
+  RE_CUDA(cudaMalloc(&s->d_nodes, h.nodes.size() * 4));
+  RE_CUDA(cudaMalloc(&s->d_leaves, h.leaves.size() * 4));
+  RE_CUDA(cudaMalloc(&s->d_tris, h.tris.size() * 4));
+  RE_CUDA(cudaMalloc(&s->d_counters, 64));
+  RE_CUDA(cudaMemcpy(s->d_nodes, h.nodes.data(), h.nodes.size() * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemcpy(s->d_leaves, h.leaves.data(), h.leaves.size() * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemcpy(s->d_tris, h.tris.data(), h.tris.size() * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemset(s->d_counters, 0, 64));
+  s->stage = std::min<uint32_t>(h.bfs_nodes, kMaxStage);
+  return RE_OK;
+}
+
+void release(re_scene* s) {
+  if (!s) return;
+  cudaFree(s->d_nodes);
+  cudaFree(s->d_leaves);
+  cudaFree(s->d_tris);
+  cudaFree(s->d_counters);
+  cudaFree(s->d_queue);
+  delete s;
+}
+
+re_status create_from_packed(const float* tris, uint32_t n, const re_kd_params* params,
+                             re_scene** out, bool host_only = false) {
+  re_kd_params p;
+  re_kd_params_default(&p);
+  if (params) p = *params;
+  if (p.leaf_size == 0 || p.max_depth == 0 || p.max_depth > 64)
+    return fail(RE_ERR_INVALID_ARG, "re_scene_create: bad kd params");
+  int dev = -1;
+  if (!host_only) RE_CUDA(cudaGetDevice(&dev));
+  re_scene* s = new (std::nothrow) re_scene();
+  if (!s) return fail(RE_ERR_OUT_OF_MEMORY, "re_scene_create: host allocation");
+  s->device = dev;
+  s->max_visits = p.max_leaf_visits ? p.max_leaf_visits : 16384;
+  const char* err = nullptr;
+  try {
+    if (!build_kdtree(tris, n, p, s->host, &err)) {
+      delete s;
+      return fail(RE_ERR_INVALID_ARG, "%s", err ? err : "kd build failed");
+    }
+  } catch (const std::bad_alloc&) {
+    delete s;
+    return fail(RE_ERR_OUT_OF_MEMORY, "re_scene_create: host allocation during build");
+  }
+  if (host_only) {
+    *out = s;
+    return RE_OK;
+  }
+  re_status st = upload(s);
+  if (st != RE_OK) {
+    release(s);
+    return st;
+  }
+  *out = s;
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API void re_kd_params_default(re_kd_params* p) {
+  if (!p) return;
+  p->max_depth = 24;
+  p->leaf_size = 8;
+  p->cost_traversal = 1.0f;
+  p->cost_intersect = 2.0f;
+  p->empty_bonus = 0.2f;
+  p->bfs_levels = 12;
+  p->threads = 0;
+  p->max_leaf_visits = 16384;
+}
+
+RE_API re_status re_scene_create(const float* verts, uint32_t num_verts, const uint32_t* faces,
+                                 uint32_t num_faces, const re_kd_params* params,
+                                 re_scene** out) {
+  if (!verts || !faces || !out || num_faces == 0 || num_verts == 0)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_create: null or empty mesh");
+  if (num_faces > (1u << 30)) return re::fail(RE_ERR_LIMIT, "re_scene_create: > 2^30 faces");
+  std::vector<float> packed;
+  try {
+    packed.resize(12 * (size_t)num_faces);
+  } catch (const std::bad_alloc&) {
+    return re::fail(RE_ERR_OUT_OF_MEMORY, "re_scene_create: host allocation");
+  }
+  // RTScene::init_triangles packing (RTScene.cpp:228-242)
+  for (uint32_t i = 0; i < num_faces; ++i) {
+    uint32_t a = faces[3 * (size_t)i], b = faces[3 * (size_t)i + 1], c = faces[3 * (size_t)i + 2];
+    if (a >= num_verts || b >= num_verts || c >= num_verts)
+      return re::fail(RE_ERR_INVALID_ARG, "re_scene_create: face %u indexes past the vertices", i);
+    float* P = &packed[12 * (size_t)i];
+    for (int k = 0; k < 3; ++k) {
+      float v0 = verts[3 * (size_t)a + k];
+      P[k] = v0;
+      P[4 + k] = verts[3 * (size_t)b + k] - v0;
+      P[8 + k] = verts[3 * (size_t)c + k] - v0;
+    }
+    P[3] = P[7] = P[11] = 0.f;
+  }
+  return re::create_from_packed(packed.data(), num_faces, params, out);
+}
+
+RE_API re_status re_scene_create_packed(const float* tris, uint32_t num_tris,
+                                        const re_kd_params* params, re_scene** out) {
+  if (!tris || !out || num_tris == 0)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_create_packed: null or empty input");
+  if (num_tris > (1u << 30)) return re::fail(RE_ERR_LIMIT, "re_scene_create_packed: > 2^30 tris");
+  return re::create_from_packed(tris, num_tris, params, out);
+}
+
+RE_API re_status re_scene_build_host(const float* tris, uint32_t num_tris,
+                                     const re_kd_params* params, re_scene** out) {
+  if (!tris || !out || num_tris == 0)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_build_host: null or empty input");
+  if (num_tris > (1u << 30)) return re::fail(RE_ERR_LIMIT, "re_scene_build_host: > 2^30 tris");
+  return re::create_from_packed(tris, num_tris, params, out, true);
+}
+
+RE_API re_status re_scene_stats_get(const re_scene* s, re_scene_stats* o) {
+  if (!s || !o) return re::fail(RE_ERR_INVALID_ARG, "re_scene_stats_get: null argument");
+  const re::FlatTree& h = s->host;
+  std::memset(o, 0, sizeof(*o));
+  o->num_tris = h.num_tris;
+  o->num_nodes = h.num_nodes;
+  o->num_leaves = h.num_leaves;
+  o->num_refs = h.num_refs;
+  o->max_depth = h.max_depth;
+  o->max_leaf_size = h.max_leaf_size;
+  o->bfs_nodes = h.bfs_nodes;
+  for (int k = 0; k < 3; ++k) {
+    o->bmin[k] = h.bmin[k];
+    o->bmax[k] = h.bmax[k];
+  }
+  o->build_seconds = h.build_seconds;
+  o->device_bytes = (h.nodes.size() + h.leaves.size() + h.tris.size()) * 4ull;
+  return RE_OK;
+}
+
+RE_API re_status re_scene_export(const re_scene* s, uint32_t* nodes, uint32_t* leaves,
+                                 float* tris) {
+  if (!s) return re::fail(RE_ERR_INVALID_ARG, "re_scene_export: null scene");
+  const re::FlatTree& h = s->host;
+  if (nodes) std::memcpy(nodes, h.nodes.data(), h.nodes.size() * 4);
+  if (leaves) std::memcpy(leaves, h.leaves.data(), h.leaves.size() * 4);
+  if (tris) std::memcpy(tris, h.tris.data(), h.tris.size() * 4);
+  return RE_OK;
+}
+
+RE_API re_status re_scene_destroy(re_scene* s) {
+  re::release(s);
+  return RE_OK;
+}
+
+RE_API re_status re_trace_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                  uint32_t flags, re_hit* d_out, void* stream) {
+  re_status st = re::check_scene(s, "re_trace_primary");
+  if (st != RE_OK) return st;
+  if (!cam || !d_out || w < 2 || h < 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_trace_primary: bad arguments");
+  if ((uint64_t)w * h > (1ull << 31)) return re::fail(RE_ERR_LIMIT, "re_trace_primary: image too large");
+  if (flags & ~1u) return re::fail(RE_ERR_INVALID_ARG, "re_trace_primary: unknown flags");
+  cudaStream_t st_ = (cudaStream_t)stream;
+  re::KdDev kd = re::kd_view(s);
+  re::CamDev cd = re::cam_view(*cam);
+  size_t smem = kd.stage * sizeof(uint2);
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
+  if (flags & RE_TRACE_ONE_SIDED) {
+    auto k = re::k_primary<1, false>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, d_out, nullptr, s->d_counters);
+  } else {
+    auto k = re::k_primary<0, false>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, d_out, nullptr, s->d_counters);
+  }
+  RE_CHECK_LAUNCH("re_trace_primary: launch");
+  return RE_OK;
+}
+
+RE_API re_status re_count_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                  uint32_t flags, uint32_t* d_counts, void* stream) {
+  re_status st = re::check_scene(s, "re_count_primary");
+  if (st != RE_OK) return st;
+  if (!cam || !d_counts || w < 2 || h < 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_count_primary: bad arguments");
+  if ((uint64_t)w * h > (1ull << 31)) return re::fail(RE_ERR_LIMIT, "re_count_primary: image too large");
+  if (flags & ~1u) return re::fail(RE_ERR_INVALID_ARG, "re_count_primary: unknown flags");
+  cudaStream_t st_ = (cudaStream_t)stream;
+  re::KdDev kd = re::kd_view(s);
+  re::CamDev cd = re::cam_view(*cam);
+  size_t smem = kd.stage * sizeof(uint2);
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
+  uint4* c4 = reinterpret_cast<uint4*>(d_counts);
+  if (flags & RE_TRACE_ONE_SIDED) {
+    auto k = re::k_primary<1, true>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, nullptr, c4, s->d_counters);
+  } else {
+    auto k = re::k_primary<0, true>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, nullptr, c4, s->d_counters);
+  }
+  RE_CHECK_LAUNCH("re_count_primary: launch");
+  return RE_OK;
+}
+
+RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n, uint32_t flags,
+                               re_hit* d_out, void* stream) {
+  re_status st = re::check_scene(s, "re_trace_rays");
+  if (st != RE_OK) return st;
+  if (!d_rays || !d_out) return re::fail(RE_ERR_INVALID_ARG, "re_trace_rays: null buffer");
+  if (n == 0) return RE_OK;
+  if (n > (1u << 31)) return re::fail(RE_ERR_LIMIT, "re_trace_rays: n > 2^31");
+  if (flags & ~3u) return re::fail(RE_ERR_INVALID_ARG, "re_trace_rays: unknown flags");
+  cudaStream_t st_ = (cudaStream_t)stream;
+  re::KdDev kd = re::kd_view(s);
+  size_t smem = kd.stage * sizeof(uint2);
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
+  const float4* r4 = reinterpret_cast<const float4*>(d_rays);
+#define RE_LAUNCH_RAYS(M, A)                                                                \
+  do {                                                                                      \
+    auto k = re::k_rays<M, A>;                                                              \
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, r4, n, d_out, s->d_counters);           \
+  } while (0)
+  switch (flags & 3u) {
+    case 0: RE_LAUNCH_RAYS(0, false); break;
+    case 1: RE_LAUNCH_RAYS(1, false); break;
+    case 2: RE_LAUNCH_RAYS(0, true); break;
+    default: RE_LAUNCH_RAYS(1, true); break;
+  }
+#undef RE_LAUNCH_RAYS
+  RE_CHECK_LAUNCH("re_trace_rays: launch");
+  return RE_OK;
+}
+
+}  // extern "C"
+
+namespace re {
+namespace {
+
+re_status ao_prepare(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                     const re_ao_params* p, const char* fn, cudaStream_t st, CamDev& cd,
+                     AoDev& ao) {
+  re_status rs = check_scene(s, fn);
+  if (rs != RE_OK) return rs;
+  if (!cam || !p || w < 2 || h < 2) return fail(RE_ERR_INVALID_ARG, "%s: bad arguments", fn);
+  if ((uint64_t)w * h > (1ull << 28)) return fail(RE_ERR_LIMIT, "%s: image > 2^28 pixels", fn);
+  size_t need = 5ull * w * h;
+  if (s->queue_cap < need) {
+    // The queue grows outside stream order: wait until no earlier frame on
+    // this stream still reads the old one.
+    RE_CUDA(cudaStreamSynchronize(st));
+    cudaFree(s->d_queue);
+    s->d_queue = nullptr;
+    s->queue_cap = 0;
+    RE_CUDA(cudaMalloc(&s->d_queue, need * 32));
+    s->queue_cap = need;
+  }
+  cd = cam_view(*cam);
+  ao.light = {p->light_dir[0], p->light_dir[1], p->light_dir[2]};
+  ao.ao_length = p->ao_length;
+  ao.bias = p->bias;
+  ao.seed = p->seed;
+  return RE_OK;
+}
+
+template <bool COUNT>
+re_status ao_primary(re_scene* s, const CamDev& cd, const AoDev& ao, uint32_t w, uint32_t h,
+                     re_hit* d_primary, uint32_t* d_mask, unsigned long long* totals,
+                     cudaStream_t st) {
+  KdDev kd = kd_view(s);
+  size_t smem = kd.stage * sizeof(uint2);
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 12, st));
+  auto k = k_ao_primary<COUNT>;
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask, s->d_queue,
+                                          s->d_counters, totals);
+  RE_CHECK_LAUNCH("ao primary launch");
+  return RE_OK;
+}
+
+template <bool COUNT>
+re_status ao_secondary(re_scene* s, uint32_t* d_mask, unsigned long long* totals,
+                       cudaStream_t st) {
+  KdDev kd = kd_view(s);
+  size_t smem = kd.stage * sizeof(uint2);
+  auto k = k_ao_secondary<COUNT>;
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, s->d_queue, d_mask, s->d_counters, totals);
+  RE_CHECK_LAUNCH("ao secondary launch");
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API re_status re_render_ao_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                      const re_ao_params* p, re_hit* d_primary,
+                                      uint32_t* d_mask, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  re::CamDev cd;
+  re::AoDev ao;
+  re_status rs = re::ao_prepare(s, cam, w, h, p, "re_render_ao_primary", st, cd, ao);
+  if (rs != RE_OK) return rs;
+  if (!d_primary || !d_mask) return re::fail(RE_ERR_INVALID_ARG, "re_render_ao_primary: null output");
+  return re::ao_primary<false>(s, cd, ao, w, h, d_primary, d_mask, nullptr, st);
+}
+
+RE_API re_status re_render_ao_secondary(re_scene* s, uint32_t* d_mask, uint32_t* d_num_secondary,
+                                        void* stream) {
+  re_status rs = re::check_scene(s, "re_render_ao_secondary");
+  if (rs != RE_OK) return rs;
+  if (!d_mask) return re::fail(RE_ERR_INVALID_ARG, "re_render_ao_secondary: null mask");
+  if (!s->d_queue) return re::fail(RE_ERR_INVALID_ARG, "re_render_ao_secondary: no primary pass ran");
+  cudaStream_t st = (cudaStream_t)stream;
+  rs = re::ao_secondary<false>(s, d_mask, nullptr, st);
+  if (rs != RE_OK) return rs;
+  if (d_num_secondary)
+    RE_CUDA(cudaMemcpyAsync(d_num_secondary, s->d_counters + 1, 4, cudaMemcpyDeviceToDevice, st));
+  return RE_OK;
+}
+
+RE_API re_status re_render_ao(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                              const re_ao_params* p, re_hit* d_primary, uint32_t* d_mask,
+                              uint32_t* d_num_secondary, void* stream) {
+  re_status rs = re_render_ao_primary(s, cam, w, h, p, d_primary, d_mask, stream);
+  if (rs != RE_OK) return rs;
+  return re_render_ao_secondary(s, d_mask, d_num_secondary, stream);
+}
+
+RE_API re_status re_render_ao_counts(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                     const re_ao_params* p, uint64_t* d_totals, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  re::CamDev cd;
+  re::AoDev ao;
+  re_status rs = re::ao_prepare(s, cam, w, h, p, "re_render_ao_counts", st, cd, ao);
+  if (rs != RE_OK) return rs;
+  if (!d_totals) return re::fail(RE_ERR_INVALID_ARG, "re_render_ao_counts: null totals");
+  unsigned long long* t = reinterpret_cast<unsigned long long*>(d_totals);
+  RE_CUDA(cudaMemsetAsync(t, 0, 8 * sizeof(uint64_t), st));
+  rs = re::ao_primary<true>(s, cd, ao, w, h, nullptr, nullptr, t, st);
+  if (rs != RE_OK) return rs;
+  return re::ao_secondary<true>(s, nullptr, t, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,246 @@
+"""GPU parity: every kernel, called through the C ABI, against the CPU oracle
+on the same seeded inputs.
+
+Bar: bit-exact for hit ids, t, u, v, masks, heights, noise values, SDF
+positions, normals and step counts (the kernels and the oracle share one
+rounding policy).  Against the reference as shipped (brute force over one
+leaf), hit ids must match except where the FP64 edge margin of either
+triangle is below 1e-6 (counted), and t/u/v within 1e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+import rayengine_b200 as rb
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+MARGIN = 1e-6
+REL_TOL = 1e-5
+
+
+def _kd(sc):
+    st = sc.stats()
+    nodes, leaves, tris = sc.export()
+    return st, po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+
+
+def _hits(t):
+    return t.cpu().numpy().reshape(-1, 4)
+
+
+def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels):
+    """Reference-as-shipped comparison with the FP64 edge-margin exemption."""
+    bf = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, w, h, pixels=pixels)
+    g = got[pixels].view(np.int32).reshape(-1, 4)
+    gid, bid = g[:, 0], bf["id"]
+    diff = np.nonzero(gid != bid)[0]
+    exempt = 0
+    if diff.size:
+        o, d = po.camera_rays(cam, w, h, pixels[diff])
+        m = np.full(diff.size, np.inf)
+        for ids in (gid[diff], bid[diff]):
+            ok = ids >= 0
+            m[ok] = np.minimum(m[ok], po.edge_margin(packed, ids[ok], o[ok], d[ok]))
+        assert np.all(m < MARGIN), f"{int((m >= MARGIN).sum())} id mismatches outside the edge margin"
+        exempt = diff.size
+    same = (gid == bid) & (bid >= 0)
+    gf = g[same, 1:].view(np.float32)
+    bfv = np.stack([bf["t"], bf["u"], bf["v"]], 1)[same]
+    rel = np.abs(gf - bfv) / np.maximum(np.abs(bfv), 1e-3)
+    assert rel.max(initial=0) <= REL_TOL
+    return exempt, int((bid >= 0).sum())
+
+
+def test_soup_small_bitexact(cuda):
+    cfg = rb.configs.SoupConfig(num_tris=4096, width=128, height=128)
+    packed = cfg.packed()
+    cam = cfg.camera()
+    with rb.KDScene.from_packed(packed) as sc:
+        st, kd = _kd(sc)
+        for mode in (rb.TRACE_TWO_SIDED, rb.TRACE_ONE_SIDED):
+            got = _hits(sc.trace_primary(cam, 128, 128, mode))
+            ref = po.primary_kd(kd, cam, 128, 128, mode=mode)
+            assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4)), mode
+            pix = np.arange(128 * 128, dtype=np.uint32)
+            exempt, nhit = _assert_vs_bruteforce(got, packed, st, cam, 128, 128, pix)
+            assert nhit > 1000
+
+
+def test_golden_reference_scenes(cuda):
+    """The committed fixtures of the reference's own build + traversal."""
+    import os
+
+    for name in ("ref_soup.npz", "ref_grid.npz"):
+        g = np.load(os.path.join(os.path.dirname(__file__), "golden", name))
+        cam = rb.build_camera(g["campos"], (0, 0, 0), g["fov"])
+        cam.view[:] = [float(x) for x in g["view"]]
+        w, h = int(g["w"]), int(g["h"])
+        with rb.KDScene.from_mesh(g["verts"], g["faces"]) as sc:
+            got = _hits(sc.trace_primary(cam, w, h))
+        gid, rid = got[:, 0], g["hits"][:, 0]
+        diff = np.nonzero(gid != rid)[0]
+        if diff.size:
+            packed = rb.pack_triangles(g["verts"], g["faces"])
+            o, d = po.camera_rays(cam, w, h, diff)
+            m = np.full(diff.size, np.inf)
+            for ids in (gid[diff], rid[diff]):
+                ok = ids >= 0
+                m[ok] = np.minimum(m[ok], po.edge_margin(packed, ids[ok], o[ok], d[ok]))
+            assert np.all(m < MARGIN), name
+        same = (gid == rid) & (rid >= 0)
+        assert np.array_equal(got[same], g["hits"][same]), name
+
+
+def test_soup_config0_full(cuda):
+    """65,536 triangles, 512x512: bit-exact against the oracle's traversal of
+    the same tree on every ray; against brute force on a ray sample."""
+    cfg = rb.configs.SoupConfig()
+    packed = cfg.packed()
+    cam = cfg.camera()
+    with rb.KDScene.from_packed(packed) as sc:
+        st, kd = _kd(sc)
+        got = _hits(sc.trace_primary(cam, 512, 512))
+        cnt = sc.count_primary(cam, 512, 512).cpu().numpy()
+    ref, rc = po.primary_kd(kd, cam, 512, 512, counts=True)
+    assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4))
+    assert np.array_equal(cnt, rc.view(np.uint32).reshape(-1, 4).astype(np.int32))
+    pix = np.random.default_rng(3).choice(512 * 512, 3000, replace=False).astype(np.uint32)
+    _assert_vs_bruteforce(got, packed, st, cam, 512, 512, pix)
+
+
+def test_caller_rays_closest_and_anyhit(cuda):
+    cfg = rb.configs.SoupConfig(num_tris=20000)
+    packed = cfg.packed()
+    rng = np.random.default_rng(4)
+    n = 50000
+    o = rng.uniform(-1.5, 1.5, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d[: n // 10, 1:] = 0.0  # axis-parallel rays (zero direction components)
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    tmax = rng.choice([np.inf, 0.5, 1e20], n).astype(np.float32)
+    rays = np.concatenate([o, tmax[:, None], d, np.zeros((n, 1), np.float32)], 1)
+    with rb.KDScene.from_packed(packed) as sc:
+        st, kd = _kd(sc)
+        dr = torch.from_numpy(rays).cuda()
+        for flags in (0, 1, 2, 3):
+            got = _hits(sc.trace_rays(dr, flags))
+            ref = po.rays_kd(kd, rays, mode=flags & 1, anyhit=bool(flags & 2))
+            if flags & 2:
+                # any-hit: occlusion must agree; the reported triangle may differ
+                assert np.array_equal(got[:, 0] >= 0, ref["id"] >= 0)
+            else:
+                assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4))
+
+
+def test_heightfield_kernel_bitexact(cuda):
+    cfg = rb.configs.HeightfieldConfig()
+    P = po.perm(cfg.seed)
+    for cells in (7, 256, 1024):
+        v = rb.heightfield(cfg.fbm(), cells, cfg.lo, cfg.hi).cpu().numpy()
+        ov, of = po.heightfield(P, cells, cfg.lo, cfg.hi, cfg.octaves, cfg.amplitude)
+        assert np.array_equal(v, ov), cells
+        assert np.array_equal(rb.grid_faces(cells), of)
+
+
+def test_fbm_kernel_bitexact(cuda):
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "noise.npz"))
+    pts = torch.from_numpy(g["pts"]).cuda()
+    for o in (1, 6, 8):
+        got = rb.generate_noise(rb.fbm_params(seed=2016, octaves=o), pts).cpu().numpy()
+        assert np.array_equal(got, g[f"fbm{o}"]), o
+    rng = np.random.default_rng(5)
+    big = rng.uniform(-1000, 1000, (1 << 20, 3)).astype(np.float32)
+    got = rb.generate_noise(rb.fbm_params(seed=7, octaves=8, scale=0.25, amplitude=3.0),
+                            torch.from_numpy(big).cuda()).cpu().numpy()
+    assert np.array_equal(got, po.fbm_batch(po.perm(7), big, 8, scale=0.25, amp=3.0))
+
+
+def test_render_ao_small_bitexact(cuda):
+    cfg = rb.configs.HeightfieldConfig(cells=128, width=320, height=180)
+    P = po.perm(cfg.seed)
+    verts, faces = po.heightfield(P, cfg.cells, cfg.lo, cfg.hi, cfg.octaves, cfg.amplitude)
+    packed = rb.pack_triangles(verts, faces)
+    cam = cfg.camera()
+    light = rb.unit(cfg.light_dir)
+    with rb.KDScene.from_mesh(verts, faces) as sc:
+        st, kd = _kd(sc)
+        hits, mask, nsec = sc.render_ao(cam, cfg.width, cfg.height, light, cfg.ao_length,
+                                        cfg.bias, cfg.ao_seed)
+        hits, mask, nsec = _hits(hits), mask.cpu().numpy(), int(nsec.item())
+    rh, rm, rn = po.frame_ao(kd, packed, cam, cfg.width, cfg.height, light, cfg.ao_length,
+                             cfg.bias, cfg.ao_seed)
+    assert np.array_equal(hits, rh.view(np.int32).reshape(-1, 4))
+    assert np.array_equal(mask.view(np.uint32), rm)
+    assert nsec == rn == 5 * int((rh["id"] >= 0).sum())
+    # the AO and shadow bits are not trivially all-set or all-clear
+    hit = (rm & 1) == 1
+    assert 0.05 < ((rm[hit] >> 1) & 1).mean() < 0.98
+    assert 0.05 < ((rm[hit] >> 2) & 15).astype(bool).mean() <= 1.0
+
+
+def test_render_ao_config1_sampled(cuda):
+    """Full 2.1M-triangle heightfield at 1920x1080: heights from the GPU,
+    bit-exact hits/masks on a pixel sample, size-independent checks on all."""
+    cfg = rb.configs.HeightfieldConfig()
+    verts, faces = cfg.mesh_on_device()
+    packed = rb.pack_triangles(verts, faces)
+    cam = cfg.camera()
+    light = rb.unit(cfg.light_dir)
+    W, H = cfg.width, cfg.height
+    with rb.KDScene.from_mesh(verts, faces) as sc:
+        st, kd = _kd(sc)
+        hits, mask, nsec = sc.render_ao(cam, W, H, light, cfg.ao_length, cfg.bias, cfg.ao_seed)
+        hits2, mask2, _ = sc.render_ao(cam, W, H, light, cfg.ao_length, cfg.bias, cfg.ao_seed)
+        hits, mask, nsec = _hits(hits), mask.cpu().numpy().view(np.uint32), int(nsec.item())
+        prim = _hits(sc.trace_primary(cam, W, H))
+    # deterministic frame to frame, and the AO frame's primary pass equals the plain one
+    assert np.array_equal(hits, _hits(hits2)) and np.array_equal(mask, mask2.cpu().numpy().view(np.uint32))
+    assert np.array_equal(hits, prim)
+    assert nsec == 5 * int((hits[:, 0] >= 0).sum())
+    assert np.array_equal(mask & 1, (hits[:, 0] >= 0).astype(np.uint32))
+    pix = np.random.default_rng(6).choice(W * H, 4000, replace=False).astype(np.uint32)
+    rh, rm, _ = po.frame_ao(kd, packed, cam, W, H, light, cfg.ao_length, cfg.bias, cfg.ao_seed,
+                            pixels=pix)
+    assert np.array_equal(hits[pix], rh.view(np.int32).reshape(-1, 4))
+    assert np.array_equal(mask[pix], rm)
+    _assert_vs_bruteforce(hits, packed, st, cam, W, H, pix[:300])
+
+
+def test_sdf_small_bitexact(cuda):
+    tc = rb.configs.TerrainConfig(width=96, height=54)
+    out = rb.sphere_trace(tc.params(), tc.camera(), tc.width, tc.height).cpu().numpy()
+    ref = po.sdf_image(po.perm(tc.seed), tc.camera(), tc.width, tc.height)
+    f = out.view(np.float32)
+    assert np.array_equal(out[:, 7].view(np.uint32), ref["status"])
+    assert np.array_equal(out[:, 6].view(np.uint32), ref["steps"])
+    hit = ref["status"] == 1
+    assert hit.sum() > 1000
+    assert np.array_equal(f[hit, 0:3], ref["pos"][hit])
+    assert np.array_equal(f[hit, 3:6], ref["normal"][hit])
+
+
+def test_sdf_config2_sampled(cuda):
+    tc = rb.configs.TerrainConfig()
+    W, H = tc.width, tc.height
+    out = rb.sphere_trace(tc.params(), tc.camera(), W, H).cpu().numpy()
+    pix = np.random.default_rng(8).choice(W * H, 3000, replace=False).astype(np.uint32)
+    ref = po.sdf_image(po.perm(tc.seed), tc.camera(), W, H, pixels=pix)
+    assert np.array_equal(out[pix, 7].view(np.uint32), ref["status"])
+    assert np.array_equal(out[pix, 6].view(np.uint32), ref["steps"])
+    f = out.view(np.float32)
+    hit = ref["status"] == 1
+    assert np.array_equal(f[pix][hit, 0:6], np.concatenate([ref["pos"], ref["normal"]], 1)[hit])
+    # whole image: hits lie on the surface and normals are unit length
+    st = out[:, 7].view(np.uint32)
+    allhit = st == 1
+    P = po.perm(tc.seed)
+    pos = f[allhit, 0:3]
+    dens = pos[:, 1] - 3.0 * po.fbm_batch(P, pos, 8, scale=0.25)
+    assert np.all(dens < 1e-4)
+    nrm = np.linalg.norm(f[allhit, 3:6], axis=1)
+    assert np.all(np.abs(nrm - 1) < 1e-5)
+    assert allhit.mean() > 0.3

@@ -1,0 +1,189 @@
+"""Host SAH kd-tree builder: structural invariants, ropes, and the oracle's
+rope traversal over the built tree against brute force (the reference as
+shipped)."""
+import numpy as np
+import pytest
+
+import rayengine_b200 as rb
+from oracle import pyoracle as po
+
+
+def build(packed, **kw):
+    sc = rb.KDScene.build_host(packed, rb.kd_params(**kw) if kw else None)
+    st = sc.stats()
+    nodes, leaves, tris = sc.export()
+    sc.close()
+    return st, nodes, leaves, tris
+
+
+def region_boxes(st, nodes, leaves):
+    """Walk the node array from the root, returning each node's region box."""
+    boxes = {0: (np.array(st["bmin"], np.float32), np.array(st["bmax"], np.float32))}
+    depth = {0: 0}
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        split, meta = nodes[i]
+        if meta & 3 == 3:
+            continue
+        k = meta & 3
+        s = np.array([split], np.uint32).view(np.float32)[0]
+        lo, hi = boxes[i]
+        c = meta >> 2
+        lhi = hi.copy(); lhi[k] = s
+        rlo = lo.copy(); rlo[k] = s
+        boxes[c] = (lo, lhi)
+        boxes[c + 1] = (rlo, hi)
+        depth[c] = depth[c + 1] = depth[i] + 1
+        stack += [c, c + 1]
+    return boxes, depth
+
+
+@pytest.fixture(scope="module")
+def soup():
+    packed = rb.configs.SoupConfig(num_tris=20000, seed=5).packed()
+    return packed, build(packed)
+
+
+def test_tree_invariants(soup):
+    packed, (st, nodes, leaves, tris) = soup
+    assert st["num_tris"] == 20000 and st["max_depth"] <= 24
+    boxes, depth = region_boxes(st, nodes, leaves)
+    assert len(boxes) == st["num_nodes"]
+    leaf_nodes = [i for i in range(st["num_nodes"]) if nodes[i, 1] & 3 == 3]
+    assert len(leaf_nodes) == st["num_leaves"]
+    lf = leaves.view(np.float32)
+    for i in leaf_nodes:
+        L = nodes[i, 1] >> 2
+        lo, hi = boxes[i]
+        assert np.array_equal(lf[L, 0:3], lo) and np.array_equal(lf[L, 3:6], hi)
+        count = leaves[L, 7]
+        assert count <= 8 or depth[i] == 24
+        assert leaves[L, 14] == depth[i]
+    # every triangle referenced at least once; ids carried in v0.w
+    ids = tris[:, 3].view(np.int32)
+    assert np.array_equal(np.unique(ids), np.arange(20000))
+    # leaf ranges tile the reference array
+    firsts = leaves[:, 6].astype(np.int64)
+    counts = leaves[:, 7].astype(np.int64)
+    order = np.argsort(firsts)
+    assert firsts[order[0]] == 0
+    assert np.all(firsts[order[1:]] == (firsts + counts)[order[:-1]])
+    assert (firsts + counts).max() == st["num_refs"]
+    # triangle payload is copied verbatim from the packed input
+    assert np.array_equal(tris[:, [0, 1, 2, 4, 5, 6, 8, 9, 10]], packed[ids][:, [0, 1, 2, 4, 5, 6, 8, 9, 10]])
+
+
+def test_ropes_point_at_face_neighbours(soup):
+    packed, (st, nodes, leaves, tris) = soup
+    boxes, _ = region_boxes(st, nodes, leaves)
+    leaf_nodes = [i for i in range(st["num_nodes"]) if nodes[i, 1] & 3 == 3]
+    rope = leaves[:, 8:14].view(np.int32)
+    rng = np.random.default_rng(0)
+    for i in rng.choice(leaf_nodes, 400, replace=False):
+        L = nodes[i, 1] >> 2
+        lo, hi = boxes[i]
+        for f in range(6):
+            k, pos = f >> 1, f & 1
+            r = rope[L, f]
+            face = hi[k] if pos else lo[k]
+            if r < 0:
+                assert face == (st["bmax"][k] if pos else st["bmin"][k])
+                continue
+            nlo, nhi = boxes[int(r)]
+            # the target region is adjacent across the face and contains it
+            assert (nlo[k] == face) if pos else (nhi[k] == face)
+            for kk in range(3):
+                if kk != k:
+                    assert nlo[kk] <= lo[kk] and nhi[kk] >= hi[kk]
+
+
+def _compare_with_bruteforce(packed, st, nodes, leaves, tris, cam, w, h, npix=1500, mode=0):
+    kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+    rng = np.random.default_rng(1)
+    pix = rng.choice(w * h, min(npix, w * h), replace=False).astype(np.uint32)
+    hk = po.primary_kd(kd, cam, w, h, mode=mode, pixels=pix)
+    hb = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, w, h, mode=mode, pixels=pix)
+    return hk, hb
+
+
+def test_rope_traversal_equals_bruteforce_soup(soup):
+    packed, (st, nodes, leaves, tris) = soup
+    cam = rb.build_camera((0, 0, 3), (0, 0, 0), (60, 60))
+    for mode in (0, 1):
+        hk, hb = _compare_with_bruteforce(packed, st, nodes, leaves, tris, cam, 256, 256, mode=mode)
+        assert (hb["id"] >= 0).sum() > 300
+        assert np.array_equal(hk.view(np.int32), hb.view(np.int32))
+
+
+def test_rope_traversal_equals_bruteforce_heightfield():
+    P = po.perm(2016)
+    verts, faces = po.heightfield(P, 64, -4.0, 4.0, 6, 1.0)
+    packed = rb.pack_triangles(verts, faces)
+    st, nodes, leaves, tris = build(packed)
+    cam = rb.build_camera((0.3, 3.0, -6.0), (0, 0, 0), (60, 40))
+    hk, hb = _compare_with_bruteforce(packed, st, nodes, leaves, tris, cam, 320, 180)
+    assert (hb["id"] >= 0).mean() > 0.5
+    assert np.array_equal(hk.view(np.int32), hb.view(np.int32))
+
+
+@pytest.mark.parametrize("case", ["coplanar", "duplicates", "axis_rays", "single", "slivers"])
+def test_edge_cases(case):
+    rng = np.random.default_rng(2)
+    if case == "coplanar":
+        # half of the triangles lie in the plane z = 0 (planar split events);
+        # the rest give the scene box thickness (a box of zero thickness is
+        # never entered: the reference loop needs t_entry < t_exit)
+        flat = rng.uniform(-1, 1, (1500, 3, 3)).astype(np.float32) * np.float32(0.1) \
+            + rng.uniform(-1, 1, (1500, 1, 3)).astype(np.float32)
+        flat[:, :, 2] = 0.0
+        solid = rng.uniform(-1, 1, (1500, 1, 3)).astype(np.float32) \
+            + rng.normal(0, 0.05, (1500, 3, 3)).astype(np.float32)
+        v = np.concatenate([flat, solid])
+    elif case == "duplicates":
+        base = rng.uniform(-1, 1, (500, 1, 3)).astype(np.float32) + rng.normal(0, 0.05, (500, 3, 3)).astype(np.float32)
+        v = np.concatenate([base, base, base])  # exact ties: lowest id must win
+    elif case == "single":
+        v = np.array([[[-1, -1, 0], [1, -1, 0], [0, 1, 0]]], np.float32)
+    elif case == "slivers":
+        c = rng.uniform(-1, 1, (2000, 1, 3)).astype(np.float32)
+        v = c + rng.normal(0, 0.05, (2000, 3, 3)).astype(np.float32) * np.float32([1, 1e-4, 1])
+    else:
+        v = rng.uniform(-1, 1, (1, 1, 3)).astype(np.float32) + rng.normal(0, 0.05, (4000, 3, 3)).astype(np.float32) * 8
+    packed = np.zeros((v.shape[0], 12), np.float32)
+    packed[:, 0:3] = v[:, 0]
+    packed[:, 4:7] = v[:, 1] - v[:, 0]
+    packed[:, 8:11] = v[:, 2] - v[:, 0]
+    st, nodes, leaves, tris = build(packed)
+    kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+    if case == "axis_rays":
+        # rays parallel to the axes (zero direction components) from random origins
+        o = rng.uniform(-1.5, 1.5, (3000, 3)).astype(np.float32)
+        d = np.zeros((3000, 3), np.float32)
+        d[np.arange(3000), rng.integers(0, 3, 3000)] = rng.choice([-1.0, 1.0], 3000)
+        rays = np.concatenate([o, np.full((3000, 1), np.inf, np.float32), d, np.zeros((3000, 1), np.float32)], 1)
+        hk = po.rays_kd(kd, rays)
+        for i in range(0, 3000, 7):
+            one = po.primary_bruteforce  # noqa: F841
+        # brute force over caller rays via a single-leaf tree
+        st1, n1, l1, t1 = build(packed, leaf_size=1 << 30)
+        kd1 = po.KdTree(n1, l1, t1, st1["bmin"], st1["bmax"])
+        assert st1["num_leaves"] == 1
+        hb = po.rays_kd(kd1, rays)
+        assert (hb["id"] >= 0).sum() > 100
+        assert np.array_equal(hk.view(np.int32), hb.view(np.int32))
+        return
+    cam = rb.build_camera((0.1, 0.2, 3), (0, 0, 0), (70, 70))
+    hk, hb = _compare_with_bruteforce(packed, st, nodes, leaves, tris, cam, 200, 200, npix=3000)
+    assert np.array_equal(hk.view(np.int32), hb.view(np.int32))
+    if case != "single":
+        assert (hb["id"] >= 0).sum() > 50
+
+
+def test_leaf_visit_cap_sets_status():
+    packed = rb.configs.SoupConfig(num_tris=20000).packed()
+    st, nodes, leaves, tris = build(packed)
+    kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+    cam = rb.build_camera((0, 0, 3), (0, 0, 0), (60, 60))
+    h, c = po.primary_kd(kd, cam, 64, 64, max_visits=2, counts=True)
+    assert c["status"].max() == 1 and c["leaf"].max() <= 2

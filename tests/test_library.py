@@ -1,0 +1,71 @@
+"""The C-ABI library loads, exports every declared entry point and validates
+arguments without touching a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rayengine_b200 as rb
+from rayengine_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "rayengine_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"RE_API\s+[\w\s\*]+?\b(re_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "re_trace_primary" in syms and "re_sdf_trace" in syms and len(syms) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each of them
+    assert set(declared_symbols()) <= set(_lib.EXPORTED), set(declared_symbols()) - set(_lib.EXPORTED)
+
+
+def test_abi_version_and_status_strings():
+    assert _lib.lib.re_abi_version() == 1
+    assert _lib.lib.re_status_string(0) == b"ok"
+    assert _lib.lib.re_status_string(4) == b"size limit exceeded"
+
+
+def test_argument_errors_are_reported_not_fatal():
+    with pytest.raises(rb.RayEngineError) as e:
+        _lib.call("re_scene_create", None, 0, None, 0, None, ctypes.byref(ctypes.c_void_p()))
+    assert e.value.status == 1 and "re_scene_create" in str(e.value)
+    with pytest.raises(rb.RayEngineError) as e:
+        _lib.call("re_gen_grid_faces", 100000, ctypes.c_void_p(1))
+    assert e.value.status == 4
+    with pytest.raises(rb.RayEngineError):
+        _lib.call("re_noise_fbm", None, None, 0, None, None)
+    p = rb.sdf_params(max_steps=0)
+    with pytest.raises(rb.RayEngineError) as e:
+        _lib.call("re_sdf_trace", ctypes.byref(p), ctypes.byref(rb.build_camera((0, 0, 1), (0, 0, 0))),
+                  4, 4, ctypes.c_void_p(16), None)
+    assert e.value.status in (1, 4)
+
+
+def test_bad_face_index_rejected():
+    verts = np.zeros((3, 3), np.float32)
+    faces = np.array([[0, 1, 5]], np.uint32)
+    with pytest.raises(rb.RayEngineError) as e:
+        rb.KDScene.from_mesh(verts, faces)
+    assert e.value.status == 1
+
+
+def test_host_only_scene_refuses_to_trace():
+    packed = rb.configs.SoupConfig(num_tris=64).packed()
+    sc = rb.KDScene.build_host(packed)
+    with pytest.raises(rb.RayEngineError) as e:
+        _lib.call("re_trace_primary", sc.handle, ctypes.byref(rb.build_camera((0, 0, 3), (0, 0, 0))),
+                  8, 8, 0, ctypes.c_void_p(16), None)
+    assert e.value.status == 5
+    sc.close()

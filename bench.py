@@ -35,7 +35,6 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-SCENE_CACHE = os.path.join(ROOT, "_build")
 
 
 # ------------------------------------------------------------- plumbing
@@ -189,8 +188,7 @@ class HeightfieldAO:
         ]
 
     def alg_bytes(self):
-        """Algorithmic bytes per launch of each kernel:
-        8 B per inner-node step, 36 B per leaf visit (32 B box+range, 4 B
+        """Algorithmic bytes per launch of each kernel: 8 B per inner-node step, 36 B per leaf visit (32 B box+range, 4 B
         rope), 48 B per triangle test, 16 B hit + 4 B mask per primary ray,
         32 B per queued secondary ray (written by the primary pass, read by
         the secondary pass)."""
@@ -246,32 +244,6 @@ class HeightfieldAO:
                           f"rays ({n + nsec} rays); oracle rope traversal over the same SAH tree, "
                           "OpenMP schedule(dynamic) over pixels"}
 
-    def reference_step_fn(self):
-        """The reference's own path on the host: RKDTreeCPU as shipped (one
-        leaf) from oracle/_ref when present, traced by the restated traversal,
-        i.e. brute-force MT over every triangle per ray."""
-        from oracle import pyoracle as po
-
-        packed = self.rb.pack_triangles(self.verts, self.faces)
-        W, H = self.cfg.width, self.cfg.height
-        built_by = "restated single-leaf build"
-        bmin, bmax = packed_bounds(self.verts, self.faces)
-        if po.ref_lib() is not None:
-            nodes, idx, root, _, _ = po.ref_build(self.verts, self.faces)
-            rn = po.ref_node_fields(nodes[root])
-            assert rn["is_leaf"] and np.array_equal(idx, np.arange(len(idx)))
-            bmin, bmax = rn["min"], rn["max"]
-            built_by = "reference RKDTreeCPU/RKDThreeGPU (oracle/_ref, one leaf)"
-        light = self.rb.unit(self.cfg.light_dir)
-        rng = np.random.default_rng(1)
-        return built_by, lambda npix: po.frame_ao_bruteforce(
-            packed, bmin, bmax, self.cam, W, H, light, self.cfg.ao_length, self.cfg.bias,
-            self.cfg.ao_seed, rng.choice(W * H, npix, replace=False).astype(np.uint32))
-
-
-def packed_bounds(verts, faces):
-    v = verts[faces.reshape(-1)]
-    return v.min(0), v.max(0)
 
 
 class SoupPrimary:
@@ -342,18 +314,6 @@ class SoupPrimary:
                 "kind": "port", "sample": f"{reps} full {W}x{H} frames; oracle rope traversal over "
                                           "the same SAH tree, OpenMP"}
 
-    def reference_step_fn(self):
-        from oracle import pyoracle as po
-
-        W, H = self.cfg.width, self.cfg.height
-        v = self.packed
-        verts = np.stack([v[:, 0:3], v[:, 0:3] + v[:, 4:7], v[:, 0:3] + v[:, 8:11]], 1).reshape(-1, 3)
-        bmin, bmax = verts.min(0), verts.max(0)
-        rng = np.random.default_rng(1)
-        return "restated single-leaf build", lambda npix: (
-            po.primary_bruteforce(self.packed, bmin, bmax, self.cam, W, H,
-                                  pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32)),
-            npix)[1]
 
 
 class TerrainSDF:
@@ -421,15 +381,68 @@ class TerrainSDF:
         return {"value": round(n / dt / 1e6, 4), "unit": "Mrays/s", "cores": po.threads(),
                 "kind": "port", "sample": f"{n} seeded-random pixels; oracle exact-SDF march, OpenMP"}
 
-    def reference_step_fn(self):
-        from oracle import pyoracle as po
 
-        W, H = self.cfg.width, self.cfg.height
-        P = po.perm(self.cfg.seed)
-        rng = np.random.default_rng(1)
-        return "restated exact-SDF march", lambda npix: (
-            po.sdf_image(P, self.cam, W, H,
-                         pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32)), npix)[1]
+
+# ---------------------------------------------------- the reference's path
+def reference_workload(name):
+    """(workload description, built-by note, step(npix) -> rays traced) for the
+    reference's own CPU path.  Scene inputs come from the CPU oracle's
+    generators (the same seeded values the kernels produce); nothing of this
+    repository's engine runs on this path."""
+    from oracle import pyoracle as po
+    import rayengine_b200.configs as C
+    from rayengine_b200 import api
+
+    rng = np.random.default_rng(1)
+    if name == "terrain_sdf":
+        cfg = C.TerrainConfig()
+        W, H = cfg.width, cfg.height
+        P = po.perm(cfg.seed)
+        cam = cfg.camera()
+
+        def step(npix):
+            po.sdf_image(P, cam, W, H, pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32))
+            return npix
+        return ("exact-SDF sphere tracing of d(p)=p.y-3fBm(0.25p), 8 octaves, 1920x1080",
+                "restated exact-SDF march (sphere_tracing.cuh:183-216)", step)
+    if name == "heightfield_ao":
+        cfg = C.HeightfieldConfig()
+        verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
+                                      cfg.amplitude)
+        desc = ("heightfield 1024x1024 cells (2,097,152 tris); 1920x1080 primary + 1 shadow + 4 AO "
+                "rays per hit")
+    else:
+        cfg = C.SoupConfig(num_tris=65536 if name == "soup" else 1 << 20)
+        tri = po.soup(cfg.seed, cfg.num_tris)
+        verts = tri.reshape(-1, 3)
+        faces = np.arange(verts.shape[0], dtype=np.uint32).reshape(-1, 3)
+        desc = f"triangle soup {cfg.num_tris} tris; {cfg.width}x{cfg.height} primary rays"
+    packed = api.pack_triangles(verts, faces)
+    v = verts[faces.reshape(-1)]
+    bmin, bmax = v.min(0), v.max(0)
+    built_by = "restated single-leaf build (RKDTreeCPU with MAX_DEPTH=1)"
+    if po.ref_lib() is not None:
+        nodes, idx, root, _, _ = po.ref_build(verts, faces)
+        rn = po.ref_node_fields(nodes[root])
+        assert rn["is_leaf"] and np.array_equal(idx, np.arange(len(idx)))
+        bmin, bmax = rn["min"], rn["max"]
+        built_by = "reference RKDTreeCPU/RKDThreeGPU compiled from its sources (one leaf)"
+    cam = cfg.camera()
+    W, H = cfg.width, cfg.height
+    if name == "heightfield_ao":
+        light = api.unit(cfg.light_dir)
+
+        def step(npix):
+            return po.frame_ao_bruteforce(packed, bmin, bmax, cam, W, H, light, cfg.ao_length,
+                                          cfg.bias, cfg.ao_seed,
+                                          rng.choice(W * H, npix, replace=False).astype(np.uint32))
+    else:
+        def step(npix):
+            po.primary_bruteforce(packed, bmin, bmax, cam, W, H,
+                                  pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32))
+            return npix
+    return desc, built_by + "; traversal restated from ray_functions.cuh:231-360, i.e. " \
+        "Moller-Trumbore over every triangle per ray", step
 
 
 WORKLOADS = {
@@ -448,17 +461,13 @@ def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return 0
-    import torch
-
-    torch.cuda.set_device(local)
-    wl = WORKLOADS[args.config](torch)
-    built_by, step = wl.reference_step_fn()
     from oracle import pyoracle as po
 
+    desc, built_by, step = reference_workload(args.config)
     # size one step to roughly one second of work on all host cores
     npix = 4
     t0 = time.perf_counter()
-    r = step(npix)
+    step(npix)
     dt = time.perf_counter() - t0
     npix = max(4, min(200000, int(npix * 1.0 / max(dt, 1e-4))))
     for _ in range(args.warmup):
@@ -473,14 +482,12 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": wl.config(),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": desc, "pixels_per_step": npix},
         "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": po.threads(),
                          "kind": "port",
                          "sample": f"{npix} seeded-random pixels per step ({rays // args.steps} "
-                                   f"rays with their shadow/AO rays); tree: {built_by}; "
-                                   "traversal restated from ray_functions.cuh:231-360, "
-                                   "i.e. Moller-Trumbore over every triangle per ray"},
+                                   f"rays per step); tree: {built_by}"},
         "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -514,6 +521,7 @@ def run_ours(args):
     cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     clocks = ClockSampler(cvd.split(",")[local] if cvd else str(local))
     clocks.start()
+    time.sleep(0.5)  # let nvidia-smi take its first samples before the timed region
     barrier(world)
     torch.cuda.synchronize()
     for k in range(args.steps):
@@ -586,8 +594,8 @@ def run_ours(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS), default="heightfield_ao")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -30,9 +30,9 @@ def _hits(t):
     return t.cpu().numpy().reshape(-1, 4)
 
 
-def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels):
+def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels, mode=0):
     """Reference-as-shipped comparison with the FP64 edge-margin exemption."""
-    bf = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, w, h, pixels=pixels)
+    bf = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, w, h, mode=mode, pixels=pixels)
     g = got[pixels].view(np.int32).reshape(-1, 4)
     gid, bid = g[:, 0], bf["id"]
     diff = np.nonzero(gid != bid)[0]
@@ -64,8 +64,8 @@ def test_soup_small_bitexact(cuda):
             ref = po.primary_kd(kd, cam, 128, 128, mode=mode)
             assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4)), mode
             pix = np.arange(128 * 128, dtype=np.uint32)
-            exempt, nhit = _assert_vs_bruteforce(got, packed, st, cam, 128, 128, pix)
-            assert nhit > 1000
+            exempt, nhit = _assert_vs_bruteforce(got, packed, st, cam, 128, 128, pix, mode)
+            assert nhit > (1000 if mode == 0 else 500)
 
 
 def test_golden_reference_scenes(cuda):
@@ -239,8 +239,9 @@ def test_sdf_config2_sampled(cuda):
     allhit = st == 1
     P = po.perm(tc.seed)
     pos = f[allhit, 0:3]
-    dens = pos[:, 1] - 3.0 * po.fbm_batch(P, pos, 8, scale=0.25)
-    assert np.all(dens < 1e-4)
+    # the kernel's density is fma(-3, fbm, y); 3*fbm is exact in float64
+    dens = pos[:, 1].astype(np.float64) - 3.0 * po.fbm_batch(P, pos, 8, scale=0.25).astype(np.float64)
+    assert np.all(dens < 1e-4 + 1e-9)
     nrm = np.linalg.norm(f[allhit, 3:6], axis=1)
     assert np.all(np.abs(nrm - 1) < 1e-5)
     assert allhit.mean() > 0.3

@@ -180,6 +180,32 @@ RE_API re_status re_render_ao_primary(re_scene* s, const re_camera* cam,
 RE_API re_status re_render_ao_secondary(re_scene* s, uint32_t* d_mask,
                                         uint32_t* d_num_secondary,
                                         void* stream);
+/* re_render_ao without any device allocation during the call.
+ *
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they render: an engine that reserves all device memory at
+ * start-up through its own pool, or a frame loop that cannot afford
+ * cudaMalloc's implicit synchronisation or an out-of-memory failure in the
+ * middle of a frame.  re_render_ao grows its secondary-ray queue with
+ * cudaMalloc on first use; this entry point instead keeps the queue in a
+ * fixed array inside the library (RE_NOALLOC_SCRATCH_BYTES on every GPU that
+ * loads the library, held until the process exits).  Inputs, outputs and the
+ * scene are the caller's, exactly as for re_render_ao, and the results are
+ * identical.
+ *   - w * h must not exceed RE_NOALLOC_MAX_PIXELS (5 secondary rays of 32
+ *     bytes per pixel); larger images return RE_ERR_LIMIT without launching.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *   - Every call on a device shares the one array: calls that overlap on the
+ *     GPU (other streams, other threads) race and must be serialised by the
+ *     caller. */
+#define RE_NOALLOC_MAX_PIXELS 419430u
+#define RE_NOALLOC_SCRATCH_BYTES (256u + 160u * RE_NOALLOC_MAX_PIXELS)
+RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam,
+                                      uint32_t w, uint32_t h,
+                                      const re_ao_params* p, re_hit* d_primary,
+                                      uint32_t* d_mask,
+                                      uint32_t* d_num_secondary, void* stream);
 /* Work counters of the same frame (device array of 8 uint64): primary
  * inner-node steps, leaf visits, triangle tests, rays; then the same four
  * for the secondary rays.  Used for the algorithmic bytes of each pass. */

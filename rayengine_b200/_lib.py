@@ -130,6 +130,7 @@ _SIGS = {
     "re_render_ao": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
     "re_render_ao_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P]),
     "re_render_ao_secondary": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_render_ao_noalloc": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
     "re_render_ao_counts": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P]),
     "re_perlin_permutation": (ctypes.c_int, [_U32, _P]),
     "re_noise_fbm": (ctypes.c_int, [ctypes.POINTER(re_fbm_params), _P, _U32, _P, _P]),

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "kd_build.hpp"
@@ -818,6 +819,101 @@ RE_API re_status re_render_ao_counts(re_scene* s, const re_camera* cam, uint32_t
   rs = re::ao_primary<true>(s, cd, ao, w, h, nullptr, nullptr, t, st);
   if (rs != RE_OK) return rs;
   return re::ao_secondary<true>(s, nullptr, t, st);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ allocation-free AO frame
+// Some callers cannot allocate device memory while they render: an engine
+// that reserves all device memory up front through its own pool, or a frame
+// loop that cannot afford cudaMalloc's implicit synchronisation or an
+// out-of-memory failure in the middle of a frame.  re_render_ao grows its
+// secondary-ray queue with cudaMalloc on first use; re_render_ao_noalloc
+// instead uses the fixed array below (held by every GPU that loads the
+// library, until the process exits).
+namespace re {
+namespace {
+
+constexpr size_t kNoAllocCounterBytes = 256;
+constexpr size_t kNoAllocQueueBytes = (size_t)5 * 32 * RE_NOALLOC_MAX_PIXELS;
+constexpr size_t kNoAllocScratchBytes = kNoAllocCounterBytes + kNoAllocQueueBytes;
+constexpr int kNoAllocMaxDevices = 64;
+
+// counters (tile cursor, queue size, queue cursor) followed by the queue
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the symbol's name is only a host-side handle; the address comes from
+// cudaGetSymbolAddress, looked up once per device with that device current.
+re_status noalloc_scratch(unsigned char** out) {
+  int dev = -1;
+  RE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(RE_ERR_LIMIT, "re_render_ao_noalloc: device ordinal %d >= %d", dev,
+                kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                      const re_ao_params* p, re_hit* d_primary, uint32_t* d_mask,
+                                      uint32_t* d_num_secondary, void* stream) {
+  re_status rs = re::check_scene(s, "re_render_ao_noalloc");
+  if (rs != RE_OK) return rs;
+  if (!cam || !p || !d_primary || !d_mask || w < 2 || h < 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_render_ao_noalloc: bad arguments");
+  if ((uint64_t)w * h > RE_NOALLOC_MAX_PIXELS)
+    return re::fail(RE_ERR_LIMIT,
+                    "re_render_ao_noalloc: %ux%u = %llu pixels exceeds the fixed scratch of %u "
+                    "pixels (5 secondary rays of 32 bytes each per pixel); use re_render_ao",
+                    w, h, (unsigned long long)w * h, (unsigned)RE_NOALLOC_MAX_PIXELS);
+  unsigned char* scratch = nullptr;
+  rs = re::noalloc_scratch(&scratch);
+  if (rs != RE_OK) return rs;
+  uint32_t* counters = reinterpret_cast<uint32_t*>(scratch);
+  float4* queue = reinterpret_cast<float4*>(scratch + re::kNoAllocCounterBytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  re::KdDev kd = re::kd_view(s);
+  re::CamDev cd = re::cam_view(*cam);
+  re::AoDev ao;
+  ao.light = {p->light_dir[0], p->light_dir[1], p->light_dir[2]};
+  ao.ao_length = p->ao_length;
+  ao.bias = p->bias;
+  ao.seed = p->seed;
+  size_t smem = kd.stage * sizeof(uint2);
+  // the array keeps the previous call's contents: the cursors must restart at zero
+  RE_CUDA(cudaMemsetAsync(counters, 0, 12, st));
+  {
+    auto k = re::k_ao_primary<false>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask, queue,
+                                                counters, nullptr);
+    RE_CHECK_LAUNCH("re_render_ao_noalloc: primary launch");
+  }
+  {
+    auto k = re::k_ao_secondary<false>;
+    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, queue, d_mask, counters, nullptr);
+    RE_CHECK_LAUNCH("re_render_ao_noalloc: secondary launch");
+  }
+  if (d_num_secondary)
+    RE_CUDA(cudaMemcpyAsync(d_num_secondary, counters + 1, 4, cudaMemcpyDeviceToDevice, st));
+  return RE_OK;
 }
 
 }  // extern "C"

@@ -166,6 +166,8 @@ class HeightfieldAO:
         self.counts = self.scene.render_ao_counts(self.cam, W, H, self.params)
         self.rays_per_step = self.counts["primary"]["rays"] + self.counts["secondary"]["rays"]
         self.kernels_per_step = 2
+        # set-up: the autotuner picks staging depth, queue layout and refill threshold
+        self.tuning = self.scene.autotune_ao(self.cam, W, H, self.params)
 
     def config(self):
         st = self.scene.stats()
@@ -177,6 +179,10 @@ class HeightfieldAO:
                 "kd_build_s": round(self.build_s, 3), "image": [c.width, c.height],
                 "rays_per_step": self.rays_per_step,
                 "secondary_rays_per_step": self.counts["secondary"]["rays"],
+                "work_per_ray": {
+                    k: {f: round(v[f] / max(1, v["rays"]), 2) for f in ("inner", "leaf", "tests")}
+                    for k, v in self.counts.items()},
+                "tuning": self.tuning,
                 "l2": "flushed between steps (256 MB write)"}
 
     def phases(self, stream):
@@ -511,6 +517,15 @@ def run_ours(args):
         for _, fn in phases:
             fn()
 
+    if args.profile:
+        # for ncu captures: one warm-up step, one flushed step, no timing
+        step()
+        flush.fill_(1)
+        step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": wl.name, "kernels_per_step": wl.kernels_per_step}))
+        return 0
+
     for i in range(args.warmup):
         flush.fill_(i & 0xFF)
         step()
@@ -599,6 +614,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS), default="heightfield_ao")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="one warm-up and one flushed step, untimed (for ncu captures)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

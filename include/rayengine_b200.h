@@ -93,6 +93,14 @@ typedef struct re_kd_params {
 
 typedef struct re_scene re_scene;
 
+/* Launch tuning of a scene (see re_autotune_ao). */
+typedef struct re_tuning {
+  uint32_t stage_nodes;      /* top nodes staged in shared memory per block (<= 8192) */
+  uint32_t queue_kind_major; /* secondary-ray queue: 0 pixel-major, 1 kind-major    */
+  uint32_t refill_min;       /* idle lanes before a warp claims new secondary rays, 1..32 */
+  uint32_t reserved;
+} re_tuning;
+
 typedef struct re_scene_stats {
   uint32_t num_tris, num_nodes, num_leaves, num_refs;
   uint32_t max_depth, max_leaf_size, bfs_nodes, pad;
@@ -206,6 +214,16 @@ RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam,
                                       const re_ao_params* p, re_hit* d_primary,
                                       uint32_t* d_mask,
                                       uint32_t* d_num_secondary, void* stream);
+/* Autotuner: times the AO frame for each combination of shared-memory
+ * staging depth, queue layout and refill threshold (one warm-up and three
+ * timed frames each, CUDA events on `stream`), keeps the fastest on the
+ * scene and returns it with its frame time.  Allocates temporary output
+ * buffers: call at set-up, not in a frame loop. */
+RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w,
+                                uint32_t h, const re_ao_params* p,
+                                re_tuning* best, float* best_ms, void* stream);
+RE_API re_status re_scene_get_tuning(const re_scene* s, re_tuning* out);
+RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t);
 /* Work counters of the same frame (device array of 8 uint64): primary
  * inner-node steps, leaf visits, triangle tests, rays; then the same four
  * for the secondary rays.  Used for the algorithmic bytes of each pass. */

@@ -154,10 +154,14 @@ static inline uint32_t fbits(float f) {
   return u;
 }
 
-void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
-                float tmax, int mode, int anyhit, uint32_t max_leaf_visits,
-                o_hit* out, o_counts* cnt) {
+/* start: leaf node to begin in when the origin lies in its region (secondary
+ * rays start in the leaf of their primary hit), else 0 = root.  out_leaf:
+ * node index of the leaf the best hit was found in. */
+void o_trace_kd_ex(const o_kdtree* kd, const float o[3], const float d[3], float tmax, int mode,
+                   int anyhit, uint32_t max_leaf_visits, uint32_t start, o_hit* out,
+                   o_counts* cnt, uint32_t* out_leaf) {
   o_counts c = {0, 0, 0, 0};
+  if (out_leaf) *out_leaf = 0;
   out->id = -1;
   out->t = K_INFINITY;
   out->u = 0.0f;
@@ -171,9 +175,18 @@ void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
   float best_t = fminf(t_root_exit, tmax);
   int32_t best_id = -1;
   float best_u = 0.0f, best_v = 0.0f;
-  uint32_t node = 0;
+  uint32_t node = 0, best_leaf = 0;
   uint32_t visits = 0;
   int done = 0;
+  if (start != 0) {
+    uint32_t meta = fbits(kd->nodes[2 * start + 1]);
+    if ((meta & 3u) == 3u) {
+      const float* L = kd->leaves + 16 * (size_t)(meta >> 2);
+      if (o[0] >= L[0] && o[0] <= L[3] && o[1] >= L[1] && o[1] <= L[4] && o[2] >= L[2] &&
+          o[2] <= L[5])
+        node = start;
+    }
+  }
   while (!done && t_entry < best_t) {
     uint32_t meta = fbits(kd->nodes[2 * node + 1]);
     while ((meta & 3u) != 3u) {
@@ -204,6 +217,7 @@ void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
           best_id = id;
           best_u = u;
           best_v = v;
+          best_leaf = node;
           if (anyhit) {
             done = 1;
             break;
@@ -248,8 +262,14 @@ void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
     out->t = best_t;
     out->u = best_u;
     out->v = best_v;
+    if (out_leaf) *out_leaf = best_leaf;
   }
   if (cnt) *cnt = c;
+}
+
+void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3], float tmax, int mode,
+                int anyhit, uint32_t max_leaf_visits, o_hit* out, o_counts* cnt) {
+  o_trace_kd_ex(kd, o, d, tmax, mode, anyhit, max_leaf_visits, 0, out, cnt, NULL);
 }
 
 /* ------------------------------------------------------------ Perlin/fBm */

@@ -81,6 +81,11 @@ typedef struct {
 void o_trace_kd(const o_kdtree* kd, const float o[3], const float d[3],
                 float tmax, int mode, int anyhit, uint32_t max_leaf_visits,
                 o_hit* out, o_counts* cnt);
+/* the same, starting in leaf node `start` when the origin lies in its region
+ * (0 = root), and reporting the node of the leaf holding the best hit */
+void o_trace_kd_ex(const o_kdtree* kd, const float o[3], const float d[3],
+                   float tmax, int mode, int anyhit, uint32_t max_leaf_visits,
+                   uint32_t start, o_hit* out, o_counts* cnt, uint32_t* out_leaf);
 
 /* --- Perlin / fBm (sdf_functions.cuh:26-135, PerlinNoise.h:16-52) ------ */
 void o_perlin_permutation(uint32_t seed, uint32_t perm[512]);

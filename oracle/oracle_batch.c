@@ -85,7 +85,8 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
     o_generate_ray(&b, w, h, p % w, p / w, o, d);
     o_hit hit;
     o_counts c;
-    o_trace_kd(kd, o, d, INFINITY, 0, 0, max_visits, &hit, &c);
+    uint32_t leaf = 0;
+    o_trace_kd_ex(kd, o, d, INFINITY, 0, 0, max_visits, 0, &hit, &c, &leaf);
     pi += c.inner_visits;
     pl += c.leaf_visits;
     pt += c.tri_tests;
@@ -113,7 +114,7 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
       for (int j = 0; j < 5; ++j) {
         o_hit sh;
         o_counts sc;
-        o_trace_kd(kd, so[j], sd[j], st[j], 0, 1, max_visits, &sh, &sc);
+        o_trace_kd_ex(kd, so[j], sd[j], st[j], 0, 1, max_visits, leaf, &sh, &sc, NULL);
         si += sc.inner_visits;
         sl += sc.leaf_visits;
         stt += sc.tri_tests;

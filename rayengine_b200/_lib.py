@@ -78,6 +78,15 @@ class re_scene_stats(ctypes.Structure):
     ]
 
 
+class re_tuning(ctypes.Structure):
+    _fields_ = [
+        ("stage_nodes", ctypes.c_uint32),
+        ("queue_kind_major", ctypes.c_uint32),
+        ("refill_min", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
 class re_ao_params(ctypes.Structure):
     _fields_ = [
         ("light_dir", ctypes.c_float * 3),
@@ -131,6 +140,9 @@ _SIGS = {
     "re_render_ao_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P]),
     "re_render_ao_secondary": (ctypes.c_int, [_P, _P, _P, _P]),
     "re_render_ao_noalloc": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
+    "re_autotune_ao": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), ctypes.POINTER(re_tuning), ctypes.POINTER(ctypes.c_float), _P]),
+    "re_scene_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_tuning)]),
+    "re_scene_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_tuning)]),
     "re_render_ao_counts": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P]),
     "re_perlin_permutation": (ctypes.c_int, [_U32, _P]),
     "re_noise_fbm": (ctypes.c_int, [ctypes.POINTER(re_fbm_params), _P, _U32, _P, _P]),

@@ -286,6 +286,25 @@ class KDScene:
         call("re_render_ao_secondary", self._h, _dptr(mask),
              _dptr(nsec) if nsec is not None else None, _stream_ptr(stream))
 
+    def tuning(self) -> dict:
+        t = _lib.re_tuning()
+        call("re_scene_get_tuning", self._h, ctypes.byref(t))
+        return {"stage_nodes": t.stage_nodes, "queue_kind_major": t.queue_kind_major,
+                "refill_min": t.refill_min}
+
+    def set_tuning(self, stage_nodes: int, queue_kind_major: int, refill_min: int) -> None:
+        t = _lib.re_tuning(stage_nodes, queue_kind_major, refill_min, 0)
+        call("re_scene_set_tuning", self._h, ctypes.byref(t))
+
+    def autotune_ao(self, cam: RCamera, w: int, h: int, params, stream=None) -> dict:
+        """Pick staging depth, queue layout and refill threshold by timing the frame."""
+        t = _lib.re_tuning()
+        ms = ctypes.c_float()
+        call("re_autotune_ao", self._h, ctypes.byref(cam), w, h, ctypes.byref(params),
+             ctypes.byref(t), ctypes.byref(ms), _stream_ptr(stream))
+        return {"stage_nodes": t.stage_nodes, "queue_kind_major": t.queue_kind_major,
+                "refill_min": t.refill_min, "frame_ms": round(ms.value, 4)}
+
     def render_ao_counts(self, cam: RCamera, w: int, h: int, params, stream=None) -> dict:
         """Traversal work of the AO frame (sums over all rays of each pass)."""
         import torch

@@ -10,10 +10,11 @@
 //   compute_terrain_normal                 RE/cuda-src/sdf_functions.cuh:535-546
 //
 // The permutation table travels as a 512-byte kernel parameter and is
-// expanded into shared memory by every block, so lattice lookups with
-// divergent indices hit shared memory instead of serialising on the
-// constant cache.  The march is FP32-ALU bound; persistent warps take 8x4
-// pixel tiles so sky rays (few steps) and grazing rays (hundreds) balance.
+// expanded into shared memory by every block (one copy per lane, so
+// lattice lookups with divergent indices never conflict on a bank).  The
+// march is FP32-ALU bound; it runs as a per-lane state machine with lane
+// refills so sky rays (few steps) and grazing rays (hundreds) keep the warps
+// full.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -27,8 +28,9 @@ __global__ void __launch_bounds__(256) k_fbm(PermTable perm, const float* __rest
                                              uint32_t n, float* __restrict__ out,
                                              uint32_t octaves, float lac, float gain,
                                              float scale, float amplitude) {
-  __shared__ uint32_t P[512];
-  load_perm(perm, P);
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float x = __ldg(&pts[3 * (size_t)i]), y = __ldg(&pts[3 * (size_t)i + 1]),
           z = __ldg(&pts[3 * (size_t)i + 2]);
@@ -40,8 +42,9 @@ __global__ void __launch_bounds__(256) k_heightfield(PermTable perm, uint32_t ce
                                                      float step, float* __restrict__ verts,
                                                      uint32_t octaves, float lac, float gain,
                                                      float scale, float amplitude) {
-  __shared__ uint32_t P[512];
-  load_perm(perm, P);
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
   uint32_t nv = cells + 1;
   uint32_t total = nv * nv;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
@@ -60,58 +63,103 @@ struct SdfDev {
   float scale, amp, step_factor, eps, tmax;
 };
 
+// Sphere tracing as a per-lane state machine with one field evaluation per
+// loop trip: phase 0 marches (t += step_factor * d), phases 1..6 evaluate
+// the central-difference taps of the normal at the hit.  Every trip runs the
+// same density code on all live lanes (a single call site keeps the loop in
+// the instruction cache), and when at least kSdfRefill lanes of a warp are
+// idle the warp claims new pixels with one atomic.  Pixel i of the claim
+// order is lane (i & 31) of 8x4 tile (i >> 5), so claims stay coherent.
+constexpr uint32_t kSdfRefill = 4;
+
 __global__ void __launch_bounds__(256) k_sdf(PermTable perm, SdfDev sp, CamDev cam, uint32_t w,
                                              uint32_t h, float4* __restrict__ out,
-                                             uint32_t* __restrict__ tile_counter) {
-  __shared__ uint32_t P[512];
-  load_perm(perm, P);
+                                             uint32_t* __restrict__ cursor) {
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
   uint32_t lane = threadIdx.x & 31u;
-  uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
+  uint32_t tiles_x = (w + 7) / 8;
+  uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
+  bool live = false, exhausted = false;
+  uint32_t pix = 0, steps = 0, phase = 0;
+  V3 o = {0, 0, 0}, d = {0, 0, 1}, p = {0, 0, 0};
+  float t = 0.f, delta = 0.f, nx = 0.f, ny = 0.f, nz = 0.f, plus = 0.f;
   for (;;) {
-    uint32_t tile = 0;
-    if (lane == 0) tile = atomicAdd(tile_counter, 1u);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile >= tiles) break;
-    uint32_t x = (tile % tiles_x) * 8 + (lane & 7u);
-    uint32_t y = (tile / tiles_x) * 4 + (lane >> 3);
-    if (x >= w || y >= h) continue;
-    V3 o, d;
-    generate_ray(cam, w, h, x, y, o, d);
-    float t = 0.0f;
-    V3 p = o;
-    uint32_t status = 2, steps = 0;
-    for (uint32_t s = 0; s < sp.max_steps; ++s) {
-      p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
-      float dist = terrain_density(P, p, sp.octaves, sp.scale, sp.amp);
-      steps = s + 1;
-      if (dist < sp.eps) {
-        status = 1;
-        break;
-      }
-      t = __fmaf_rn(sp.step_factor, dist, t);
-      if (t > sp.tmax) {
-        status = 0;
-        break;
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && (nidle >= kSdfRefill || nidle == 32u)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(cursor, nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= total) exhausted = true;
+      if (!live) {
+        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+        uint32_t tile = i >> 5, l = i & 31u;
+        uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
+        if (i < total && x < w && y < h) {
+          generate_ray(cam, w, h, x, y, o, d);
+          pix = y * w + x;
+          t = 0.f;
+          steps = 0;
+          phase = 0;
+          live = true;
+        }
       }
     }
-    float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (status == 1) {
-      float delta = 0.002f * t;
-      float nx = terrain_density(P, v3(p.x + delta, p.y, p.z), sp.octaves, sp.scale, sp.amp) -
-                 terrain_density(P, v3(p.x - delta, p.y, p.z), sp.octaves, sp.scale, sp.amp);
-      float ny = terrain_density(P, v3(p.x, p.y + delta, p.z), sp.octaves, sp.scale, sp.amp) -
-                 terrain_density(P, v3(p.x, p.y - delta, p.z), sp.octaves, sp.scale, sp.amp);
-      float nz = terrain_density(P, v3(p.x, p.y, p.z + delta), sp.octaves, sp.scale, sp.amp) -
-                 terrain_density(P, v3(p.x, p.y, p.z - delta), sp.octaves, sp.scale, sp.amp);
-      V3 n = normalize(v3(nx, ny, nz));
-      r0 = make_float4(p.x, p.y, p.z, n.x);
-      r1 = make_float4(n.y, n.z, __uint_as_float(steps), __uint_as_float(status));
+    if (__ballot_sync(0xFFFFFFFFu, live) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!live) continue;
+    V3 q;
+    if (phase == 0) {
+      q = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
     } else {
-      r1 = make_float4(0.f, 0.f, __uint_as_float(steps), __uint_as_float(status));
+      float sgn_delta = (phase & 1u) ? delta : -delta;
+      q = p;
+      if (phase <= 2) q.x = p.x + sgn_delta;
+      else if (phase <= 4) q.y = p.y + sgn_delta;
+      else q.z = p.z + sgn_delta;
     }
-    size_t pix = (size_t)y * w + x;
-    out[2 * pix] = r0;
-    out[2 * pix + 1] = r1;
+    float v = terrain_density(P, q, sp.octaves, sp.scale, sp.amp);
+    uint32_t status = 3;  // 3 = keep going
+    if (phase == 0) {
+      ++steps;
+      if (v < sp.eps) {
+        p = q;
+        delta = 0.002f * t;
+        phase = 1;
+      } else {
+        t = __fmaf_rn(sp.step_factor, v, t);
+        if (t > sp.tmax) status = 0;
+        else if (steps >= sp.max_steps) status = 2;
+      }
+    } else {
+      if (phase & 1u) {
+        plus = v;
+      } else {
+        float diff = plus - v;
+        if (phase == 2) nx = diff;
+        else if (phase == 4) ny = diff;
+        else nz = diff;
+      }
+      if (phase == 6) status = 1;
+      else ++phase;
+    }
+    if (status != 3) {
+      float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1;
+      if (status == 1) {
+        V3 n = normalize(v3(nx, ny, nz));
+        r0 = make_float4(p.x, p.y, p.z, n.x);
+        r1 = make_float4(n.y, n.z, __uint_as_float(steps), __uint_as_float(status));
+      } else {
+        r1 = make_float4(0.f, 0.f, __uint_as_float(steps), __uint_as_float(status));
+      }
+      out[2 * (size_t)pix] = r0;
+      out[2 * (size_t)pix + 1] = r1;
+      live = false;
+    }
   }
 }
 
@@ -130,7 +178,7 @@ int blocks_for(uint64_t n) {
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
-// Scratch counter for the SDF tile queue, one per device.
+// Claim cursor of the SDF kernel, one per device.
 uint32_t* sdf_counter() {
   static uint32_t* ptrs[64] = {nullptr};
   int dev = 0;
@@ -150,7 +198,9 @@ RE_API re_status re_noise_fbm(const re_fbm_params* p, const float* d_pts, uint32
   if (p->octaves > 32) return re::fail(RE_ERR_LIMIT, "re_noise_fbm: octaves > 32");
   if (n == 0) return RE_OK;
   re::PermTable t = re::make_perm(p->seed);
-  re::k_fbm<<<re::blocks_for(n), 256, 0, (cudaStream_t)stream>>>(
+  RE_CUDA(cudaFuncSetAttribute(re::k_fbm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kPermSmemBytes));
+  re::k_fbm<<<re::blocks_for(n), 256, re::kPermSmemBytes, (cudaStream_t)stream>>>(
       t, d_pts, n, d_out, p->octaves, p->lacunarity, p->gain, p->scale, p->amplitude);
   RE_CHECK_LAUNCH("re_noise_fbm: launch");
   return RE_OK;
@@ -165,7 +215,9 @@ RE_API re_status re_heightfield(const re_fbm_params* p, uint32_t cells, float lo
   re::PermTable t = re::make_perm(p->seed);
   float step = (hi - lo) / (float)cells;
   uint64_t total = (uint64_t)(cells + 1) * (cells + 1);
-  re::k_heightfield<<<re::blocks_for(total), 256, 0, (cudaStream_t)stream>>>(
+  RE_CUDA(cudaFuncSetAttribute(re::k_heightfield, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kPermSmemBytes));
+  re::k_heightfield<<<re::blocks_for(total), 256, re::kPermSmemBytes, (cudaStream_t)stream>>>(
       t, cells, lo, step, d_verts, p->octaves, p->lacunarity, p->gain, p->scale, p->amplitude);
   RE_CHECK_LAUNCH("re_heightfield: launch");
   return RE_OK;
@@ -200,12 +252,15 @@ RE_API re_status re_sdf_trace(const re_sdf_params* p, const re_camera* cam, uint
   cd.focal = b.focal;
   cudaStream_t st = (cudaStream_t)stream;
   RE_CUDA(cudaMemsetAsync(counter, 0, 4, st));
+  RE_CUDA(cudaFuncSetAttribute(re::k_sdf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kPermSmemBytes));
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, re::k_sdf, 256, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, re::k_sdf, 256, re::kPermSmemBytes) !=
+          cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  re::k_sdf<<<per_sm * re::sm_count(), 256, 0, st>>>(t, sp, cd, w, h,
-                                                     reinterpret_cast<float4*>(d_out), counter);
+  re::k_sdf<<<per_sm * re::sm_count(), 256, re::kPermSmemBytes, st>>>(
+      t, sp, cd, w, h, reinterpret_cast<float4*>(d_out), counter);
   RE_CHECK_LAUNCH("re_sdf_trace: launch");
   return RE_OK;
 }

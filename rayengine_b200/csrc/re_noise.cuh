@@ -19,30 +19,38 @@ struct PermTable {
   uint8_t p[512];
 };
 
+// The table lives in shared memory once per lane: entry j of lane c is the
+// word 32*j + c, so a warp's 32 lookups (divergent lattice indices) always
+// fall in 32 different banks.  512 entries x 32 lanes x 4 B = 64 KB.
+constexpr uint32_t kPermSmemBytes = 512 * 32 * 4;
+
 __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
-  for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) s[i] = t.p[i];
+  for (uint32_t i = threadIdx.x; i < 512 * 32; i += blockDim.x) s[i] = t.p[i >> 5];
   __syncthreads();
 }
 
+struct Perm {
+  const uint32_t* __restrict__ s;
+  uint32_t lane;
+  __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return s[(j << 5) + lane]; }
+};
+
+__device__ __forceinline__ Perm perm_view(const uint32_t* s) { return Perm{s, threadIdx.x & 31u}; }
+
+// gradientDotV (sdf_functions.cuh:26-47) without branches: each case is a
+// sum of two signed coordinates, picked here with selects from bit masks
+// (bit h set = property holds for case h).  The operands and their signs are
+// exactly the reference's, so the single rounded addition is unchanged.
+//   first operand is y for cases 8-12, 14, 15 (x otherwise), negated for
+//   1, 3, 5, 7, 9, 11, 13, 14, 15; second operand is y for 0-3 and 13, x for
+//   12 (z otherwise), negated for 2, 3, 6, 7, 10, 11, 15.
 __device__ __forceinline__ float grad_dot(uint32_t h, float x, float y, float z) {
-  switch (h & 15u) {
-    case 0: return x + y;
-    case 1: return -x + y;
-    case 2: return x - y;
-    case 3: return -x - y;
-    case 4: return x + z;
-    case 5: return -x + z;
-    case 6: return x - z;
-    case 7: return -x - z;
-    case 8: return y + z;
-    case 9: return -y + z;
-    case 10: return y - z;
-    case 11: return -y - z;
-    case 12: return y + x;
-    case 13: return -x + y;
-    case 14: return -y + z;
-    default: return -y - z;
-  }
+  uint32_t b = 1u << (h & 15u);
+  float u = (b & 0xDF00u) ? y : x;
+  u = (b & 0xEAAAu) ? -u : u;
+  float v = (b & 0x200Fu) ? y : ((b & 0x1000u) ? x : z);
+  v = (b & 0x8CCCu) ? -v : v;
+  return u + v;
 }
 
 __device__ __forceinline__ float quintic(float t) {
@@ -51,10 +59,10 @@ __device__ __forceinline__ float quintic(float t) {
   return ((t * t) * t) * in;
 }
 
-__device__ __forceinline__ float perlin(const uint32_t* __restrict__ P, float x, float y, float z) {
+__device__ __forceinline__ float perlin(const Perm& P, float x, float y, float z) {
   float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-  int xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
-  int xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
+  uint32_t xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
+  uint32_t xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
   float tx = x - fx, ty = y - fy, tz = z - fz;
   float u = quintic(tx), v = quintic(ty), w = quintic(tz);
   float x1 = tx - 1.0f, y1 = ty - 1.0f, z1 = tz - 1.0f;
@@ -86,9 +94,10 @@ __device__ __forceinline__ float perlin(const uint32_t* __restrict__ P, float x,
   return r;
 }
 
-__device__ __forceinline__ float fbm(const uint32_t* __restrict__ P, float x, float y, float z,
+__device__ __forceinline__ float fbm(const Perm& P, float x, float y, float z,
                                      uint32_t octaves, float lacunarity, float gain) {
   float sum = 0.0f, amp = 1.0f;
+#pragma unroll 4
   for (uint32_t i = 0; i < octaves; ++i) {
     sum = __fmaf_rn(amp, perlin(P, x, y, z), sum);
     x *= lacunarity;
@@ -100,7 +109,7 @@ __device__ __forceinline__ float fbm(const uint32_t* __restrict__ P, float x, fl
 }
 
 // d(p) = p.y - amp * fbm(scale * p), lacunarity 2, gain 0.5
-__device__ __forceinline__ float terrain_density(const uint32_t* __restrict__ P, V3 p,
+__device__ __forceinline__ float terrain_density(const Perm& P, V3 p,
                                                  uint32_t octaves, float scale, float amp) {
   float f = fbm(P, scale * p.x, scale * p.y, scale * p.z, octaves, 2.0f, 0.5f);
   return __fmaf_rn(-amp, f, p.y);

@@ -96,7 +96,8 @@ __device__ __forceinline__ bool ray_tri(V3 o, V3 d, float4 T0, float4 T1, float4
 struct HitState {
   float t, u, v;
   int32_t id;
-  uint32_t ref;  // leaf-order triangle slot of the best hit
+  uint32_t ref;        // leaf-order triangle slot of the best hit
+  uint32_t leaf_node;  // node index of the leaf the best hit was found in
 };
 
 __device__ __forceinline__ uint2 load_node(const KdDev& kd, const uint2* snodes, uint32_t i) {
@@ -106,96 +107,157 @@ __device__ __forceinline__ uint2 load_node(const KdDev& kd, const uint2* snodes,
 // Stackless rope traversal (stackless_kdtree_traversal,
 // ray_functions.cuh:231-360) with the exit face taken from the slab test and
 // split decisions made on the ray parameter so that a point on a split plane
-// goes to the side the ray moves into.  Returns false when the ray misses the
-// root box.
-template <int MODE, bool ANYHIT, bool COUNT>
-__device__ __forceinline__ void traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
-                                         float tmax, HitState& hs, Counters& c) {
-  hs.t = K_INF;
-  hs.u = 0.f;
-  hs.v = 0.f;
-  hs.id = -1;
-  hs.ref = 0xFFFFFFFFu;
-  V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
-  float t_entry, t_root_exit;
-  if (!ray_box(kd.bmin, kd.bmax, o, inv, t_entry, t_root_exit)) return;
-  float best_t = fminf(t_root_exit, tmax);
-  int32_t best_id = -1;
-  float best_u = 0.f, best_v = 0.f;
-  uint32_t best_ref = 0xFFFFFFFFu;
-  uint32_t node = 0, visits = 0;
-  bool done = false;
-  while (!done && t_entry < best_t) {
-    uint2 nd = load_node(kd, snodes, node);
-    while ((nd.y & 3u) != 3u) {
-      uint32_t k = nd.y & 3u;
-      float split = __uint_as_float(nd.x);
-      float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
-      bool left;
-      if (dk > 0.0f)
-        left = t_entry < (split - ok) * ik;
-      else if (dk < 0.0f)
-        left = t_entry >= (split - ok) * ik;
-      else
-        left = ok < split;
-      node = (nd.y >> 2) + (left ? 0u : 1u);
-      nd = load_node(kd, snodes, node);
-      if (COUNT) c.inner++;
+// goes to the side the ray moves into.
+//
+// The walk is a per-lane state machine: trav_init() clips the ray to the
+// root box, each trav_step() descends to one leaf, tests its triangles and
+// follows one rope.  Kernels either run a ray to completion (traverse()) or
+// interleave steps of many rays and refill finished lanes (k_ao_secondary).
+//
+// start: a leaf node to begin in instead of descending from the root (a
+// secondary ray starts where its primary ray hit); used only when the ray
+// origin lies in that leaf's region, otherwise the walk starts at the root.
+// Either way every leaf the ray crosses is visited, so hits are unchanged.
+struct Trav {
+  V3 o, d, inv;
+  float t_entry, best_t, best_u, best_v;
+  int32_t best_id;
+  uint32_t best_ref, best_leaf, node, visits;
+  bool live;
+};
+
+__device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, float tmax,
+                                          uint32_t start) {
+  s.o = o;
+  s.d = d;
+  s.inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  s.best_id = -1;
+  s.best_u = 0.f;
+  s.best_v = 0.f;
+  s.best_ref = 0xFFFFFFFFu;
+  s.best_leaf = 0;
+  s.node = 0;
+  s.visits = 0;
+  float t_root_exit;
+  s.live = ray_box(kd.bmin, kd.bmax, o, s.inv, s.t_entry, t_root_exit);
+  if (!s.live) return;
+  s.best_t = fminf(t_root_exit, tmax);
+  s.live = s.t_entry < s.best_t;
+  if (s.live && start != 0) {
+    uint2 sn = __ldg(&kd.nodes[start]);
+    if ((sn.y & 3u) == 3u) {
+      const float4* SL = kd.leaves + 4 * (size_t)(sn.y >> 2);
+      float4 A = __ldg(SL), B = __ldg(SL + 1);
+      if (o.x >= A.x && o.x <= A.w && o.y >= A.y && o.y <= B.x && o.z >= A.z && o.z <= B.y)
+        s.node = start;
     }
-    const float4* L = kd.leaves + 4 * (size_t)(nd.y >> 2);
-    float4 A = __ldg(L), B = __ldg(L + 1);
-    if (COUNT) c.leaf++;
-    uint32_t first = __float_as_uint(B.z), count = __float_as_uint(B.w);
-    for (uint32_t i = first; i < first + count; ++i) {
-      const float4* T = kd.tris + 3 * (size_t)i;
-      float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
-      int32_t id = __float_as_int(T0.w);
-      float t, u, v;
-      if (COUNT) c.tests++;
-      if (ray_tri<MODE>(o, d, T0, T1, T2, t, u, v)) {
-        if (t < best_t || (t == best_t && id < best_id && best_id >= 0)) {
-          best_t = t;
-          best_id = id;
-          best_u = u;
-          best_v = v;
-          best_ref = i;
-          if (ANYHIT) {
-            done = true;
-            break;
-          }
+  }
+}
+
+template <int MODE, bool ANYHIT, bool COUNT>
+__device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2* snodes,
+                                          Counters& c) {
+  const V3 o = s.o, d = s.d, inv = s.inv;
+  const float t_entry = s.t_entry;
+  uint32_t node = s.node;
+  uint2 nd = load_node(kd, snodes, node);
+  while ((nd.y & 3u) != 3u) {
+    uint32_t k = nd.y & 3u;
+    float split = __uint_as_float(nd.x);
+    float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
+    bool left;
+    if (dk > 0.0f)
+      left = t_entry < (split - ok) * ik;
+    else if (dk < 0.0f)
+      left = t_entry >= (split - ok) * ik;
+    else
+      left = ok < split;
+    node = (nd.y >> 2) + (left ? 0u : 1u);
+    nd = load_node(kd, snodes, node);
+    if (COUNT) c.inner++;
+  }
+  const float4* L = kd.leaves + 4 * (size_t)(nd.y >> 2);
+  float4 A = __ldg(L), B = __ldg(L + 1);
+  if (COUNT) c.leaf++;
+  uint32_t first = __float_as_uint(B.z), count = __float_as_uint(B.w);
+  for (uint32_t i = first; i < first + count; ++i) {
+    const float4* T = kd.tris + 3 * (size_t)i;
+    float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
+    int32_t id = __float_as_int(T0.w);
+    float t, u, v;
+    if (COUNT) c.tests++;
+    if (ray_tri<MODE>(o, d, T0, T1, T2, t, u, v)) {
+      if (t < s.best_t || (t == s.best_t && id < s.best_id && s.best_id >= 0)) {
+        s.best_t = t;
+        s.best_id = id;
+        s.best_u = u;
+        s.best_v = v;
+        s.best_ref = i;
+        s.best_leaf = node;
+        if (ANYHIT) {
+          s.live = false;
+          return;
         }
       }
     }
-    if (done) break;
-    float texit = __int_as_float(0x7f800000);
-    int face = -1;
-    {
-      float tk;
-      if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
-      else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
-      if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
-      else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
-      if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
-      else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
-    }
-    if (face < 0) break;
-    t_entry = fmaxf(t_entry, texit);
-    if (!(t_entry < best_t)) break;
-    int32_t rope = __ldg(reinterpret_cast<const int32_t*>(L + 2) + face);
-    if (rope < 0) break;
-    node = (uint32_t)rope;
-    if (++visits >= kd.max_visits) {
-      c.status = 1;
-      break;
-    }
   }
-  if (best_id >= 0) {
-    hs.t = best_t;
-    hs.u = best_u;
-    hs.v = best_v;
-    hs.id = best_id;
-    hs.ref = best_ref;
+  float texit = __int_as_float(0x7f800000);
+  int face = -1;
+  {
+    float tk;
+    if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
+    else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
+    if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
+    else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
+    if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
+    else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
   }
+  if (face < 0) {
+    s.live = false;
+    return;
+  }
+  s.t_entry = fmaxf(t_entry, texit);
+  if (!(s.t_entry < s.best_t)) {
+    s.live = false;
+    return;
+  }
+  int32_t rope = __ldg(reinterpret_cast<const int32_t*>(L + 2) + face);
+  if (rope < 0) {
+    s.live = false;
+    return;
+  }
+  s.node = (uint32_t)rope;
+  if (++s.visits >= kd.max_visits) {
+    c.status = 1;
+    s.live = false;
+  }
+}
+
+__device__ __forceinline__ void trav_result(const Trav& s, HitState& hs) {
+  if (s.best_id >= 0) {
+    hs.t = s.best_t;
+    hs.u = s.best_u;
+    hs.v = s.best_v;
+    hs.id = s.best_id;
+    hs.ref = s.best_ref;
+    hs.leaf_node = s.best_leaf;
+  } else {
+    hs.t = K_INF;
+    hs.u = 0.f;
+    hs.v = 0.f;
+    hs.id = -1;
+    hs.ref = 0xFFFFFFFFu;
+    hs.leaf_node = 0;
+  }
+}
+
+template <int MODE, bool ANYHIT, bool COUNT>
+__device__ __forceinline__ void traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
+                                         float tmax, uint32_t start, HitState& hs, Counters& c) {
+  Trav s;
+  trav_init(s, kd, o, d, tmax, start);
+  while (s.live) trav_step<MODE, ANYHIT, COUNT>(s, kd, snodes, c);
+  trav_result(s, hs);
 }
 
 __device__ __forceinline__ void stage_nodes(const KdDev& kd, uint2* snodes) {
@@ -236,7 +298,7 @@ __global__ void __launch_bounds__(256) k_primary(KdDev kd, CamDev cam, uint32_t 
     generate_ray(cam, w, h, x, y, o, d);
     HitState hs;
     Counters c = {0, 0, 0, 0};
-    traverse<MODE, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), hs, c);
+    traverse<MODE, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), 0u, hs, c);
     size_t pix = (size_t)y * w + x;
     if (COUNT)
       counts[pix] = make_uint4(c.inner, c.leaf, c.tests, c.status);
@@ -262,7 +324,7 @@ __global__ void __launch_bounds__(256) k_rays(KdDev kd, const float4* __restrict
     V3 o = {R0.x, R0.y, R0.z}, d = {R1.x, R1.y, R1.z};
     HitState hs;
     Counters c = {0, 0, 0, 0};
-    traverse<MODE, ANYHIT, false>(kd, snodes, o, d, R0.w, hs, c);
+    traverse<MODE, ANYHIT, false>(kd, snodes, o, d, R0.w, 0u, hs, c);
     store_hit(out, i, hs);
   }
 }
@@ -272,6 +334,17 @@ struct AoDev {
   V3 light;
   float ao_length, bias;
   uint32_t seed;
+};
+
+// Secondary-ray queue and its tuning: ray kind k (0 shadow, 1..4 AO) of the
+// r-th hit is record k * kind_stride + r * rank_stride.  Pixel-major
+// (kind_stride 1, rank_stride 5) keeps a pixel's five rays together (better
+// cache reuse); kind-major (kind_stride = capacity, rank_stride 1) gives a
+// warp rays of one kind from neighbouring pixels.  refill_min: idle lanes a
+// warp waits for before claiming new rays (32 = whole warps only).
+struct AoQueue {
+  float4* q;
+  uint32_t kind_stride, rank_stride, refill_min;
 };
 
 // Warp-sum of per-thread work counters, one 64-bit atomic per warp and field.
@@ -288,14 +361,17 @@ __device__ __forceinline__ void flush_counts(const Counters& c, uint32_t rays,
 }
 
 // Primary rays of the AO frame: closest hit, pixel mask bit 0, and the five
-// secondary rays of every hit appended to the queue (one warp-aggregated
-// atomic per warp).  COUNT: also sum the traversal work into totals[0..3].
+// secondary rays of every hit appended to the queue.
+//
+// Records go to the AoQueue layout; one warp-aggregated atomic per warp
+// (ballot + popc) assigns hit ranks.  counters: [0] tile cursor, [1] hits,
+// [2] secondary cursor, [3] secondary rays.  COUNT: also sum the traversal
+// work into totals[0..3].
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev ao, uint32_t w,
                                                     uint32_t h, re_hit* __restrict__ out,
                                                     uint32_t* __restrict__ mask,
-                                                    float4* __restrict__ queue,
-                                                    uint32_t* __restrict__ counters,
+                                                    AoQueue aq, uint32_t* __restrict__ counters,
                                                     unsigned long long* __restrict__ totals) {
   extern __shared__ uint2 snodes[];
   stage_nodes(kd, snodes);
@@ -314,7 +390,7 @@ __global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev 
     V3 o = {0, 0, 0}, d = {0, 0, 1};
     if (valid) {
       generate_ray(cam, w, h, x, y, o, d);
-      traverse<0, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), hs, c);
+      traverse<0, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), 0u, hs, c);
       ++rays;
       size_t pix = (size_t)y * w + x;
       if (!COUNT) {
@@ -326,10 +402,13 @@ __global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev 
     uint32_t ballot = __ballot_sync(0xFFFFFFFFu, hit);
     if (!ballot) continue;
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&counters[1], 5u * __popc(ballot));
+    if (lane == 0) {
+      base = atomicAdd(&counters[1], (uint32_t)__popc(ballot));
+      atomicAdd(&counters[3], 5u * __popc(ballot));
+    }
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
     if (!hit) continue;
-    uint32_t slot = base + 5u * __popc(ballot & ((1u << lane) - 1u));
+    uint32_t rank = base + __popc(ballot & ((1u << lane) - 1u));
     // geometric normal of the hit triangle, facing the incoming ray
     const float4* T = kd.tris + 3 * (size_t)hs.ref;
     float4 T1 = __ldg(T + 1), T2 = __ldg(T + 2);
@@ -339,9 +418,14 @@ __global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev 
     V3 org = {__fmaf_rn(n.x, ao.bias, p.x), __fmaf_rn(n.y, ao.bias, p.y),
               __fmaf_rn(n.z, ao.bias, p.z)};
     uint32_t pix = y * w + x;
-    queue[2 * (size_t)slot] = make_float4(org.x, org.y, org.z, K_INF);
-    queue[2 * (size_t)slot + 1] = make_float4(ao.light.x, ao.light.y, ao.light.z,
-                                              __uint_as_float(pix * 8u + 1u));
+    // record: {origin, start leaf node} {direction, pixel*8 + mask bit}; the
+    // shadow ray (bit 1) is unbounded, AO rays (bits 2..5) have ao_length
+    float start = __uint_as_float(hs.leaf_node);
+    float4* queue = aq.q;
+    size_t q0 = (size_t)rank * aq.rank_stride;
+    queue[2 * q0] = make_float4(org.x, org.y, org.z, start);
+    queue[2 * q0 + 1] = make_float4(ao.light.x, ao.light.y, ao.light.z,
+                                    __uint_as_float(pix * 8u + 1u));
     // createCoordinateSystem (cuda_helper_functions.h:197-204)
     V3 nt;
     if (fabsf(n.x) > fabsf(n.y)) {
@@ -364,40 +448,71 @@ __global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev 
       V3 dir = {__fmaf_rn(lz, nt.x, __fmaf_rn(ly, n.x, lx * nb.x)),
                 __fmaf_rn(lz, nt.y, __fmaf_rn(ly, n.y, lx * nb.y)),
                 __fmaf_rn(lz, nt.z, __fmaf_rn(ly, n.z, lx * nb.z))};
-      size_t q = slot + 1 + j;
-      queue[2 * q] = make_float4(org.x, org.y, org.z, ao.ao_length);
+      size_t q = q0 + (size_t)(1 + j) * aq.kind_stride;
+      queue[2 * q] = make_float4(org.x, org.y, org.z, start);
       queue[2 * q + 1] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(pix * 8u + 2u + j));
     }
   }
   if (COUNT) flush_counts(c, rays, totals);
 }
 
-// Any-hit pass over the queued secondary rays; unoccluded rays set their
-// bit in the pixel mask.  The ray count is read on the device.
+// Any-hit pass over the queued secondary rays; unoccluded rays set their bit
+// in the pixel mask.  Each lane runs its ray one leaf at a time; when at
+// least aq.refill_min lanes of a warp are idle the warp claims that many new
+// rays with one atomic, so lanes need not wait for the slowest ray of the
+// warp.  The number of hits is read on the device.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_ao_secondary(KdDev kd, const float4* __restrict__ queue,
+__global__ void __launch_bounds__(256, 5) k_ao_secondary(KdDev kd, AoDev ao, AoQueue aq,
                                                       uint32_t* __restrict__ mask,
                                                       uint32_t* __restrict__ counters,
                                                       unsigned long long* __restrict__ totals) {
   extern __shared__ uint2 snodes[];
   stage_nodes(kd, snodes);
   uint32_t lane = threadIdx.x & 31u;
-  uint32_t n = counters[1];
+  uint32_t nh = counters[1];
+  uint32_t n = 5u * nh;
   Counters c = {0, 0, 0, 0};
   uint32_t rays = 0;
+  Trav s;
+  s.live = false;
+  uint32_t tag = 0;
+  bool exhausted = false;
   for (;;) {
-    uint32_t chunk = warp_fetch(&counters[2]);
-    if (chunk * 32 >= n) break;
-    uint32_t i = chunk * 32 + lane;
-    if (i >= n) continue;
-    float4 R0 = __ldg(&queue[2 * (size_t)i]), R1 = __ldg(&queue[2 * (size_t)i + 1]);
-    V3 o = {R0.x, R0.y, R0.z}, d = {R1.x, R1.y, R1.z};
-    HitState hs;
-    traverse<0, true, COUNT>(kd, snodes, o, d, R0.w, hs, c);
-    ++rays;
-    if (!COUNT && hs.id < 0) {
-      uint32_t tag = __float_as_uint(R1.w);
-      atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !s.live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && (nidle >= aq.refill_min || nidle == 32u)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&counters[2], nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= n) exhausted = true;
+      if (!s.live) {
+        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+        if (i < n) {
+          uint32_t kind, e;
+          if (aq.kind_stride == 1u) {
+            e = i;
+            kind = i % 5u;
+          } else {
+            kind = i / nh;
+            e = kind * aq.kind_stride + (i - kind * nh);
+          }
+          float4 R0 = __ldg(&aq.q[2 * (size_t)e]), R1 = __ldg(&aq.q[2 * (size_t)e + 1]);
+          tag = __float_as_uint(R1.w);
+          float tmax = kind == 0 ? K_INF : ao.ao_length;
+          trav_init(s, kd, v3(R0.x, R0.y, R0.z), v3(R1.x, R1.y, R1.z), tmax,
+                    __float_as_uint(R0.w));
+          ++rays;
+          if (!s.live && !COUNT) atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, s.live) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (s.live) {
+      trav_step<0, true, COUNT>(s, kd, snodes, c);
+      if (!s.live && !COUNT && s.best_id < 0) atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
     }
   }
   if (COUNT) flush_counts(c, rays, totals + 4);
@@ -418,6 +533,9 @@ struct re_scene {
   uint32_t max_visits = 16384;
   uint32_t stage = 0;
   int blocks_per_sm = 0;
+  float ao_length = 1.0f;    // AO ray length of the last primary pass
+  uint32_t queue_stride = 0;  // record capacity per ray kind in d_queue
+  re_tuning tune = {0, 0, 32, 0};
 };
 
 namespace re {
@@ -480,7 +598,22 @@ re_status upload(re_scene* s) {
   RE_CUDA(cudaMemcpy(s->d_tris, h.tris.data(), h.tris.size() * 4, cudaMemcpyHostToDevice));
   RE_CUDA(cudaMemset(s->d_counters, 0, 64));
   s->stage = std::min<uint32_t>(h.bfs_nodes, kMaxStage);
+  s->tune.stage_nodes = s->stage;
   return RE_OK;
+}
+
+AoQueue ao_queue(const re_scene* s, float4* q, uint32_t capacity) {
+  AoQueue aq;
+  aq.q = q;
+  if (s->tune.queue_kind_major) {
+    aq.kind_stride = capacity;
+    aq.rank_stride = 1;
+  } else {
+    aq.kind_stride = 1;
+    aq.rank_stride = 5;
+  }
+  aq.refill_min = s->tune.refill_min;
+  return aq;
 }
 
 void release(re_scene* s) {
@@ -722,6 +855,7 @@ re_status ao_prepare(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
   if (!cam || !p || w < 2 || h < 2) return fail(RE_ERR_INVALID_ARG, "%s: bad arguments", fn);
   if ((uint64_t)w * h > (1ull << 28)) return fail(RE_ERR_LIMIT, "%s: image > 2^28 pixels", fn);
   size_t need = 5ull * w * h;
+  s->queue_stride = w * h;
   if (s->queue_cap < need) {
     // The queue grows outside stream order: wait until no earlier frame on
     // this stream still reads the old one.
@@ -737,6 +871,7 @@ re_status ao_prepare(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
   ao.ao_length = p->ao_length;
   ao.bias = p->bias;
   ao.seed = p->seed;
+  s->ao_length = p->ao_length;
   return RE_OK;
 }
 
@@ -746,11 +881,12 @@ re_status ao_primary(re_scene* s, const CamDev& cd, const AoDev& ao, uint32_t w,
                      cudaStream_t st) {
   KdDev kd = kd_view(s);
   size_t smem = kd.stage * sizeof(uint2);
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 12, st));
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 16, st));
   auto k = k_ao_primary<COUNT>;
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask, s->d_queue,
-                                          s->d_counters, totals);
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask,
+                                          ao_queue(s, s->d_queue, s->queue_stride), s->d_counters,
+                                          totals);
   RE_CHECK_LAUNCH("ao primary launch");
   return RE_OK;
 }
@@ -759,10 +895,13 @@ template <bool COUNT>
 re_status ao_secondary(re_scene* s, uint32_t* d_mask, unsigned long long* totals,
                        cudaStream_t st) {
   KdDev kd = kd_view(s);
+  AoDev ao{};
+  ao.ao_length = s->ao_length;
   size_t smem = kd.stage * sizeof(uint2);
   auto k = k_ao_secondary<COUNT>;
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k<<<grid_for(k, smem), 256, smem, st>>>(kd, s->d_queue, d_mask, s->d_counters, totals);
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, ao, ao_queue(s, s->d_queue, s->queue_stride),
+                                          d_mask, s->d_counters, totals);
   RE_CHECK_LAUNCH("ao secondary launch");
   return RE_OK;
 }
@@ -794,7 +933,7 @@ RE_API re_status re_render_ao_secondary(re_scene* s, uint32_t* d_mask, uint32_t*
   rs = re::ao_secondary<false>(s, d_mask, nullptr, st);
   if (rs != RE_OK) return rs;
   if (d_num_secondary)
-    RE_CUDA(cudaMemcpyAsync(d_num_secondary, s->d_counters + 1, 4, cudaMemcpyDeviceToDevice, st));
+    RE_CUDA(cudaMemcpyAsync(d_num_secondary, s->d_counters + 3, 4, cudaMemcpyDeviceToDevice, st));
   return RE_OK;
 }
 
@@ -897,22 +1036,113 @@ RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam, uint32_
   ao.seed = p->seed;
   size_t smem = kd.stage * sizeof(uint2);
   // the array keeps the previous call's contents: the cursors must restart at zero
-  RE_CUDA(cudaMemsetAsync(counters, 0, 12, st));
+  RE_CUDA(cudaMemsetAsync(counters, 0, 16, st));
   {
     auto k = re::k_ao_primary<false>;
     RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask, queue,
-                                                counters, nullptr);
+    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask,
+                                                re::ao_queue(s, queue, w * h), counters, nullptr);
     RE_CHECK_LAUNCH("re_render_ao_noalloc: primary launch");
   }
   {
     auto k = re::k_ao_secondary<false>;
     RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, queue, d_mask, counters, nullptr);
+    k<<<re::grid_for(k, smem), 256, smem, st>>>(kd, ao, re::ao_queue(s, queue, w * h), d_mask,
+                                                counters, nullptr);
     RE_CHECK_LAUNCH("re_render_ao_noalloc: secondary launch");
   }
   if (d_num_secondary)
-    RE_CUDA(cudaMemcpyAsync(d_num_secondary, counters + 1, 4, cudaMemcpyDeviceToDevice, st));
+    RE_CUDA(cudaMemcpyAsync(d_num_secondary, counters + 3, 4, cudaMemcpyDeviceToDevice, st));
+  return RE_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- autotuner
+extern "C" {
+
+RE_API re_status re_scene_get_tuning(const re_scene* s, re_tuning* out) {
+  if (!s || !out) return re::fail(RE_ERR_INVALID_ARG, "re_scene_get_tuning: null argument");
+  *out = s->tune;
+  return RE_OK;
+}
+
+RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t) {
+  if (!s || !t) return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: null argument");
+  if (t->refill_min < 1 || t->refill_min > 32)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: refill_min must be in [1, 32]");
+  if (t->queue_kind_major > 1)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0 or 1");
+  s->tune = *t;
+  s->tune.stage_nodes = std::min(std::min(t->stage_nodes, s->host.bfs_nodes), re::kMaxStage);
+  s->stage = s->tune.stage_nodes;
+  return RE_OK;
+}
+
+// Times the AO frame for every combination of staging depth, queue layout
+// and refill threshold (one warm-up and three timed frames each, CUDA events
+// on the caller's stream) and keeps the fastest on the scene.  Set-up time
+// only: it allocates its own output buffers.
+RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                const re_ao_params* p, re_tuning* best_out, float* best_ms_out,
+                                void* stream) {
+  re_status rs = re::check_scene(s, "re_autotune_ao");
+  if (rs != RE_OK) return rs;
+  if (!cam || !p || w < 2 || h < 2) return re::fail(RE_ERR_INVALID_ARG, "re_autotune_ao: bad arguments");
+  if ((uint64_t)w * h > (1ull << 28)) return re::fail(RE_ERR_LIMIT, "re_autotune_ao: image > 2^28 pixels");
+  cudaStream_t st = (cudaStream_t)stream;
+  re_hit* hits = nullptr;
+  uint32_t* mask = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  RE_CUDA(cudaMalloc(&hits, (size_t)w * h * sizeof(re_hit)));
+  cudaError_t ce = cudaMalloc(&mask, (size_t)w * h * 4);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  re_tuning keep = s->tune, best = s->tune;
+  float best_ms = 1e30f;
+  uint32_t bfs = std::min(s->host.bfs_nodes, re::kMaxStage);
+  const uint32_t stages[4] = {0u, std::min(1024u, bfs), std::min(4096u, bfs), bfs};
+  const uint32_t refills[4] = {4u, 8u, 16u, 32u};
+  for (int si = 0; si < 4 && ce == cudaSuccess && rs == RE_OK; ++si) {
+    if (si > 0 && stages[si] == stages[si - 1]) continue;
+    for (uint32_t km = 0; km < 2 && rs == RE_OK; ++km) {
+      for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
+        re_tuning t = {stages[si], km, refills[ri], 0};
+        rs = re_scene_set_tuning(s, &t);
+        if (rs != RE_OK) break;
+        rs = re_render_ao(s, cam, w, h, p, hits, mask, nullptr, stream);
+        if (rs != RE_OK) break;
+        ce = cudaEventRecord(e0, st);
+        for (int r = 0; r < 3 && rs == RE_OK; ++r) rs = re_render_ao(s, cam, w, h, p, hits, mask, nullptr, stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce != cudaSuccess) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = s->tune;
+        }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(hits);
+  cudaFree(mask);
+  if (ce != cudaSuccess) {
+    s->tune = keep;
+    s->stage = keep.stage_nodes;
+    return re::cuda_fail(ce, "re_autotune_ao");
+  }
+  if (rs != RE_OK) {
+    s->tune = keep;
+    s->stage = keep.stage_nodes;
+    return rs;
+  }
+  re_scene_set_tuning(s, &best);
+  if (best_out) *best_out = best;
+  if (best_ms_out) *best_ms_out = best_ms / 3.0f;
   return RE_OK;
 }
 

@@ -245,3 +245,31 @@ def test_sdf_config2_sampled(cuda):
     nrm = np.linalg.norm(f[allhit, 3:6], axis=1)
     assert np.all(np.abs(nrm - 1) < 1e-5)
     assert allhit.mean() > 0.3
+
+
+def test_tunings_give_identical_frames(cuda):
+    """Staging depth, queue layout and refill threshold change only speed."""
+    cfg = rb.configs.HeightfieldConfig(cells=128, width=320, height=180)
+    P = po.perm(cfg.seed)
+    verts, faces = po.heightfield(P, cfg.cells, cfg.lo, cfg.hi, cfg.octaves, cfg.amplitude)
+    cam = cfg.camera()
+    light = rb.unit(cfg.light_dir)
+    with rb.KDScene.from_mesh(verts, faces) as sc:
+        ref = None
+        for stage, km, refill in ((0, 0, 32), (64, 1, 4), (4096, 0, 8), (4096, 1, 1), (1, 1, 32)):
+            sc.set_tuning(stage, km, refill)
+            got = [x.cpu().numpy() for x in sc.render_ao(cam, cfg.width, cfg.height, light,
+                                                         cfg.ao_length, cfg.bias, cfg.ao_seed)]
+            if ref is None:
+                ref = got
+            else:
+                for a, b in zip(got, ref):
+                    assert np.array_equal(a, b), (stage, km, refill)
+        params = rb.ao_params(cfg.light_dir, cfg.ao_length, cfg.bias, cfg.ao_seed)
+        best = sc.autotune_ao(cam, cfg.width, cfg.height, params)
+        assert best["frame_ms"] > 0 and 1 <= best["refill_min"] <= 32
+        assert sc.tuning()["refill_min"] == best["refill_min"]
+        got = [x.cpu().numpy() for x in sc.render_ao(cam, cfg.width, cfg.height, light,
+                                                     cfg.ao_length, cfg.bias, cfg.ao_seed)]
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)

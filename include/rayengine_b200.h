@@ -282,6 +282,85 @@ RE_API re_status re_sdf_trace(const re_sdf_params* p, const re_camera* cam,
                               uint32_t w, uint32_t h, re_sdf_hit* d_out,
                               void* stream);
 
+/* ---- neural SDF surrogate ------------------------------------------
+ * No counterpart in the reference (it has no learned component): a
+ * Fourier-feature MLP (3 -> 128 features -> 4 x 64 softplus -> 1) that
+ * stands in for the terrain density d(p) = p.y - amp*fbm(scale*p) while
+ * sphere tracing, with the exact field finishing every ray.  Trained on the
+ * device by hand-written forward/backward/Adam kernels; evaluated with BF16
+ * operands on the tensor cores (tcgen05, FP32 accumulation in tensor
+ * memory). */
+typedef struct re_nsdf re_nsdf;
+
+typedef struct re_nsdf_config {
+  float box_min[3], box_max[3]; /* input box, mapped to [-1, 1]^3          */
+  float f0;                     /* lowest feature frequency (cycles/unit)   */
+  uint32_t seed;                /* weight initialisation and sampling seed  */
+} re_nsdf_config;
+
+typedef struct re_nsdf_trace_params {
+  float lipschitz;      /* bound on the network's gradient norm           */
+  float safety;         /* step = safety * distance / lipschitz            */
+  float switch_dist;    /* hand over to the exact field below this         */
+  float min_step;       /* smallest network step                           */
+  uint32_t max_network_steps; /* 0 = 256                                   */
+  uint32_t max_exact_steps;   /* 0 = the field's max_steps                 */
+} re_nsdf_trace_params;
+
+RE_API uint32_t re_nsdf_num_params(void);
+/* Axis-aligned box of the view frustum [0, tmax] with y clamped. */
+RE_API re_status re_nsdf_box_for_camera(const re_camera* cam, uint32_t w,
+                                        uint32_t h, float tmax, float y_lo,
+                                        float y_hi, float* box_min,
+                                        float* box_max);
+RE_API re_status re_nsdf_create(const re_nsdf_config* cfg, re_nsdf** out);
+RE_API re_status re_nsdf_destroy(re_nsdf* s);
+/* Parameters as FP32 (re_nsdf_num_params values): W1 [64][128], b1, W2,
+ * b2, W3, b3, W4, b4 ([64][64] and 64 each), w5 [64], b5. */
+RE_API re_status re_nsdf_get_params(const re_nsdf* s, float* host);
+RE_API re_status re_nsdf_set_params(re_nsdf* s, const float* host);
+/* Training data: num_points float4 {x, y, z, label}, half uniform in the
+ * box and half within N(0, 0.02) of exact-traced camera hits; label = the
+ * exact field's first-order distance d / |grad d| clipped to [-4, 4]. */
+RE_API re_status re_nsdf_generate(re_nsdf* s, const re_sdf_params* field,
+                                  const re_camera* cam, uint32_t w, uint32_t h,
+                                  uint32_t num_points, uint32_t seed,
+                                  void* stream);
+RE_API re_status re_nsdf_get_data(const re_nsdf* s, float* host_xyzl,
+                                  uint32_t max_points);
+/* `steps` Adam steps (L1 loss) on batches of `batch` points sampled from the
+ * generated data; batch must be a multiple of 512.  loss_out (host, steps
+ * floats) may be NULL.  Synchronises the stream. */
+RE_API re_status re_nsdf_train(re_nsdf* s, uint32_t steps, uint32_t batch,
+                               float lr, float* loss_out, void* stream);
+/* Gradient of the mean L1 loss of n points (device float4 {x,y,z,label},
+ * n a multiple of 512) w.r.t. the parameters (device, re_nsdf_num_params
+ * floats) and the predictions (device, n floats, may be NULL). */
+RE_API re_status re_nsdf_loss_grad(re_nsdf* s, const float* d_xyzl, uint32_t n,
+                                   float* d_grad, float* d_pred, void* stream);
+/* Network distance of n points (device, 3 floats each): tensor cores. */
+RE_API re_status re_nsdf_eval(re_nsdf* s, const float* d_pts, uint32_t n,
+                              float* d_out, void* stream);
+/* The same with the training arithmetic (SIMT FP32, BF16-rounded). */
+RE_API re_status re_nsdf_eval_reference(re_nsdf* s, const float* d_pts,
+                                        uint32_t n, float* d_out, void* stream);
+/* Largest forward-difference gradient norm over `samples` training points. */
+RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h,
+                                   float* out, void* stream);
+/* Neural march then exact refinement; output as re_sdf_trace (steps =
+ * network steps + exact steps). */
+RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
+                               const re_nsdf_trace_params* tp,
+                               const re_camera* cam, uint32_t w, uint32_t h,
+                               re_sdf_hit* d_out, void* stream);
+/* Rays handed to the exact field by the last trace, and the device error
+ * flag (1 = a tensor-core wait reached its bound). */
+RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
+                                      int* error);
+/* Checkpoint: parameters, Adam moments and step count. */
+RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
+RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,8 +120,29 @@ class re_sdf_params(ctypes.Structure):
     ]
 
 
+class re_nsdf_config(ctypes.Structure):
+    _fields_ = [
+        ("box_min", ctypes.c_float * 3),
+        ("box_max", ctypes.c_float * 3),
+        ("f0", ctypes.c_float),
+        ("seed", ctypes.c_uint32),
+    ]
+
+
+class re_nsdf_trace_params(ctypes.Structure):
+    _fields_ = [
+        ("lipschitz", ctypes.c_float),
+        ("safety", ctypes.c_float),
+        ("switch_dist", ctypes.c_float),
+        ("min_step", ctypes.c_float),
+        ("max_network_steps", ctypes.c_uint32),
+        ("max_exact_steps", ctypes.c_uint32),
+    ]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
+_F = ctypes.c_float
 _SIGS = {
     "re_abi_version": (ctypes.c_int, []),
     "re_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -150,6 +171,23 @@ _SIGS = {
     "re_gen_soup": (ctypes.c_int, [ctypes.c_uint64, _U32, _P]),
     "re_gen_grid_faces": (ctypes.c_int, [_U32, _P]),
     "re_sdf_trace": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_nsdf_num_params": (ctypes.c_uint32, []),
+    "re_nsdf_box_for_camera": (ctypes.c_int, [ctypes.POINTER(re_camera), _U32, _U32, _F, _F, _F, _P, _P]),
+    "re_nsdf_create": (ctypes.c_int, [ctypes.POINTER(re_nsdf_config), ctypes.POINTER(_P)]),
+    "re_nsdf_destroy": (ctypes.c_int, [_P]),
+    "re_nsdf_get_params": (ctypes.c_int, [_P, _P]),
+    "re_nsdf_set_params": (ctypes.c_int, [_P, _P]),
+    "re_nsdf_generate": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _U32, _U32, _P]),
+    "re_nsdf_get_data": (ctypes.c_int, [_P, _P, _U32]),
+    "re_nsdf_train": (ctypes.c_int, [_P, _U32, _U32, _F, _P, _P]),
+    "re_nsdf_loss_grad": (ctypes.c_int, [_P, _P, _U32, _P, _P, _P]),
+    "re_nsdf_eval": (ctypes.c_int, [_P, _P, _U32, _P, _P]),
+    "re_nsdf_eval_reference": (ctypes.c_int, [_P, _P, _U32, _P, _P]),
+    "re_nsdf_lipschitz": (ctypes.c_int, [_P, _U32, _F, ctypes.POINTER(_F), _P]),
+    "re_nsdf_trace": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int)]),
+    "re_nsdf_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "re_nsdf_load": (ctypes.c_int, [_P, ctypes.c_char_p]),
 }
 
 EXPORTED = tuple(_SIGS)

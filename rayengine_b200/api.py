@@ -348,3 +348,134 @@ def sphere_trace(params, cam: RCamera, w: int, h: int, out=None, stream=None):
     call("re_sdf_trace", ctypes.byref(params), ctypes.byref(cam), w, h, _dptr(out),
          _stream_ptr(stream))
     return out
+
+
+# ------------------------------------------------------ neural SDF surrogate
+def nsdf_trace_params(lipschitz, safety=0.9, switch_dist=0.05, min_step=1e-3,
+                      max_network_steps=256, max_exact_steps=0):
+    p = _lib.re_nsdf_trace_params()
+    p.lipschitz, p.safety, p.switch_dist, p.min_step = lipschitz, safety, switch_dist, min_step
+    p.max_network_steps, p.max_exact_steps = max_network_steps, max_exact_steps
+    return p
+
+
+class NeuralSDF:
+    """Fourier-feature MLP surrogate of the terrain density (trained and run
+    on the device; tensor-core inference)."""
+
+    def __init__(self, box_min, box_max, f0: float = 0.5, seed: int = 1):
+        cfg = _lib.re_nsdf_config()
+        cfg.box_min[:] = [float(x) for x in box_min]
+        cfg.box_max[:] = [float(x) for x in box_max]
+        cfg.f0, cfg.seed = f0, seed
+        self.box_min, self.box_max, self.f0 = list(cfg.box_min), list(cfg.box_max), f0
+        h = ctypes.c_void_p()
+        call("re_nsdf_create", ctypes.byref(cfg), ctypes.byref(h))
+        self._h = h
+
+    @staticmethod
+    def box_for_camera(cam, w, h, tmax, y_lo, y_hi):
+        lo = np.zeros(3, np.float32)
+        hi = np.zeros(3, np.float32)
+        call("re_nsdf_box_for_camera", ctypes.byref(cam), w, h, tmax, y_lo, y_hi,
+             lo.ctypes.data, hi.ctypes.data)
+        return lo, hi
+
+    @property
+    def num_params(self) -> int:
+        return int(lib.re_nsdf_num_params())
+
+    def close(self):
+        if self._h:
+            lib.re_nsdf_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.num_params, np.float32)
+        call("re_nsdf_get_params", self._h, out.ctypes.data)
+        return out
+
+    def set_params(self, params: np.ndarray) -> None:
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.shape == (self.num_params,)
+        call("re_nsdf_set_params", self._h, params.ctypes.data)
+
+    def generate(self, field, cam, w, h, num_points, seed=1, stream=None):
+        call("re_nsdf_generate", self._h, ctypes.byref(field), ctypes.byref(cam), w, h,
+             num_points, seed, _stream_ptr(stream))
+
+    def data(self, max_points) -> np.ndarray:
+        out = np.empty((max_points, 4), np.float32)
+        call("re_nsdf_get_data", self._h, out.ctypes.data, max_points)
+        return out
+
+    def train(self, steps, batch=65536, lr=1e-3, stream=None) -> np.ndarray:
+        loss = np.empty(steps, np.float32)
+        call("re_nsdf_train", self._h, steps, batch, lr, loss.ctypes.data, _stream_ptr(stream))
+        return loss
+
+    def loss_grad(self, xyzl, stream=None):
+        import torch
+
+        n = xyzl.shape[0]
+        g = torch.empty(self.num_params, dtype=torch.float32, device="cuda")
+        pred = torch.empty(n, dtype=torch.float32, device="cuda")
+        call("re_nsdf_loss_grad", self._h, _dptr(xyzl), n, _dptr(g), _dptr(pred),
+             _stream_ptr(stream))
+        return g, pred
+
+    def eval(self, pts, out=None, stream=None):
+        import torch
+
+        n = pts.shape[0]
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device="cuda")
+        call("re_nsdf_eval", self._h, _dptr(pts), n, _dptr(out), _stream_ptr(stream))
+        return out
+
+    def eval_reference(self, pts, out=None, stream=None):
+        import torch
+
+        n = pts.shape[0]
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device="cuda")
+        call("re_nsdf_eval_reference", self._h, _dptr(pts), n, _dptr(out), _stream_ptr(stream))
+        return out
+
+    def lipschitz(self, samples=200000, h=1e-2, stream=None) -> float:
+        v = ctypes.c_float()
+        call("re_nsdf_lipschitz", self._h, samples, h, ctypes.byref(v), _stream_ptr(stream))
+        return float(v.value)
+
+    def trace(self, field, tp, cam, w, h, out=None, stream=None):
+        import torch
+
+        if out is None:
+            out = torch.empty((h * w, 8), dtype=torch.int32, device="cuda")
+        call("re_nsdf_trace", self._h, ctypes.byref(field), ctypes.byref(tp), ctypes.byref(cam),
+             w, h, _dptr(out), _stream_ptr(stream))
+        return out
+
+    def trace_status(self):
+        n = ctypes.c_uint32()
+        e = ctypes.c_int()
+        call("re_nsdf_trace_status", self._h, ctypes.byref(n), ctypes.byref(e))
+        return int(n.value), int(e.value)
+
+    def save(self, path: str):
+        call("re_nsdf_save", self._h, path.encode())
+
+    def load(self, path: str):
+        call("re_nsdf_load", self._h, path.encode())

@@ -1,0 +1,1564 @@
+// Neural SDF surrogate of the volumetric terrain (config 3 of the path).
+//
+// The reference has no learned component.  The network stands in for the
+// fBm terrain density (sdf_functions.cuh:147-206, d(p) = p.y - 3 fBm(p/4) in
+// the configs) during sphere tracing; the exact field stays the judge and
+// finishes every hit (sphere_tracing.cuh:183-216 restated in re_noise.cu).
+//
+//   data      k_nsdf_data: 50% points uniform in the view box, 50% near the
+//             surface (exact-traced camera hits + N(0, 0.02) offsets),
+//             labelled by the exact field's first-order distance d / |grad d|
+//   training  hand-written SIMT FP32 kernels with BF16-rounded weights and
+//             activations (the inference precision): k_fwd_first, k_fwd,
+//             k_fwd_head (L1 loss), k_bwd, k_reduce, k_adam; one step is
+//             captured once in a CUDA graph and replayed
+//   inference tcgen05 (sm_100a): 128-point tiles, BF16 operands in shared
+//             memory (K-major canonical layout, no swizzle), FP32
+//             accumulators in tensor memory, one elected thread issues the
+//             MMAs and commits to an mbarrier; softplus epilogue from TMEM
+//   tracing   k_nsdf_march (persistent, lane refill) steps by the network's
+//             distance scaled by its measured Lipschitz bound until it is
+//             within `switch_dist` of the surface, then k_sdf_refine finishes
+//             the ray with exact-field steps and the exact normal.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "re_common.hpp"
+#include "re_noise.cuh"
+#include "re_nsdf.cuh"
+
+namespace re {
+namespace nsdf {
+
+// ------------------------------------------------------------ shared
+struct FieldDev {
+  uint32_t octaves, max_steps;
+  float scale, amp, step_factor, eps, tmax;
+};
+
+__device__ __forceinline__ uint32_t mix32(uint32_t a, uint32_t b, uint32_t c) {
+  return hash_u32(a, b, c);
+}
+__device__ __forceinline__ float u01(uint32_t h) { return (float)(h >> 8) * 5.9604644775390625e-08f; }
+
+// ------------------------------------------------------ data generation
+__global__ void __launch_bounds__(256) k_nsdf_data(PermTable perm, FieldDev f, CamDev cam,
+                                                   uint32_t w, uint32_t h, float3 bmin, float3 bmax,
+                                                   uint32_t n, uint32_t seed,
+                                                   float4* __restrict__ out) {
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float px = 0.f, py = 0.f, pz = 0.f;
+    bool placed = false;
+    if (i & 1u) {
+      // near-surface sample: an exact-traced camera hit plus N(0, 0.02) per axis
+      uint32_t pix = mix32(seed, i, 11u) % (w * h);
+      V3 o, d;
+      generate_ray(cam, w, h, pix % w, pix / w, o, d);
+      float t = 0.f;
+      for (uint32_t s = 0; s < f.max_steps; ++s) {
+        V3 p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+        float dist = terrain_density(P, p, f.octaves, f.scale, f.amp);
+        if (dist < f.eps) {
+          float u1 = fmaxf(u01(mix32(seed, i, 12u)), 1e-7f), u2 = u01(mix32(seed, i, 13u));
+          float u3 = fmaxf(u01(mix32(seed, i, 14u)), 1e-7f), u4 = u01(mix32(seed, i, 15u));
+          float r1 = sqrtf(-2.f * __logf(u1)), r2 = sqrtf(-2.f * __logf(u3));
+          float s1, c1, s2, c2;
+          __sincosf(6.28318531f * u2, &s1, &c1);
+          __sincosf(6.28318531f * u4, &s2, &c2);
+          px = p.x + 0.02f * r1 * c1;
+          py = p.y + 0.02f * r1 * s1;
+          pz = p.z + 0.02f * r2 * c2;
+          placed = px >= bmin.x && px <= bmax.x && py >= bmin.y && py <= bmax.y &&
+                   pz >= bmin.z && pz <= bmax.z;
+          break;
+        }
+        t = __fmaf_rn(f.step_factor, dist, t);
+        if (t > f.tmax) break;
+      }
+    }
+    if (!placed) {
+      px = bmin.x + (bmax.x - bmin.x) * u01(mix32(seed, i, 1u));
+      py = bmin.y + (bmax.y - bmin.y) * u01(mix32(seed, i, 2u));
+      pz = bmin.z + (bmax.z - bmin.z) * u01(mix32(seed, i, 3u));
+    }
+    // label: first-order distance d / |grad d| of the exact field, clipped
+    const float e = 1e-3f;
+    float d0 = terrain_density(P, v3(px, py, pz), f.octaves, f.scale, f.amp);
+    float gx = terrain_density(P, v3(px + e, py, pz), f.octaves, f.scale, f.amp) -
+               terrain_density(P, v3(px - e, py, pz), f.octaves, f.scale, f.amp);
+    float gy = terrain_density(P, v3(px, py + e, pz), f.octaves, f.scale, f.amp) -
+               terrain_density(P, v3(px, py - e, pz), f.octaves, f.scale, f.amp);
+    float gz = terrain_density(P, v3(px, py, pz + e), f.octaves, f.scale, f.amp) -
+               terrain_density(P, v3(px, py, pz - e), f.octaves, f.scale, f.amp);
+    float g = sqrtf(gx * gx + gy * gy + gz * gz) / (2.f * e);
+    float label = d0 / fmaxf(g, 0.25f);
+    label = fminf(fmaxf(label, -4.f), 4.f);
+    out[i] = make_float4(px, py, pz, label);
+  }
+}
+
+// ------------------------------------------------------------- training
+// Activations are stored row-major [B][64] (A = BF16-rounded softplus(Z));
+// the features X0 [B][128].  GEMM tiles: 64 rows x 64 outputs per block of
+// 256 threads, 4x4 outputs per thread, operands staged in shared memory.
+constexpr int kRowsFwd = 64;
+constexpr int kRowsBwd = 512;  // rows per backward block (partial weight grads)
+constexpr size_t kFwdFirstSmem = (size_t)(kHidden + kRowsFwd) * (kIn + 1) * 4;
+template <int K>
+constexpr size_t bwd_smem() {
+  return (size_t)(kRowsFwd * (kHidden + 1) + kRowsFwd * (K + 1) + kHidden * (K + 1)) * 4;
+}
+
+struct TrainBufs {
+  float* x0;      // [B][128]
+  float* z[4];    // [B][64] pre-activations
+  float* a[4];    // [B][64] activations (BF16-rounded)
+  float* da;      // [B][64] gradient w.r.t. the current layer's output
+  float* da2;     // [B][64]
+  float* label;   // [B]
+  float* part;    // [nbwd][kNumParams] partial gradients (layers 1-4)
+  float* part_head;  // [nfwd][kHidden + 1] partial gradients of w5, b5
+  float* part_loss;  // [nfwd]
+};
+
+// features of point `p` for row r of a block: thread part 0 -> chain 0, part
+// 1 -> chain 1, part 2 -> q and zero padding
+__device__ __forceinline__ void features_part(const InputMap& m, float px, float py, float pz,
+                                              int part, float* row /* 128 */) {
+  float q[3];
+  normalise(m, px, py, pz, q);
+  if (part < 2) {
+    float v[48];
+    chain_features(m, q, part, v);
+#pragma unroll
+    for (int i = 0; i < 48; ++i) row[part * 48 + i] = bf16_round(v[i]);
+  } else if (part == 2) {
+    row[96] = bf16_round(q[0]);
+    row[97] = bf16_round(q[1]);
+    row[98] = bf16_round(q[2]);
+#pragma unroll
+    for (int i = 99; i < 128; ++i) row[i] = 0.f;
+  }
+}
+
+// Layer 1: sample (or take) the batch, compute features, Z1 = X0 W1^T + b1.
+__global__ void __launch_bounds__(256) k_fwd_first(InputMap m, const float4* __restrict__ data,
+                                                   uint32_t npts, const uint32_t* __restrict__ step_ctr,
+                                                   uint32_t seed, int direct,
+                                                   const float* __restrict__ params, TrainBufs tb) {
+  extern __shared__ float fsm[];
+  float(*Ws)[kIn + 1] = reinterpret_cast<float(*)[kIn + 1]>(fsm);
+  float(*Xs)[kIn + 1] = reinterpret_cast<float(*)[kIn + 1]>(fsm + kHidden * (kIn + 1));
+  int t = threadIdx.x;
+  for (int i = t; i < kHidden * kIn; i += 256) Ws[i / kIn][i % kIn] = bf16_round(params[OFF_W1 + i]);
+  uint32_t row0 = blockIdx.x * kRowsFwd;
+  {
+    int r = t >> 2, part = t & 3;
+    uint32_t b = row0 + r;
+    uint32_t idx = direct ? b : mix32(seed, *step_ctr, b) % npts;
+    float4 pt = __ldg(&data[idx]);
+    features_part(m, pt.x, pt.y, pt.z, part, &Xs[r][0]);
+    if (part == 3) tb.label[b] = pt.w;
+  }
+  __syncthreads();
+  for (int i = t; i < kRowsFwd * kIn; i += 256) tb.x0[(size_t)row0 * kIn + i] = Xs[i / kIn][i % kIn];
+  int ty = t >> 4, tx = t & 15;
+  float acc[4][4] = {};
+  for (int k = 0; k < kIn; ++k) {
+    float a[4], w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = Xs[ty * 4 + i][k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[j] = Ws[tx * 4 + j][k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], w[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int c = tx * 4 + j;
+      float z = acc[i][j] + params[OFF_B1 + c];
+      size_t o = (size_t)(row0 + ty * 4 + i) * kHidden + c;
+      tb.z[0][o] = z;
+      tb.a[0][o] = bf16_round(softplus_approx(z));
+    }
+}
+
+// Layers 2-4: Z = A W^T + b.
+__global__ void __launch_bounds__(256) k_fwd(int layer, const float* __restrict__ params,
+                                             TrainBufs tb) {
+  __shared__ float Ws[kHidden][kHidden + 1];
+  __shared__ float As[kRowsFwd][kHidden + 1];
+  int t = threadIdx.x;
+  const float* W = params + w_off(layer);
+  const float* bias = params + b_off(layer);
+  for (int i = t; i < kHidden * kHidden; i += 256) Ws[i / kHidden][i % kHidden] = bf16_round(W[i]);
+  uint32_t row0 = blockIdx.x * kRowsFwd;
+  const float* A = tb.a[layer - 1];
+  for (int i = t; i < kRowsFwd * kHidden; i += 256)
+    As[i / kHidden][i % kHidden] = A[(size_t)row0 * kHidden + i];
+  __syncthreads();
+  int ty = t >> 4, tx = t & 15;
+  float acc[4][4] = {};
+  for (int k = 0; k < kHidden; ++k) {
+    float a[4], w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[j] = Ws[tx * 4 + j][k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], w[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int c = tx * 4 + j;
+      float z = acc[i][j] + bias[c];
+      size_t o = (size_t)(row0 + ty * 4 + i) * kHidden + c;
+      tb.z[layer][o] = z;
+      tb.a[layer][o] = bf16_round(softplus_approx(z));
+    }
+}
+
+// Head: out = A4 w5 + b5, L1 loss, dOut = sign(out - label) / B, dA4 =
+// dOut * w5, partial gradients of w5 and b5 and the loss per block.
+__global__ void __launch_bounds__(256) k_fwd_head(const float* __restrict__ params, uint32_t batch,
+                                                  TrainBufs tb, float* __restrict__ out_pred) {
+  __shared__ float red[kRowsFwd][kHidden + 1];
+  __shared__ float g_s[kRowsFwd];
+  __shared__ float loss_s[kRowsFwd];
+  int t = threadIdx.x;
+  uint32_t row0 = blockIdx.x * kRowsFwd;
+  int r = t >> 2, part = t & 3;  // 4 threads per row, 16 columns each
+  size_t base = (size_t)(row0 + r) * kHidden;
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    int c = part * 16 + j;
+    s = __fmaf_rn(tb.a[3][base + c], bf16_round(params[OFF_W5 + c]), s);
+  }
+  s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
+  s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
+  float pred = s + params[OFF_B5];
+  float diff = pred - tb.label[row0 + r];
+  float g = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) / (float)batch;
+  if (part == 0) {
+    g_s[r] = g;
+    loss_s[r] = fabsf(diff);
+    if (out_pred) out_pred[row0 + r] = pred;
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    int c = part * 16 + j;
+    tb.da[base + c] = g * bf16_round(params[OFF_W5 + c]);
+    red[r][c] = g * tb.a[3][base + c];
+  }
+  __syncthreads();
+  float* ph = tb.part_head + (size_t)blockIdx.x * (kHidden + 2);
+  if (t < kHidden) {
+    float acc = 0.f;
+    for (int i = 0; i < kRowsFwd; ++i) acc += red[i][t];
+    ph[t] = acc;
+  } else if (t == kHidden) {
+    float acc = 0.f;
+    for (int i = 0; i < kRowsFwd; ++i) acc += g_s[i];
+    ph[kHidden] = acc;
+  } else if (t == kHidden + 1) {
+    float acc = 0.f;
+    for (int i = 0; i < kRowsFwd; ++i) acc += loss_s[i];
+    ph[kHidden + 1] = acc;
+  }
+}
+
+// Backward through hidden layer `layer` (0-based): dZ = dA * softplus'(Z),
+// partial dW = dZ^T A_prev and db = sum dZ over this block's 512 rows, and
+// dA_prev = dZ W (layers > 0).
+template <int K>
+__global__ void __launch_bounds__(256) k_bwd(int layer, const float* __restrict__ params,
+                                             TrainBufs tb, const float* __restrict__ da_in,
+                                             float* __restrict__ da_out) {
+  extern __shared__ float bsm[];
+  float(*dZs)[kHidden + 1] = reinterpret_cast<float(*)[kHidden + 1]>(bsm);
+  float(*As)[K + 1] = reinterpret_cast<float(*)[K + 1]>(bsm + kRowsFwd * (kHidden + 1));
+  float(*Ws)[K + 1] =
+      reinterpret_cast<float(*)[K + 1]>(bsm + kRowsFwd * (kHidden + 1) + kRowsFwd * (K + 1));
+  int t = threadIdx.x;
+  const float* W = params + w_off(layer);
+  if (layer > 0)
+    for (int i = t; i < kHidden * K; i += 256) Ws[i / K][i % K] = bf16_round(W[i]);
+  const float* Z = tb.z[layer];
+  const float* Aprev = layer > 0 ? tb.a[layer - 1] : tb.x0;
+  int ty = t >> 4, tx = t & 15;
+  constexpr int KC = K / 16;  // weight-gradient columns per thread
+  float gw[4][KC] = {};
+  float gb = 0.f;
+  for (int chunk = 0; chunk < kRowsBwd / kRowsFwd; ++chunk) {
+    uint32_t row0 = blockIdx.x * kRowsBwd + chunk * kRowsFwd;
+    __syncthreads();
+    for (int i = t; i < kRowsFwd * kHidden; i += 256) {
+      size_t o = (size_t)row0 * kHidden + i;
+      dZs[i / kHidden][i % kHidden] = da_in[o] * softplus_approx_deriv(Z[o]);
+    }
+    for (int i = t; i < kRowsFwd * K; i += 256) As[i / K][i % K] = Aprev[(size_t)row0 * K + i];
+    __syncthreads();
+    // weight gradient: rows n = ty*4+i, columns k = tx*KC + j
+    for (int r = 0; r < kRowsFwd; ++r) {
+      float dz[4], a[KC];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dz[i] = dZs[r][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) a[j] = As[r][tx * KC + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < KC; ++j) gw[i][j] = __fmaf_rn(dz[i], a[j], gw[i][j]);
+    }
+    if (t < kHidden)
+      for (int r = 0; r < kRowsFwd; ++r) gb += dZs[r][t];
+    if (layer > 0) {
+      // dA_prev = dZ W : rows ty*4+i, columns tx*4+j (K = 64)
+      float acc[4][4] = {};
+      for (int n = 0; n < kHidden; ++n) {
+        float dz[4], w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) dz[i] = dZs[ty * 4 + i][n];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) w[j] = Ws[n][tx * 4 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(dz[i], w[j], acc[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          da_out[(size_t)(row0 + ty * 4 + i) * K + tx * 4 + j] = acc[i][j];
+    }
+  }
+  float* pp = tb.part + (size_t)blockIdx.x * kNumParams;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < KC; ++j) pp[w_off(layer) + (ty * 4 + i) * K + tx * KC + j] = gw[i][j];
+  if (t < kHidden) pp[b_off(layer) + t] = gb;
+}
+
+// grad[p] = sum of the partial gradients; the loss of the step is appended
+// to loss_hist.
+__global__ void k_reduce(TrainBufs tb, uint32_t nbwd, uint32_t nfwd, float* __restrict__ grad,
+                         float* __restrict__ loss_hist, const uint32_t* __restrict__ step_ctr,
+                         uint32_t batch) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < (uint32_t)OFF_W5) {
+    float s = 0.f;
+    for (uint32_t b = 0; b < nbwd; ++b) s += tb.part[(size_t)b * kNumParams + p];
+    grad[p] = s;
+  } else if (p < (uint32_t)kNumParams + 1) {
+    uint32_t c = p - OFF_W5;  // 0..63 w5, 64 b5, 65 loss
+    float s = 0.f;
+    for (uint32_t b = 0; b < nfwd; ++b) s += tb.part_head[(size_t)b * (kHidden + 2) + c];
+    if (p < (uint32_t)kNumParams)
+      grad[p] = s;
+    else if (loss_hist)
+      loss_hist[*step_ctr] = s / (float)batch;
+  }
+}
+
+__global__ void k_adam(float* __restrict__ params, const float* __restrict__ grad,
+                       float* __restrict__ m, float* __restrict__ v, uint32_t* __restrict__ step_ctr,
+                       float lr) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t step = *step_ctr + 1;
+  if (p < (uint32_t)kNumParams) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    float g = grad[p];
+    float mm = b1 * m[p] + (1.f - b1) * g;
+    float vv = b2 * v[p] + (1.f - b2) * g * g;
+    m[p] = mm;
+    v[p] = vv;
+    float mh = mm / (1.f - powf(b1, (float)step));
+    float vh = vv / (1.f - powf(b2, (float)step));
+    params[p] -= lr * mh / (sqrtf(vh) + eps);
+  }
+}
+
+__global__ void k_step_inc(uint32_t* step_ctr) { *step_ctr += 1; }
+
+// ------------------------------------------------ tensor-core inference
+// Canonical K-major BF16 layout without swizzle: 8 rows x 8 k-elements
+// (16 B per row) form a 128-byte core matrix; core matrices follow each
+// other along K every 128 B (LBO) and along rows every K*16 B (SBO).
+__host__ __device__ __forceinline__ uint32_t canon_off(uint32_t row, uint32_t k, uint32_t K) {
+  return (row >> 3) * (K * 16u) + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// Packed inference weights: W1 (64x128), W2..W4 (64x64) in the canonical
+// layout, then FP32 b1..b4, w5 (BF16-rounded) and b5.
+constexpr uint32_t kPackW1 = kHidden * kIn * 2;            // 16384
+constexpr uint32_t kPackWh = kHidden * kHidden * 2;        // 8192
+constexpr uint32_t kPackWBytes = kPackW1 + 3 * kPackWh;    // 40960
+constexpr uint32_t kPackFloats = 4 * kHidden + kHidden + 1;
+constexpr uint32_t kPackBytes = kPackWBytes + kPackFloats * 4;
+
+__global__ void k_pack(const float* __restrict__ params, unsigned char* __restrict__ pack) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (uint32_t)(kHidden * kIn)) {
+    uint32_t n = i / kIn, k = i % kIn;
+    *reinterpret_cast<__nv_bfloat16*>(pack + canon_off(n, k, kIn)) =
+        __float2bfloat16_rn(params[OFF_W1 + i]);
+  }
+  if (i < (uint32_t)(3 * kHidden * kHidden)) {
+    uint32_t l = i / (kHidden * kHidden), e = i % (kHidden * kHidden);
+    uint32_t n = e / kHidden, k = e % kHidden;
+    *reinterpret_cast<__nv_bfloat16*>(pack + kPackW1 + l * kPackWh + canon_off(n, k, kHidden)) =
+        __float2bfloat16_rn(params[w_off(1 + l) + e]);
+  }
+  if (i < kPackFloats) {
+    float* f = reinterpret_cast<float*>(pack + kPackWBytes);
+    float v;
+    if (i < 4u * kHidden)
+      v = params[b_off(i / kHidden) + i % kHidden];
+    else if (i < 5u * kHidden)
+      v = bf16_round(params[OFF_W5 + i - 4 * kHidden]);
+    else
+      v = params[OFF_B5];
+    f[i] = v;
+  }
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo_bytes) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+         ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: D FP32, A/B BF16, both K-major, N = 64, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_addr(bar))
+      : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false if the bound was reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t a = smem_addr(bar);
+  for (uint32_t i = 0; i < (1u << 24); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// Shared memory of one inference CTA (256 threads = 2 threads per row).
+struct __align__(1024) TcSmem {
+  unsigned char w[kPackWBytes];  // W1..W4, canonical
+  unsigned char x[128 * kIn * 2];  // layer input, canonical (K = 128 or 64)
+  float bias[4][kHidden];
+  float w5[kHidden];
+  float b5;
+  float half[2][128];   // partial head sums per row
+  float p[128][4];      // point (x, y, z, live) per row
+  float dist[128];
+  uint64_t bar;
+  uint32_t tmem;
+  int error;
+};
+
+constexpr uint32_t kTmemCols = 64;
+
+// One 128-point tile through the network.  Called by all 256 threads; row
+// r = 32*(warp%4) + lane, column half ch = warp / 4.  Inputs in s.p, output
+// in s.dist.  Returns false if an MMA did not complete within the bound.
+__device__ __forceinline__ bool mlp_tile(TcSmem& s, const InputMap& m, uint32_t& phase) {
+  int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int row = 32 * (warp & 3) + lane, ch = warp >> 2;
+  // features: ch 0 -> chain 0 (chunks 0..5), ch 1 -> chain 1 (6..11) + q (12..15)
+  {
+    float q[3];
+    normalise(m, s.p[row][0], s.p[row][1], s.p[row][2], q);
+    float v[48];
+    chain_features(m, q, ch, v);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      uint4 u;
+      u.x = pack_bf16x2(v[c * 8 + 0], v[c * 8 + 1]);
+      u.y = pack_bf16x2(v[c * 8 + 2], v[c * 8 + 3]);
+      u.z = pack_bf16x2(v[c * 8 + 4], v[c * 8 + 5]);
+      u.w = pack_bf16x2(v[c * 8 + 6], v[c * 8 + 7]);
+      *reinterpret_cast<uint4*>(s.x + canon_off(row, (ch * 6 + c) * 8, kIn)) = u;
+    }
+    if (ch == 1) {
+      uint4 u;
+      u.x = pack_bf16x2(q[0], q[1]);
+      u.y = pack_bf16x2(q[2], 0.f);
+      u.z = 0u;
+      u.w = 0u;
+      *reinterpret_cast<uint4*>(s.x + canon_off(row, 96, kIn)) = u;
+      uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+      for (int c = 13; c < 16; ++c) *reinterpret_cast<uint4*>(s.x + canon_off(row, c * 8, kIn)) = zero;
+    }
+  }
+  bool ok = true;
+  float act[32];
+#pragma unroll 1
+  for (int layer = 0; layer < 4; ++layer) {
+    uint32_t K = layer == 0 ? kIn : kHidden;
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (tid == 0) {
+      uint32_t xa = smem_addr(s.x);
+      uint32_t wa = smem_addr(s.w + (layer == 0 ? 0u : kPackW1 + (layer - 1) * kPackWh));
+#pragma unroll 1
+      for (uint32_t kk = 0; kk < K / 16; ++kk)
+        mma_bf16(s.tmem, umma_desc(xa + kk * 256u, K * 16u), umma_desc(wa + kk * 256u, K * 16u),
+                 kk > 0 ? 1u : 0u);
+      mma_commit(&s.bar);
+    }
+    ok = mbar_wait(&s.bar, phase) && ok;
+    phase ^= 1u;
+    fence_after();
+    tmem_ld32(s.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * ch), act);
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      act[j] = bf16_round(softplus_approx(act[j] + s.bias[layer][32 * ch + j]));
+    if (layer < 3) {
+      // next layer's input (K = 64): this thread's 32 columns = 4 chunks
+      fence_before();
+      __syncthreads();  // every thread has read its accumulators; x is free
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        uint4 u;
+        u.x = pack_bf16x2(act[c * 8 + 0], act[c * 8 + 1]);
+        u.y = pack_bf16x2(act[c * 8 + 2], act[c * 8 + 3]);
+        u.z = pack_bf16x2(act[c * 8 + 4], act[c * 8 + 5]);
+        u.w = pack_bf16x2(act[c * 8 + 6], act[c * 8 + 7]);
+        *reinterpret_cast<uint4*>(s.x + canon_off(row, 32 * ch + c * 8, kHidden)) = u;
+      }
+    }
+  }
+  float d = 0.f;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) d = __fmaf_rn(act[j], s.w5[32 * ch + j], d);
+  s.half[ch][row] = d;
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (ch == 0) s.dist[row] = s.half[0][row] + s.half[1][row] + s.b5;
+  // block-uniform result, so every thread leaves its loop on the same trip
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+__device__ __forceinline__ void tc_setup(TcSmem& s, const unsigned char* __restrict__ pack) {
+  int tid = threadIdx.x;
+  for (uint32_t i = tid; i < kPackWBytes / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(s.w)[i] = __ldg(reinterpret_cast<const uint4*>(pack) + i);
+  const float* f = reinterpret_cast<const float*>(pack + kPackWBytes);
+  for (uint32_t i = tid; i < 4 * kHidden; i += blockDim.x) s.bias[i / kHidden][i % kHidden] = f[i];
+  for (uint32_t i = tid; i < kHidden; i += blockDim.x) s.w5[i] = f[4 * kHidden + i];
+  if (tid == 0) {
+    s.b5 = f[5 * kHidden];
+    s.error = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s.bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((tid >> 5) == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s.tmem)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+}
+
+__device__ __forceinline__ void tc_teardown(TcSmem& s) {
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem),
+                 "r"(kTmemCols));
+}
+
+// Batch evaluation: out[i] = network(pts[i]).
+__global__ void __launch_bounds__(256) k_tc_eval(InputMap m, const unsigned char* __restrict__ pack,
+                                                 const float* __restrict__ pts, uint32_t n,
+                                                 float* __restrict__ out, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  tc_setup(s, pack);
+  uint32_t phase = 0;
+  int tid = threadIdx.x;
+  uint32_t tiles = (n + 127) / 128;
+  bool ok = true;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    if (tid < 128) {
+      uint32_t i = tile * 128 + tid;
+      bool live = i < n;
+      s.p[tid][0] = live ? pts[3 * (size_t)i] : 0.f;
+      s.p[tid][1] = live ? pts[3 * (size_t)i + 1] : 0.f;
+      s.p[tid][2] = live ? pts[3 * (size_t)i + 2] : 0.f;
+    }
+    __syncthreads();
+    ok = mlp_tile(s, m, phase);
+    if (tid < 128) {
+      uint32_t i = tile * 128 + tid;
+      if (i < n) out[i] = s.dist[tid];
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  tc_teardown(s);
+}
+
+// Reference evaluation with the training arithmetic (SIMT FP32, BF16-rounded
+// weights and activations), one thread per point.
+__global__ void __launch_bounds__(128) k_ref_eval(InputMap m, const float* __restrict__ params,
+                                                  const float* __restrict__ pts, uint32_t n,
+                                                  float* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x[kIn];
+  float q[3];
+  normalise(m, pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2], q);
+  float v[48];
+  chain_features(m, q, 0, v);
+  for (int k = 0; k < 48; ++k) x[k] = bf16_round(v[k]);
+  chain_features(m, q, 1, v);
+  for (int k = 0; k < 48; ++k) x[48 + k] = bf16_round(v[k]);
+  x[96] = bf16_round(q[0]);
+  x[97] = bf16_round(q[1]);
+  x[98] = bf16_round(q[2]);
+  for (int k = 99; k < kIn; ++k) x[k] = 0.f;
+  float h[kHidden], h2[kHidden];
+  for (int c = 0; c < kHidden; ++c) {
+    float z = 0.f;
+    for (int k = 0; k < kIn; ++k) z = __fmaf_rn(x[k], bf16_round(params[OFF_W1 + c * kIn + k]), z);
+    h[c] = bf16_round(softplus_approx(z + params[OFF_B1 + c]));
+  }
+  for (int l = 1; l < 4; ++l) {
+    for (int c = 0; c < kHidden; ++c) {
+      float z = 0.f;
+      for (int k = 0; k < kHidden; ++k)
+        z = __fmaf_rn(h[k], bf16_round(params[w_off(l) + c * kHidden + k]), z);
+      h2[c] = bf16_round(softplus_approx(z + params[b_off(l) + c]));
+    }
+    for (int c = 0; c < kHidden; ++c) h[c] = h2[c];
+  }
+  float d = 0.f;
+  for (int c = 0; c < kHidden; ++c) d = __fmaf_rn(h[c], bf16_round(params[OFF_W5 + c]), d);
+  out[i] = d + params[OFF_B5];
+}
+
+// ------------------------------------------------------------- tracing
+struct MarchDev {
+  float alpha;        // step = alpha * network distance (1 / Lipschitz bound)
+  float switch_dist;  // hand over to the exact field below this distance
+  float min_step;     // floor of a network step
+  float tmax;
+  uint32_t max_steps;  // network steps before handing over regardless
+};
+
+// Neural phase.  Rows are ray slots; a warp of row owners (warps 0-3) refills
+// its idle slots from the pixel cursor (claim order = 8x4 tiles).  Rays that
+// come within switch_dist of the surface (or exhaust their network steps)
+// are appended to the refinement queue {pixel, t, steps}; rays that leave
+// [0, tmax] are written as misses.
+__global__ void __launch_bounds__(256) k_nsdf_march(InputMap m, const unsigned char* __restrict__ pack,
+                                                    MarchDev md, CamDev cam, uint32_t w, uint32_t h,
+                                                    uint32_t* __restrict__ counters,
+                                                    uint4* __restrict__ queue,
+                                                    float4* __restrict__ out,
+                                                    int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ int any_live;
+  tc_setup(s, pack);
+  uint32_t phase = 0;
+  int tid = threadIdx.x, lane = tid & 31;
+  uint32_t tiles_x = (w + 7) / 8;
+  uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
+  // ray state lives in the row owners (threads 0..127)
+  bool live = false, exhausted = false;
+  uint32_t pix = 0, steps = 0;
+  V3 o = {0, 0, 0}, d = {0, 0, 1};
+  float t = 0.f;
+  bool ok = true;
+  for (uint32_t guard = 0; guard < (1u << 24) && ok; ++guard) {
+    if (tid == 0) any_live = 0;
+    __syncthreads();
+    if (tid < 128) {
+      uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
+      uint32_t nidle = __popc(idle);
+      if (!exhausted && (nidle >= 8u || nidle == 32u)) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&counters[0], nidle);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base + nidle >= total) exhausted = true;
+        if (!live) {
+          uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+          uint32_t tile = i >> 5, l = i & 31u;
+          uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
+          if (i < total && x < w && y < h) {
+            generate_ray(cam, w, h, x, y, o, d);
+            pix = y * w + x;
+            t = 0.f;
+            steps = 0;
+            live = true;
+          }
+        }
+      }
+      V3 p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+      s.p[tid][0] = p.x;
+      s.p[tid][1] = p.y;
+      s.p[tid][2] = p.z;
+      uint32_t live_b = __ballot_sync(0xFFFFFFFFu, live);
+      if (lane == 0 && (live_b != 0u || !exhausted)) atomicOr(&any_live, 1);
+    }
+    __syncthreads();
+    if (!any_live) break;
+    ok = mlp_tile(s, m, phase);
+    if (tid < 128 && live) {
+      float dn = s.dist[tid];
+      ++steps;
+      if (dn < md.switch_dist || steps >= md.max_steps) {
+        uint32_t slot = atomicAdd(&counters[1], 1u);
+        queue[slot] = make_uint4(pix, __float_as_uint(t), steps, 0u);
+        live = false;
+      } else {
+        t += fmaxf(md.alpha * dn, md.min_step);
+        if (t > md.tmax) {
+          out[2 * (size_t)pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+          out[2 * (size_t)pix + 1] =
+              make_float4(0.f, 0.f, __uint_as_float(steps), __uint_as_float(0u));
+          live = false;
+        }
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  tc_teardown(s);
+}
+
+// Exact phase: continue each queued ray from its t with the exact field
+// (t += step_factor * d, hit when d < eps), then the central-difference
+// normal, as the exact tracer does.  Same state machine and lane refill as
+// k_sdf; the step count reported is network steps + exact steps.
+__global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f,
+                                                    uint32_t exact_max_steps, CamDev cam,
+                                                    uint32_t w, uint32_t h,
+                                                    const uint4* __restrict__ queue,
+                                                    uint32_t* __restrict__ counters,
+                                                    float4* __restrict__ out) {
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t total = counters[1];
+  bool live = false, exhausted = false;
+  uint32_t pix = 0, steps = 0, base_steps = 0, phase = 0;
+  V3 o = {0, 0, 0}, d = {0, 0, 1}, p = {0, 0, 0};
+  float t = 0.f, delta = 0.f, nx = 0.f, ny = 0.f, nz = 0.f, plus = 0.f;
+  for (;;) {
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && (nidle >= 4u || nidle == 32u)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&counters[2], nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= total) exhausted = true;
+      if (!live) {
+        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+        if (i < total) {
+          uint4 q = queue[i];
+          pix = q.x;
+          generate_ray(cam, w, h, pix % w, pix / w, o, d);
+          t = __uint_as_float(q.y);
+          base_steps = q.z;
+          steps = 0;
+          phase = 0;
+          live = true;
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, live) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!live) continue;
+    V3 qp;
+    if (phase == 0) {
+      qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+    } else {
+      float sd = (phase & 1u) ? delta : -delta;
+      qp = p;
+      if (phase <= 2) qp.x = p.x + sd;
+      else if (phase <= 4) qp.y = p.y + sd;
+      else qp.z = p.z + sd;
+    }
+    float v = terrain_density(P, qp, f.octaves, f.scale, f.amp);
+    uint32_t status = 3;
+    if (phase == 0) {
+      ++steps;
+      if (v < f.eps) {
+        p = qp;
+        delta = 0.002f * t;
+        phase = 1;
+      } else {
+        t = __fmaf_rn(f.step_factor, v, t);
+        if (t > f.tmax) status = 0;
+        else if (steps >= exact_max_steps) status = 2;
+      }
+    } else {
+      if (phase & 1u) {
+        plus = v;
+      } else {
+        float diff = plus - v;
+        if (phase == 2) nx = diff;
+        else if (phase == 4) ny = diff;
+        else nz = diff;
+      }
+      if (phase == 6) status = 1;
+      else ++phase;
+    }
+    if (status != 3) {
+      float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1;
+      uint32_t total_steps = base_steps + steps;
+      if (status == 1) {
+        V3 n = normalize(v3(nx, ny, nz));
+        r0 = make_float4(p.x, p.y, p.z, n.x);
+        r1 = make_float4(n.y, n.z, __uint_as_float(total_steps), __uint_as_float(status));
+      } else {
+        r1 = make_float4(0.f, 0.f, __uint_as_float(total_steps), __uint_as_float(status));
+      }
+      out[2 * (size_t)pix] = r0;
+      out[2 * (size_t)pix + 1] = r1;
+      live = false;
+    }
+  }
+}
+
+// Lipschitz estimate: max over sample points of the finite-difference
+// gradient norm of the network (points in pts, 4 evaluations each: p, p+hx,
+// p+hy, p+hz laid out by the caller).
+__global__ void k_grad_norm(const float* __restrict__ vals, uint32_t n, float h,
+                            unsigned int* __restrict__ max_bits) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float g = 0.f;
+  if (i < n) {
+    float v0 = vals[4 * (size_t)i];
+    float gx = (vals[4 * (size_t)i + 1] - v0) / h, gy = (vals[4 * (size_t)i + 2] - v0) / h,
+          gz = (vals[4 * (size_t)i + 3] - v0) / h;
+    g = sqrtf(gx * gx + gy * gy + gz * gz);
+  }
+  for (int off = 16; off > 0; off >>= 1) g = fmaxf(g, __shfl_xor_sync(0xFFFFFFFFu, g, off));
+  if ((threadIdx.x & 31u) == 0) atomicMax(max_bits, __float_as_uint(g));
+}
+
+}  // namespace nsdf
+}  // namespace re
+
+// ----------------------------------------------------------------- host
+struct re_nsdf {
+  int device = 0;
+  re::nsdf::InputMap map;
+  uint32_t seed = 1;
+  float* params = nullptr;  // [kNumParams]
+  float* grad = nullptr;
+  float* adam_m = nullptr;
+  float* adam_v = nullptr;
+  unsigned char* pack = nullptr;
+  bool pack_valid = false;
+  uint32_t* step_ctr = nullptr;
+  float4* data = nullptr;
+  uint32_t npts = 0;
+  // training buffers for `batch` rows
+  uint32_t batch = 0;
+  re::nsdf::TrainBufs tb{};
+  float* loss_hist = nullptr;
+  uint32_t loss_cap = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  float graph_lr = -1.f;
+  // tracing scratch
+  uint32_t* counters = nullptr;  // [0] pixel cursor [1] queue size [2] refine cursor
+  uint4* queue = nullptr;
+  size_t queue_cap = 0;
+  int* err = nullptr;
+  float lipschitz = 0.f;
+  uint32_t total_steps_done = 0;
+};
+
+namespace re {
+namespace {
+
+using namespace nsdf;
+
+void free_train(re_nsdf* s) {
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graph_exec = nullptr;
+  s->graph = nullptr;
+  cudaFree(s->tb.x0);
+  for (int l = 0; l < 4; ++l) {
+    cudaFree(s->tb.z[l]);
+    cudaFree(s->tb.a[l]);
+  }
+  cudaFree(s->tb.da);
+  cudaFree(s->tb.da2);
+  cudaFree(s->tb.label);
+  cudaFree(s->tb.part);
+  cudaFree(s->tb.part_head);
+  s->tb = TrainBufs{};
+  s->batch = 0;
+}
+
+re_status alloc_train(re_nsdf* s, uint32_t batch) {
+  if (s->batch == batch) return RE_OK;
+  free_train(s);
+  RE_CUDA(cudaFuncSetAttribute(k_fwd_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kFwdFirstSmem));
+  RE_CUDA(cudaFuncSetAttribute(k_bwd<kHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bwd_smem<kHidden>()));
+  RE_CUDA(cudaFuncSetAttribute(k_bwd<kIn>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bwd_smem<kIn>()));
+  size_t B = batch;
+  RE_CUDA(cudaMalloc(&s->tb.x0, B * kIn * 4));
+  for (int l = 0; l < 4; ++l) {
+    RE_CUDA(cudaMalloc(&s->tb.z[l], B * kHidden * 4));
+    RE_CUDA(cudaMalloc(&s->tb.a[l], B * kHidden * 4));
+  }
+  RE_CUDA(cudaMalloc(&s->tb.da, B * kHidden * 4));
+  RE_CUDA(cudaMalloc(&s->tb.da2, B * kHidden * 4));
+  RE_CUDA(cudaMalloc(&s->tb.label, B * 4));
+  RE_CUDA(cudaMalloc(&s->tb.part, (B / kRowsBwd) * kNumParams * 4));
+  RE_CUDA(cudaMalloc(&s->tb.part_head, (B / kRowsFwd) * (kHidden + 2) * 4));
+  s->batch = batch;
+  return RE_OK;
+}
+
+re_status check(const re_nsdf* s, const char* fn) {
+  if (!s) return fail(RE_ERR_INVALID_ARG, "%s: null model", fn);
+  int dev = -1;
+  RE_CUDA(cudaGetDevice(&dev));
+  if (dev != s->device)
+    return fail(RE_ERR_INVALID_ARG, "%s: model lives on device %d, current device is %d", fn,
+                s->device, dev);
+  return RE_OK;
+}
+
+// One optimisation step on a batch (sampled from s->data, or given points
+// when direct): forward, L1 loss, backward, reduction, optional Adam.
+re_status enqueue_step(re_nsdf* s, const float4* data, uint32_t npts, int direct, float lr,
+                       bool adam, float* pred, cudaStream_t st) {
+  uint32_t B = s->batch;
+  uint32_t nfwd = B / kRowsFwd, nbwd = B / kRowsBwd;
+  k_fwd_first<<<nfwd, 256, kFwdFirstSmem, st>>>(s->map, data, npts, s->step_ctr, s->seed, direct,
+                                                s->params, s->tb);
+  for (int l = 1; l < 4; ++l) k_fwd<<<nfwd, 256, 0, st>>>(l, s->params, s->tb);
+  k_fwd_head<<<nfwd, 256, 0, st>>>(s->params, B, s->tb, pred);
+  // backward: da holds dA4; alternate da / da2
+  float* din = s->tb.da;
+  float* dout = s->tb.da2;
+  for (int l = 3; l >= 1; --l) {
+    k_bwd<kHidden><<<nbwd, 256, bwd_smem<kHidden>(), st>>>(l, s->params, s->tb, din, dout);
+    std::swap(din, dout);
+  }
+  k_bwd<kIn><<<nbwd, 256, bwd_smem<kIn>(), st>>>(0, s->params, s->tb, din, nullptr);
+  k_reduce<<<(kNumParams + 2 + 255) / 256, 256, 0, st>>>(s->tb, nbwd, nfwd, s->grad,
+                                                         adam ? s->loss_hist : nullptr,
+                                                         s->step_ctr, B);
+  if (adam) {
+    k_adam<<<(kNumParams + 255) / 256, 256, 0, st>>>(s->params, s->grad, s->adam_m, s->adam_v,
+                                                     s->step_ctr, lr);
+    k_step_inc<<<1, 1, 0, st>>>(s->step_ctr);
+  }
+  RE_CHECK_LAUNCH("nsdf training step launch");
+  return RE_OK;
+}
+
+re_status ensure_pack(re_nsdf* s, cudaStream_t st) {
+  if (s->pack_valid) return RE_OK;
+  // one thread per element of the largest section (W2..W4: 3 x 64 x 64)
+  constexpr int kPackThreads = 3 * kHidden * kHidden > kHidden * kIn ? 3 * kHidden * kHidden
+                                                                      : kHidden * kIn;
+  k_pack<<<(kPackThreads + 255) / 256, 256, 0, st>>>(s->params, s->pack);
+  RE_CHECK_LAUNCH("nsdf pack launch");
+  s->pack_valid = true;
+  return RE_OK;
+}
+
+constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
+
+template <typename K>
+int tc_grid(K kernel) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, kTcSmemBytes) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  per_sm = std::min(per_sm, 4);  // 4 x 64 TMEM columns of 512
+  return per_sm * sm_count();
+}
+
+CamDev cam_dev(const re_camera& c) {
+  CamBasis b;
+  camera_basis(c, b);
+  CamDev d;
+  d.campos = {b.campos[0], b.campos[1], b.campos[2]};
+  d.middle = {b.middle[0], b.middle[1], b.middle[2]};
+  d.horizontal = {b.horizontal[0], b.horizontal[1], b.horizontal[2]};
+  d.vertical = {b.vertical[0], b.vertical[1], b.vertical[2]};
+  d.focal = b.focal;
+  return d;
+}
+
+PermTable perm_of(uint32_t seed) {
+  uint32_t full[512];
+  perlin_permutation(seed, full);
+  PermTable t;
+  for (int i = 0; i < 512; ++i) t.p[i] = (uint8_t)full[i];
+  return t;
+}
+
+FieldDev field_of(const re_sdf_params& p) {
+  FieldDev f;
+  f.octaves = p.octaves;
+  f.max_steps = p.max_steps;
+  f.scale = p.scale;
+  f.amp = p.amplitude;
+  f.step_factor = p.step_factor;
+  f.eps = p.eps;
+  f.tmax = p.tmax;
+  return f;
+}
+
+re_status check_field(const re_sdf_params* p, const char* fn) {
+  if (!p) return fail(RE_ERR_INVALID_ARG, "%s: null field", fn);
+  if (p->octaves > 32) return fail(RE_ERR_LIMIT, "%s: octaves > 32", fn);
+  if (p->max_steps == 0 || p->max_steps > (1u << 20))
+    return fail(RE_ERR_LIMIT, "%s: max_steps must be in [1, 2^20]", fn);
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API uint32_t re_nsdf_num_params(void) { return (uint32_t)re::nsdf::kNumParams; }
+
+RE_API re_status re_nsdf_box_for_camera(const re_camera* cam, uint32_t w, uint32_t h, float tmax,
+                                        float y_lo, float y_hi, float* box_min, float* box_max) {
+  if (!cam || !box_min || !box_max || w < 2 || h < 2 || !(tmax > 0.f) || !(y_hi > y_lo))
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_box_for_camera: bad arguments");
+  re::CamBasis b;
+  re::camera_basis(*cam, b);
+  double lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) lo[k] = hi[k] = b.campos[k];
+  for (int cx = -1; cx <= 1; cx += 2)
+    for (int cy = -1; cy <= 1; cy += 2) {
+      double dir[3], n = 0;
+      for (int k = 0; k < 3; ++k) {
+        dir[k] = (b.middle[k] + cx * b.horizontal[k] + cy * b.vertical[k] - b.campos[k]) * b.focal;
+        n += dir[k] * dir[k];
+      }
+      n = std::sqrt(n);
+      for (int k = 0; k < 3; ++k) {
+        double e = b.campos[k] + dir[k] / n * tmax;
+        lo[k] = std::min(lo[k], e);
+        hi[k] = std::max(hi[k], e);
+      }
+    }
+  lo[1] = std::max(lo[1], (double)y_lo);
+  hi[1] = std::min(hi[1], (double)y_hi);
+  if (!(hi[1] > lo[1])) {
+    lo[1] = y_lo;
+    hi[1] = y_hi;
+  }
+  for (int k = 0; k < 3; ++k) {
+    box_min[k] = (float)lo[k];
+    box_max[k] = (float)hi[k];
+  }
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_create(const re_nsdf_config* cfg, re_nsdf** out) {
+  using namespace re::nsdf;
+  if (!cfg || !out) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_create: null argument");
+  for (int k = 0; k < 3; ++k)
+    if (!(cfg->box_max[k] > cfg->box_min[k]))
+      return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_create: empty box");
+  if (!(cfg->f0 > 0.f)) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_create: f0 must be > 0");
+  re_nsdf* s = new (std::nothrow) re_nsdf();
+  if (!s) return re::fail(RE_ERR_OUT_OF_MEMORY, "re_nsdf_create: host allocation");
+  cudaError_t e = cudaGetDevice(&s->device);
+  for (int k = 0; k < 3; ++k) {
+    s->map.center[k] = 0.5f * (cfg->box_min[k] + cfg->box_max[k]);
+    s->map.inv_half[k] = 2.0f / (cfg->box_max[k] - cfg->box_min[k]);
+  }
+  s->map.f0 = cfg->f0;
+  s->seed = cfg->seed;
+  if (e == cudaSuccess) e = cudaMalloc(&s->params, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->grad, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->adam_m, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->adam_v, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->pack, re::nsdf::kPackBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&s->step_ctr, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&s->counters, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&s->err, 4);
+  if (e == cudaSuccess) e = cudaMemset(s->adam_m, 0, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMemset(s->adam_v, 0, kNumParams * 4);
+  if (e == cudaSuccess) e = cudaMemset(s->step_ctr, 0, 16);
+  if (e == cudaSuccess) e = cudaMemset(s->err, 0, 4);
+  if (e == cudaSuccess) {
+    // Glorot-uniform weights, zero biases (std::mt19937 seeded by cfg->seed)
+    std::vector<float> h(kNumParams, 0.f);
+    std::mt19937 gen(cfg->seed);
+    auto fill = [&](int off, int fan_out, int fan_in) {
+      float a = std::sqrt(6.0f / (float)(fan_in + fan_out));
+      std::uniform_real_distribution<float> U(-a, a);
+      for (int i = 0; i < fan_out * fan_in; ++i) h[off + i] = U(gen);
+    };
+    fill(OFF_W1, kHidden, kIn);
+    fill(OFF_W2, kHidden, kHidden);
+    fill(OFF_W3, kHidden, kHidden);
+    fill(OFF_W4, kHidden, kHidden);
+    fill(OFF_W5, 1, kHidden);
+    e = cudaMemcpy(s->params, h.data(), kNumParams * 4, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    re_status st = re::cuda_fail(e, "re_nsdf_create");
+    re_nsdf_destroy(s);
+    return st;
+  }
+  *out = s;
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_destroy(re_nsdf* s) {
+  if (!s) return RE_OK;
+  re::free_train(s);
+  cudaFree(s->params);
+  cudaFree(s->grad);
+  cudaFree(s->adam_m);
+  cudaFree(s->adam_v);
+  cudaFree(s->pack);
+  cudaFree(s->step_ctr);
+  cudaFree(s->data);
+  cudaFree(s->loss_hist);
+  cudaFree(s->counters);
+  cudaFree(s->queue);
+  cudaFree(s->err);
+  delete s;
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_get_params(const re_nsdf* s, float* host) {
+  re_status st = re::check(s, "re_nsdf_get_params");
+  if (st != RE_OK) return st;
+  if (!host) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_get_params: null output");
+  RE_CUDA(cudaMemcpy(host, s->params, re::nsdf::kNumParams * 4, cudaMemcpyDeviceToHost));
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_set_params(re_nsdf* s, const float* host) {
+  re_status st = re::check(s, "re_nsdf_set_params");
+  if (st != RE_OK) return st;
+  if (!host) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_set_params: null input");
+  RE_CUDA(cudaMemcpy(s->params, host, re::nsdf::kNumParams * 4, cudaMemcpyHostToDevice));
+  s->pack_valid = false;
+  s->lipschitz = 0.f;
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_generate(re_nsdf* s, const re_sdf_params* field, const re_camera* cam,
+                                  uint32_t w, uint32_t h, uint32_t num_points, uint32_t seed,
+                                  void* stream) {
+  re_status st = re::check(s, "re_nsdf_generate");
+  if (st != RE_OK) return st;
+  st = re::check_field(field, "re_nsdf_generate");
+  if (st != RE_OK) return st;
+  if (!cam || w < 2 || h < 2 || num_points < 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_generate: bad arguments");
+  if (num_points > (1u << 28)) return re::fail(RE_ERR_LIMIT, "re_nsdf_generate: > 2^28 points");
+  cudaStream_t cs = (cudaStream_t)stream;
+  if (s->npts != num_points) {
+    RE_CUDA(cudaStreamSynchronize(cs));
+    cudaFree(s->data);
+    s->data = nullptr;
+    s->npts = 0;
+    RE_CUDA(cudaMalloc(&s->data, (size_t)num_points * sizeof(float4)));
+    s->npts = num_points;
+  }
+  float3 bmin, bmax;
+  bmin.x = s->map.center[0] - 1.f / s->map.inv_half[0];
+  bmin.y = s->map.center[1] - 1.f / s->map.inv_half[1];
+  bmin.z = s->map.center[2] - 1.f / s->map.inv_half[2];
+  bmax.x = s->map.center[0] + 1.f / s->map.inv_half[0];
+  bmax.y = s->map.center[1] + 1.f / s->map.inv_half[1];
+  bmax.z = s->map.center[2] + 1.f / s->map.inv_half[2];
+  RE_CUDA(cudaFuncSetAttribute(re::nsdf::k_nsdf_data, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kPermSmemBytes));
+  re::nsdf::k_nsdf_data<<<re::sm_count() * 3, 256, re::kPermSmemBytes, cs>>>(
+      re::perm_of(field->seed), re::field_of(*field), re::cam_dev(*cam), w, h, bmin, bmax,
+      num_points, seed, s->data);
+  RE_CHECK_LAUNCH("re_nsdf_generate: launch");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_get_data(const re_nsdf* s, float* host_xyzl, uint32_t max_points) {
+  re_status st = re::check(s, "re_nsdf_get_data");
+  if (st != RE_OK) return st;
+  if (!host_xyzl) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_get_data: null output");
+  uint32_t n = std::min(max_points, s->npts);
+  RE_CUDA(cudaMemcpy(host_xyzl, s->data, (size_t)n * 16, cudaMemcpyDeviceToHost));
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_train(re_nsdf* s, uint32_t steps, uint32_t batch, float lr,
+                               float* loss_out, void* stream) {
+  re_status st = re::check(s, "re_nsdf_train");
+  if (st != RE_OK) return st;
+  if (!s->data || s->npts == 0) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_train: no data (call re_nsdf_generate)");
+  if (batch == 0 || batch % re::nsdf::kRowsBwd != 0 || batch > (1u << 22))
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_train: batch must be a positive multiple of %d up to 2^22",
+                    re::nsdf::kRowsBwd);
+  if (steps == 0) return RE_OK;
+  cudaStream_t cs = (cudaStream_t)stream;
+  st = re::alloc_train(s, batch);
+  if (st != RE_OK) return st;
+  uint32_t done = s->total_steps_done;
+  if (s->loss_cap < done + steps) {
+    RE_CUDA(cudaStreamSynchronize(cs));
+    float* nh = nullptr;
+    uint32_t cap = std::max(done + steps, 2 * s->loss_cap);
+    RE_CUDA(cudaMalloc(&nh, (size_t)cap * 4));
+    if (s->loss_hist) {
+      RE_CUDA(cudaMemcpy(nh, s->loss_hist, (size_t)s->loss_cap * 4, cudaMemcpyDeviceToDevice));
+      cudaFree(s->loss_hist);
+    }
+    s->loss_hist = nh;
+    s->loss_cap = cap;
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->graph_exec = nullptr;
+    s->graph = nullptr;
+  }
+  if (!s->graph_exec || s->graph_lr != lr) {
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->graph_exec = nullptr;
+    s->graph = nullptr;
+    cudaStream_t cap_stream;
+    RE_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      st = re::enqueue_step(s, s->data, s->npts, 0, lr, true, nullptr, cap_stream);
+      e = cudaStreamEndCapture(cap_stream, &s->graph);
+    }
+    if (e == cudaSuccess && st == RE_OK) e = cudaGraphInstantiate(&s->graph_exec, s->graph, 0);
+    cudaStreamDestroy(cap_stream);
+    if (st != RE_OK) return st;
+    if (e != cudaSuccess) return re::cuda_fail(e, "re_nsdf_train: graph capture");
+    s->graph_lr = lr;
+  }
+  for (uint32_t i = 0; i < steps; ++i) RE_CUDA(cudaGraphLaunch(s->graph_exec, cs));
+  s->pack_valid = false;
+  s->lipschitz = 0.f;
+  if (loss_out)
+    RE_CUDA(cudaMemcpyAsync(loss_out, s->loss_hist + done, (size_t)steps * 4,
+                            cudaMemcpyDeviceToHost, cs));
+  RE_CUDA(cudaStreamSynchronize(cs));
+  s->total_steps_done = done + steps;
+  return RE_OK;
+}
+
+// Loss gradient of a given batch (points + labels as float4), no update.
+RE_API re_status re_nsdf_loss_grad(re_nsdf* s, const float* d_xyzl, uint32_t n, float* d_grad,
+                                   float* d_pred, void* stream) {
+  re_status st = re::check(s, "re_nsdf_loss_grad");
+  if (st != RE_OK) return st;
+  if (!d_xyzl || !d_grad || n == 0 || n % re::nsdf::kRowsBwd != 0)
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_loss_grad: n must be a positive multiple of %d",
+                    re::nsdf::kRowsBwd);
+  cudaStream_t cs = (cudaStream_t)stream;
+  st = re::alloc_train(s, n);
+  if (st != RE_OK) return st;
+  st = re::enqueue_step(s, reinterpret_cast<const float4*>(d_xyzl), n, 1, 0.f, false, d_pred, cs);
+  if (st != RE_OK) return st;
+  RE_CUDA(cudaMemcpyAsync(d_grad, s->grad, re::nsdf::kNumParams * 4, cudaMemcpyDeviceToDevice, cs));
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_eval(re_nsdf* s, const float* d_pts, uint32_t n, float* d_out,
+                              void* stream) {
+  re_status st = re::check(s, "re_nsdf_eval");
+  if (st != RE_OK) return st;
+  if (!d_pts || !d_out) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_eval: null buffer");
+  if (n == 0) return RE_OK;
+  cudaStream_t cs = (cudaStream_t)stream;
+  st = re::ensure_pack(s, cs);
+  if (st != RE_OK) return st;
+  auto k = re::nsdf::k_tc_eval;
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)re::kTcSmemBytes));
+  int grid = std::min<int>(re::tc_grid(k), (int)((n + 127) / 128));
+  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
+  k<<<grid, 256, re::kTcSmemBytes, cs>>>(s->map, s->pack, d_pts, n, d_out, s->err);
+  RE_CHECK_LAUNCH("re_nsdf_eval: launch");
+  int herr = 0;
+  RE_CUDA(cudaMemcpyAsync(&herr, s->err, 4, cudaMemcpyDeviceToHost, cs));
+  RE_CUDA(cudaStreamSynchronize(cs));
+  if (herr) return re::fail(RE_ERR_INTERNAL, "re_nsdf_eval: tensor-core wait bound reached");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_eval_reference(re_nsdf* s, const float* d_pts, uint32_t n, float* d_out,
+                                        void* stream) {
+  re_status st = re::check(s, "re_nsdf_eval_reference");
+  if (st != RE_OK) return st;
+  if (!d_pts || !d_out) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_eval_reference: null buffer");
+  if (n == 0) return RE_OK;
+  re::nsdf::k_ref_eval<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(s->map, s->params, d_pts,
+                                                                            n, d_out);
+  RE_CHECK_LAUNCH("re_nsdf_eval_reference: launch");
+  return RE_OK;
+}
+
+// Lipschitz estimate of the network over `samples` training points:
+// max |grad| by forward differences with step h.
+RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h, float* out,
+                                   void* stream) {
+  re_status st = re::check(s, "re_nsdf_lipschitz");
+  if (st != RE_OK) return st;
+  if (!out || samples == 0 || !(h > 0.f) || !s->data)
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_lipschitz: bad arguments or no data");
+  cudaStream_t cs = (cudaStream_t)stream;
+  uint32_t n = std::min(samples, s->npts);
+  std::vector<float4> pts(n);
+  RE_CUDA(cudaMemcpy(pts.data(), s->data, (size_t)n * 16, cudaMemcpyDeviceToHost));
+  std::vector<float> q(12 * (size_t)n);
+  for (uint32_t i = 0; i < n; ++i) {
+    float p[3] = {pts[i].x, pts[i].y, pts[i].z};
+    for (int k = 0; k < 4; ++k)
+      for (int a = 0; a < 3; ++a) q[12 * (size_t)i + 3 * k + a] = p[a] + ((k == a + 1) ? h : 0.f);
+  }
+  float *dq = nullptr, *dv = nullptr;
+  unsigned int* dm = nullptr;
+  RE_CUDA(cudaMalloc(&dq, q.size() * 4));
+  cudaError_t e = cudaMalloc(&dv, (size_t)n * 4 * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&dm, 4);
+  if (e == cudaSuccess) e = cudaMemcpy(dq, q.data(), q.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dm, 0, 4);
+  if (e == cudaSuccess) {
+    st = re_nsdf_eval(s, dq, 4 * n, dv, stream);
+    if (st == RE_OK) {
+      re::nsdf::k_grad_norm<<<(n + 255) / 256, 256, 0, cs>>>(dv, n, h, dm);
+      e = cudaGetLastError();
+      unsigned int bits = 0;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, dm, 4, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+      float v;
+      std::memcpy(&v, &bits, 4);
+      *out = v;
+      s->lipschitz = v;
+    }
+  }
+  cudaFree(dq);
+  cudaFree(dv);
+  cudaFree(dm);
+  if (st != RE_OK) return st;
+  if (e != cudaSuccess) return re::cuda_fail(e, "re_nsdf_lipschitz");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
+                               const re_nsdf_trace_params* tp, const re_camera* cam, uint32_t w,
+                               uint32_t h, re_sdf_hit* d_out, void* stream) {
+  re_status st = re::check(s, "re_nsdf_trace");
+  if (st != RE_OK) return st;
+  st = re::check_field(field, "re_nsdf_trace");
+  if (st != RE_OK) return st;
+  if (!tp || !cam || !d_out || w < 2 || h < 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace: bad arguments");
+  if ((uint64_t)w * h > (1ull << 28)) return re::fail(RE_ERR_LIMIT, "re_nsdf_trace: image > 2^28 pixels");
+  if (!(tp->lipschitz > 0.f)) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace: lipschitz must be > 0");
+  cudaStream_t cs = (cudaStream_t)stream;
+  size_t need = (size_t)w * h;
+  if (s->queue_cap < need) {
+    RE_CUDA(cudaStreamSynchronize(cs));
+    cudaFree(s->queue);
+    s->queue = nullptr;
+    s->queue_cap = 0;
+    RE_CUDA(cudaMalloc(&s->queue, need * sizeof(uint4)));
+    s->queue_cap = need;
+  }
+  st = re::ensure_pack(s, cs);
+  if (st != RE_OK) return st;
+  re::nsdf::MarchDev md;
+  md.alpha = tp->safety / tp->lipschitz;
+  md.switch_dist = tp->switch_dist;
+  md.min_step = tp->min_step;
+  md.tmax = field->tmax;
+  md.max_steps = tp->max_network_steps ? tp->max_network_steps : 256;
+  re::CamDev cd = re::cam_dev(*cam);
+  RE_CUDA(cudaMemsetAsync(s->counters, 0, 16, cs));
+  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
+  auto k = re::nsdf::k_nsdf_march;
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)re::kTcSmemBytes));
+  k<<<re::tc_grid(k), 256, re::kTcSmemBytes, cs>>>(s->map, s->pack, md, cd, w, h, s->counters,
+                                                   s->queue, reinterpret_cast<float4*>(d_out),
+                                                   s->err);
+  RE_CHECK_LAUNCH("re_nsdf_trace: march launch");
+  auto kr = re::nsdf::k_sdf_refine;
+  RE_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kPermSmemBytes));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, 256, re::kPermSmemBytes) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  uint32_t exact_steps = tp->max_exact_steps ? tp->max_exact_steps : field->max_steps;
+  kr<<<per_sm * re::sm_count(), 256, re::kPermSmemBytes, cs>>>(
+      re::perm_of(field->seed), re::field_of(*field), exact_steps, cd, w, h, s->queue, s->counters,
+      reinterpret_cast<float4*>(d_out));
+  RE_CHECK_LAUNCH("re_nsdf_trace: refine launch");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined, int* error) {
+  re_status st = re::check(s, "re_nsdf_trace_status");
+  if (st != RE_OK) return st;
+  uint32_t c[4] = {0, 0, 0, 0};
+  int e = 0;
+  RE_CUDA(cudaMemcpy(c, s->counters, 16, cudaMemcpyDeviceToHost));
+  RE_CUDA(cudaMemcpy(&e, s->err, 4, cudaMemcpyDeviceToHost));
+  if (num_refined) *num_refined = c[1];
+  if (error) *error = e;
+  return RE_OK;
+}
+
+// Checkpoint: 16-byte header ("RENSDF01", parameter count, steps done),
+// the input map, then parameters and both Adam moments as FP32.
+RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path) {
+  using namespace re::nsdf;
+  re_status st = re::check(s, "re_nsdf_save");
+  if (st != RE_OK) return st;
+  if (!path) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_save: null path");
+  std::vector<float> buf(3 * (size_t)kNumParams);
+  RE_CUDA(cudaMemcpy(buf.data(), s->params, kNumParams * 4, cudaMemcpyDeviceToHost));
+  RE_CUDA(cudaMemcpy(buf.data() + kNumParams, s->adam_m, kNumParams * 4, cudaMemcpyDeviceToHost));
+  RE_CUDA(cudaMemcpy(buf.data() + 2 * kNumParams, s->adam_v, kNumParams * 4, cudaMemcpyDeviceToHost));
+  uint32_t steps = 0;
+  RE_CUDA(cudaMemcpy(&steps, s->step_ctr, 4, cudaMemcpyDeviceToHost));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_save: cannot open %s", path);
+  uint32_t hdr[4] = {0x534E4552u, 0x31304653u, (uint32_t)kNumParams, steps};
+  bool ok = std::fwrite(hdr, 4, 4, f) == 4 && std::fwrite(&s->map, sizeof(s->map), 1, f) == 1 &&
+            std::fwrite(buf.data(), 4, buf.size(), f) == buf.size();
+  std::fclose(f);
+  if (!ok) return re::fail(RE_ERR_INTERNAL, "re_nsdf_save: write failed");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_load(re_nsdf* s, const char* path) {
+  using namespace re::nsdf;
+  re_status st = re::check(s, "re_nsdf_load");
+  if (st != RE_OK) return st;
+  if (!path) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_load: null path");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_load: cannot open %s", path);
+  uint32_t hdr[4];
+  InputMap m;
+  std::vector<float> buf(3 * (size_t)kNumParams);
+  bool ok = std::fread(hdr, 4, 4, f) == 4 && hdr[0] == 0x534E4552u && hdr[1] == 0x31304653u &&
+            hdr[2] == (uint32_t)kNumParams && std::fread(&m, sizeof(m), 1, f) == 1 &&
+            std::fread(buf.data(), 4, buf.size(), f) == buf.size();
+  std::fclose(f);
+  if (!ok) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_load: %s is not a checkpoint of this network", path);
+  RE_CUDA(cudaMemcpy(s->params, buf.data(), kNumParams * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemcpy(s->adam_m, buf.data() + kNumParams, kNumParams * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemcpy(s->adam_v, buf.data() + 2 * kNumParams, kNumParams * 4, cudaMemcpyHostToDevice));
+  RE_CUDA(cudaMemcpy(s->step_ctr, &hdr[3], 4, cudaMemcpyHostToDevice));
+  s->map = m;
+  s->total_steps_done = hdr[3];
+  s->pack_valid = false;
+  s->lipschitz = 0.f;
+  return RE_OK;
+}
+
+}  // extern "C"

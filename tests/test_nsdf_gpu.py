@@ -1,0 +1,100 @@
+"""Neural SDF surrogate on the GPU against the CPU oracle (oracle/nsdf_oracle.py).
+
+Tolerances: the device evaluates sin/cos with the special-function unit and
+rounds features, weights and activations to BF16; the oracle rounds at the
+same places from exact sin/cos, so a rounding boundary can flip one BF16 ulp
+(2^-8 relative) of a feature.  Outputs are compared to 2e-2 of the output
+scale, gradients by relative L2 error < 5e-2 and cosine > 0.998.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+import torch
+
+import rayengine_b200 as rb
+from oracle import nsdf_oracle as no
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+BOX = ([-40.0, -6.0, -20.0], [40.0, 11.0, 60.0])
+F0 = 0.5
+
+
+def _model(seed=3):
+    m = rb.NeuralSDF(BOX[0], BOX[1], F0, seed)
+    return m
+
+
+def _pts(n, seed=0):
+    rng = np.random.default_rng(seed)
+    return np.stack([rng.uniform(BOX[0][k], BOX[1][k], n) for k in range(3)], 1).astype(np.float32)
+
+
+def test_tensor_core_eval_matches_reference_and_oracle(cuda):
+    with _model() as m:
+        p = m.get_params()
+        # larger weights than the initialisation so every layer matters
+        rng = np.random.default_rng(7)
+        p = (p * 2.0 + rng.normal(0, 0.02, p.shape)).astype(np.float32)
+        m.set_params(p)
+        pts = _pts(5000)
+        d = torch.from_numpy(pts).cuda()
+        tc = m.eval(d).cpu().numpy()
+        ref = m.eval_reference(d).cpu().numpy()
+        orc, _, _ = no.forward(p, pts, *BOX, F0, bf16_round=True)
+        scale = np.abs(orc).max() + 1e-6
+        assert np.abs(ref - orc).max() / scale < 2e-2
+        assert np.abs(tc - ref).max() / scale < 2e-2
+        assert np.corrcoef(tc, orc)[0, 1] > 0.999
+        # odd sizes: partial tiles
+        for n in (1, 127, 129, 1000):
+            out = m.eval(d[:n].contiguous()).cpu().numpy()
+            assert np.allclose(out, tc[:n], atol=1e-6 * scale)
+
+
+def test_loss_gradient_matches_oracle(cuda):
+    with _model() as m:
+        p = m.get_params()
+        n = 1024
+        pts = _pts(n, 1)
+        labels = np.random.default_rng(2).normal(0, 1, n).astype(np.float32)
+        xyzl = torch.from_numpy(np.concatenate([pts, labels[:, None]], 1)).cuda()
+        g, pred = m.loss_grad(xyzl)
+        g, pred = g.cpu().numpy().astype(np.float64), pred.cpu().numpy()
+        loss, go, po_ = no.loss_grad(p, pts, labels, *BOX, F0, bf16_round=True)
+        assert np.abs(pred - po_).max() < 2e-2 * (np.abs(po_).max() + 1e-6)
+        # predictions that straddle the label can flip the sign of the L1
+        # gradient; compare on the whole vector
+        rel = np.linalg.norm(g - go) / np.linalg.norm(go)
+        cos = g @ go / (np.linalg.norm(g) * np.linalg.norm(go))
+        assert rel < 5e-2 and cos > 0.998, (rel, cos)
+
+
+def test_training_reduces_loss_and_checkpoints(cuda):
+    tc = rb.configs.TerrainConfig(width=192, height=108)
+    cam = tc.camera()
+    lo, hi = rb.NeuralSDF.box_for_camera(cam, tc.width, tc.height, 60.0, -6.0, 11.0)
+    with rb.NeuralSDF(lo, hi, F0, 5) as m:
+        m.generate(tc.params(), cam, tc.width, tc.height, 1 << 18, seed=9)
+        data = m.data(4096)
+        # labels: first-order distance of the exact field
+        P = po.perm(tc.seed)
+        dens = data[:, 1].astype(np.float64) - 3.0 * po.fbm_batch(P, data[:, :3], 8, scale=0.25)
+        agree = np.sign(dens) == np.sign(data[:, 3])
+        assert agree.mean() > 0.99
+        near = np.abs(data[1::2, 3]) < 0.2
+        assert near.mean() > 0.5  # the near-surface half is near the surface
+        losses = m.train(300, batch=8192, lr=2e-3)
+        assert np.all(np.isfinite(losses))
+        assert losses[-20:].mean() < 0.5 * losses[:5].mean()
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "net.bin")
+            m.save(path)
+            p1 = m.get_params()
+            m.train(5, batch=8192, lr=2e-3)
+            assert not np.array_equal(m.get_params(), p1)
+            m.load(path)
+            assert np.array_equal(m.get_params(), p1)

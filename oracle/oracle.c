@@ -633,3 +633,82 @@ void o_secondary_rays(const float hitp[3], const float n[3], uint32_t seed,
     tmax_out[1 + j] = 1.0f;
   }
 }
+
+/* ------------------------------------------------------- FP64 judge */
+/* The same lattice noise in double precision (exact quintic and trilinear
+ * polynomial), for the error of float hit positions. */
+static double quintic_d(double t) { return t * t * t * (t * (t * 6.0 - 15.0) + 10.0); }
+
+static double grad_dot_d(uint32_t h, double x, double y, double z) {
+  switch (h & 15u) {
+    case 0: return x + y;
+    case 1: return -x + y;
+    case 2: return x - y;
+    case 3: return -x - y;
+    case 4: return x + z;
+    case 5: return -x + z;
+    case 6: return x - z;
+    case 7: return -x - z;
+    case 8: return y + z;
+    case 9: return -y + z;
+    case 10: return y - z;
+    case 11: return -y - z;
+    case 12: return y + x;
+    case 13: return -x + y;
+    case 14: return -y + z;
+    default: return -y - z;
+  }
+}
+
+double o_perlin_d(const uint32_t P[512], double x, double y, double z) {
+  double fx = floor(x), fy = floor(y), fz = floor(z);
+  int xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
+  int xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
+  double tx = x - fx, ty = y - fy, tz = z - fz;
+  double u = quintic_d(tx), v = quintic_d(ty), w = quintic_d(tz);
+  uint32_t px0 = P[xi0], px1 = P[xi1];
+  uint32_t p00 = P[px0 + yi0], p10 = P[px1 + yi0], p01 = P[px0 + yi1], p11 = P[px1 + yi1];
+  double a = grad_dot_d(P[p00 + zi0], tx, ty, tz), b = grad_dot_d(P[p10 + zi0], tx - 1, ty, tz);
+  double c = grad_dot_d(P[p01 + zi0], tx, ty - 1, tz), d = grad_dot_d(P[p11 + zi0], tx - 1, ty - 1, tz);
+  double e = grad_dot_d(P[p00 + zi1], tx, ty, tz - 1), f = grad_dot_d(P[p10 + zi1], tx - 1, ty, tz - 1);
+  double g = grad_dot_d(P[p01 + zi1], tx, ty - 1, tz - 1), h = grad_dot_d(P[p11 + zi1], tx - 1, ty - 1, tz - 1);
+  return a + (b - a) * u + (c - a) * v + (e - a) * w + (a + d - b - c) * u * v +
+         (a + f - b - e) * u * w + (a + g - c - e) * v * w +
+         (b + c + e + h - a - d - f - g) * u * v * w;
+}
+
+double o_terrain_density_d(const uint32_t P[512], const double p[3], int octaves, double scale,
+                           double amp) {
+  double x = scale * p[0], y = scale * p[1], z = scale * p[2], s = 0.0, a = 1.0;
+  for (int i = 0; i < octaves; ++i) {
+    s += a * o_perlin_d(P, x, y, z);
+    x *= 2.0;
+    y *= 2.0;
+    z *= 2.0;
+    a *= 0.5;
+  }
+  return p[1] - amp * s;
+}
+
+/* March the ray (o, d promoted to double) with t += factor * d until the
+ * density is below 1e-10 (the first crossing approached from outside), or
+ * t > tmax.  Returns 1 and the position on a hit. */
+int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int octaves,
+                 double scale, double amp, double factor, double tmax, int max_steps,
+                 double pos[3], double* t_out) {
+  double t = 0.0;
+  for (int s = 0; s < max_steps; ++s) {
+    double p[3] = {o[0] + t * (double)d[0], o[1] + t * (double)d[1], o[2] + t * (double)d[2]};
+    double dist = o_terrain_density_d(P, p, octaves, scale, amp);
+    if (dist < 1e-10) {
+      pos[0] = p[0];
+      pos[1] = p[1];
+      pos[2] = p[2];
+      *t_out = t;
+      return 1;
+    }
+    t += factor * dist;
+    if (t > tmax) return 0;
+  }
+  return 0;
+}

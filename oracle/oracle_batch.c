@@ -203,3 +203,30 @@ void o_batch_frame_ao_bruteforce(const float* packed, int32_t n, const float bmi
   }
   if (nsec) *nsec = (uint32_t)total;
 }
+
+double o_terrain_density_d(const uint32_t P[512], const double p[3], int octaves, double scale,
+                           double amp);
+int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int octaves,
+                 double scale, double amp, double factor, double tmax, int max_steps,
+                 double pos[3], double* t_out);
+
+/* FP64 judge over pixels: out[i] = {x, y, z, hit} of the surface point. */
+void o_batch_sdf_judge(const uint32_t perm[512], const o_camera* cam, uint32_t w, uint32_t h,
+                       int octaves, double scale, double amp, double factor, double tmax,
+                       int max_steps, const uint32_t* pixels, int64_t npix, double* out,
+                       int threads) {
+  o_camera_basis b;
+  o_camera_setup(cam, &b);
+#pragma omp parallel for schedule(dynamic, 8) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < npix; ++i) {
+    uint32_t p = pixels[i];
+    float o[3], d[3];
+    o_generate_ray(&b, w, h, p % w, p / w, o, d);
+    double pos[3] = {0, 0, 0}, t = 0;
+    int hit = o_sdf_root_d(perm, o, d, octaves, scale, amp, factor, tmax, max_steps, pos, &t);
+    out[4 * i] = pos[0];
+    out[4 * i + 1] = pos[1];
+    out[4 * i + 2] = pos[2];
+    out[4 * i + 3] = hit;
+  }
+}

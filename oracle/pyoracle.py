@@ -321,3 +321,27 @@ def frame_ao_bruteforce(packed, bmin, bmax, cam, w, h, light_dir, ao_length, bia
     if return_results:
         return out, mask, nsec.value
     return n + nsec.value
+
+
+def sdf_judge(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6, tmax=200.0,
+              max_steps=4096, nthreads=0):
+    """FP64 surface points of the given pixels' rays: (n, 3) positions and a hit mask."""
+    pix = np.ascontiguousarray(pixels, np.uint32)
+    out = np.zeros((pix.shape[0], 4), np.float64)
+    oc = camera(cam)
+    lib().o_batch_sdf_judge(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                            ctypes.c_int(octaves), ctypes.c_double(scale), ctypes.c_double(amp),
+                            ctypes.c_double(factor), ctypes.c_double(tmax), ctypes.c_int(max_steps),
+                            _p(pix), ctypes.c_int64(pix.shape[0]), _p(out), ctypes.c_int(nthreads))
+    return out[:, :3], out[:, 3] > 0.5
+
+
+def hit_errors(sdf_out, judge_pos, judge_hit, pixels):
+    """Per-pixel |p_gpu - p_fp64| where both hit, plus hit/miss disagreements."""
+    o = np.asarray(sdf_out)
+    f = o.view(np.float32).reshape(-1, 8)[pixels]
+    status = o.view(np.uint32).reshape(-1, 8)[pixels, 7]
+    gpu_hit = status == 1
+    both = gpu_hit & judge_hit
+    err = np.linalg.norm(f[both, 0:3].astype(np.float64) - judge_pos[both], axis=1)
+    return err, int((gpu_hit != judge_hit).sum()), int(both.sum())

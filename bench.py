@@ -129,8 +129,32 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+# FP32 issue peak of the SIMT pipes (no measured figure exists for it):
+# 148 SMs x 128 FP32 lanes x 1965 MHz, one operation (an FMA counts once)
+# per lane per clock
+FP32_TOPS_NOMINAL = 148 * 128 * 1.965e9 / 1e12
+# FP32 operations of one evaluation of d(p) = p.y - 3 fBm(0.25 p), 8
+# octaves, counted from the formula (FMA = 1): Perlin 70 (3 floor, 3 frac,
+# 15 quintic, 3 offsets, 16 gradient dots, 19 for k1..k7, 11 interpolation)
+# + 5 fBm bookkeeping per octave, + 4 for the scale and the final FMA
+SDF_OPS_PER_EVAL = 8 * 75 + 4
+# BF16 tensor FLOPs of one network evaluation: 2 (128*64 + 3*64*64 + 64)
+NSDF_FLOPS_PER_EVAL = 41088
+
+
+def hbm_roofline(wl, phase_ms, peaks):
+    ab = wl.alg_bytes()
+    dom = max(phase_ms, key=phase_ms.get)
+    achieved = ab[dom] / (phase_ms[dom] / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "peak_source": peaks["source"], "alg_bytes_per_launch": ab[dom],
+            "traffic": ncu_traffic(f"{wl.name}:{dom}")}
 
 
 def ncu_traffic(key: str):
@@ -354,6 +378,16 @@ class TerrainSDF:
     def alg_bytes(self):
         return {"sdf": 32 * self.rays_per_step}
 
+    def roofline(self, phase_ms, peaks):
+        evals = self.steps + 6 * self.hits
+        achieved = evals * SDF_OPS_PER_EVAL / (phase_ms["sdf"] / 1e3) / 1e12
+        return {"bound": "fp32-simt", "kernel": "sdf", "achieved": round(achieved, 3),
+                "peak": round(FP32_TOPS_NOMINAL, 2), "unit": "Tops/s",
+                "frac": round(achieved / FP32_TOPS_NOMINAL, 4),
+                "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1965 MHz",
+                "alg_ops_per_launch": evals * SDF_OPS_PER_EVAL,
+                "traffic": ncu_traffic(f"{self.name}:sdf")}
+
     def host_buffers(self, torch):
         W, H = self.cfg.width, self.cfg.height
         return (torch.empty((H * W, 8), dtype=torch.int32, pin_memory=True), None)
@@ -389,6 +423,109 @@ class TerrainSDF:
 
 
 
+class NeuralTerrainSDF:
+    """The terrain of TerrainSDF traced through the neural surrogate: the
+    network is trained at set-up (8M points, 20k Adam steps of 65,536), then
+    a step = one 1920x1080 frame of network march + exact phase."""
+    name = "nsdf_terrain"
+    dtype = "bf16 (network, FP32 accumulate) + f32 (exact field)"
+
+    def __init__(self, torch):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.ncfg = rb.configs.NeuralTerrainConfig()
+        self.cfg = cfg = self.ncfg.terrain
+        self.cam = cfg.camera()
+        self.params = cfg.params()
+        W, H = cfg.width, cfg.height
+        t0 = time.perf_counter()
+        self.model, self.tp, losses = self.ncfg.build()
+        torch.cuda.synchronize()
+        self.train_s = time.perf_counter() - t0
+        self.final_loss = float(np.mean(losses[-100:]))
+        self.out = torch.empty((H * W, 8), dtype=torch.int32, device="cuda")
+        self.model.trace(self.params, self.tp, self.cam, W, H, self.out)
+        self.stats = self.model.trace_status()
+        if self.stats["error"]:
+            raise RuntimeError("tensor-core wait bound reached in the network march")
+        o = self.out.cpu().numpy()
+        self.hits = int((o[:, 7] == 1).sum())
+        # the exact tracer on the same frame, same run, for the ratio
+        ex = torch.empty_like(self.out)
+        for _ in range(3):
+            rb.sphere_trace(self.params, self.cam, W, H, ex)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(20):
+            rb.sphere_trace(self.params, self.cam, W, H, ex)
+        b.record()
+        torch.cuda.synchronize()
+        self.exact_ms = a.elapsed_time(b) / 20
+        self.rays_per_step = W * H
+        self.kernels_per_step = 2
+
+    def config(self):
+        n = self.ncfg
+        st = self.stats
+        R = self.rays_per_step
+        return {"workload": "neural-SDF surrogate of d(p)=p.y-3fBm(0.25p) (8 octaves), 1920x1080: "
+                            "Fourier features (16 freqs) -> 4x64 softplus MLP, BF16 tcgen05 inference; "
+                            "network march then exact phase (bracket + 4 regula-falsi steps) + exact "
+                            "central-difference normal",
+                "training": {"points": n.num_points, "steps": n.train_steps, "batch": n.batch,
+                             "lr": n.lr, "seconds": round(self.train_s, 2),
+                             "final_l1_loss": round(self.final_loss, 5)},
+                "trace_params": {"lipschitz": round(self.tp.lipschitz, 4),
+                                 "lipschitz_quantile": n.lipschitz_quantile,
+                                 "safety": n.safety, "switch_dist": n.switch_dist,
+                                 "min_step": n.min_step, "max_network_steps": n.max_network_steps,
+                                 "root_steps": n.root_steps},
+                "per_ray": {"network_evals": round(st["network_evals"] / R, 3),
+                            "network_rows": round(st["network_rows"] / R, 3),
+                            "exact_evals": round(st["exact_evals"] / R, 3),
+                            "normal_evals": round(st["normal_evals"] / R, 3)},
+                "exact_sdf_same_run": {"ms_per_frame": round(self.exact_ms, 4),
+                                       "mrays": round(R / self.exact_ms / 1e3, 3)},
+                "rays_per_step": R, "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        W, H = self.cfg.width, self.cfg.height
+        m = self.model
+        return [("nsdf_march", lambda: m.trace(self.params, self.tp, self.cam, W, H, self.out, stream,
+                                               phase="network")),
+                ("sdf_refine", lambda: m.trace(self.params, self.tp, self.cam, W, H, self.out, stream,
+                                               phase="exact"))]
+
+    def roofline(self, phase_ms, peaks):
+        rows = self.stats["network_rows"]
+        achieved = rows * NSDF_FLOPS_PER_EVAL / (phase_ms["nsdf_march"] / 1e3) / 1e12
+        return {"bound": "tensor", "kernel": "nsdf_march", "achieved": round(achieved, 2),
+                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": round(achieved / peaks["bf16_tflops"], 4), "peak_source": peaks["source"],
+                "alg_flops_per_launch": rows * NSDF_FLOPS_PER_EVAL,
+                "traffic": ncu_traffic(f"{self.name}:nsdf_march")}
+
+    def host_buffers(self, torch):
+        W, H = self.cfg.width, self.cfg.height
+        return (torch.empty((H * W, 8), dtype=torch.int32, pin_memory=True), None)
+
+    def e2e_step(self, torch, stream, host_out, _):
+        W, H = self.cfg.width, self.cfg.height
+        self.model.trace(self.params, self.tp, self.cam, W, H, self.out, stream)
+        host_out.copy_(self.out, non_blocking=True)
+
+    def e2e_bytes(self):
+        import ctypes
+
+        return (ctypes.sizeof(self.rb.RCamera) + ctypes.sizeof(self.params) +
+                ctypes.sizeof(self.tp), self.cfg.width * self.cfg.height * 32)
+
+    def cpu_baseline(self, budget_s=12.0):
+        # the reference's method for this field on the host: the exact march
+        return TerrainSDF.cpu_baseline(self, budget_s)
+
+
 # ---------------------------------------------------- the reference's path
 def reference_workload(name):
     """(workload description, built-by note, step(npix) -> rays traced) for the
@@ -400,7 +537,7 @@ def reference_workload(name):
     from rayengine_b200 import api
 
     rng = np.random.default_rng(1)
-    if name == "terrain_sdf":
+    if name in ("terrain_sdf", "nsdf_terrain"):
         cfg = C.TerrainConfig()
         W, H = cfg.width, cfg.height
         P = po.perm(cfg.seed)
@@ -456,6 +593,7 @@ WORKLOADS = {
     "soup": SoupPrimary,
     "soup1m": lambda torch: SoupPrimary(torch, num_tris=1 << 20),
     "terrain_sdf": TerrainSDF,
+    "nsdf_terrain": NeuralTerrainSDF,
 }
 
 METRIC = "Mrays/s on 1 B200: plain rope-kd/exact-SDF vs wavefront+neural SDF @<=1e-3 err"
@@ -575,20 +713,16 @@ def run_ours(args):
     h2d, d2h = wl.e2e_bytes()
 
     peaks = measured_peaks()
-    ab = wl.alg_bytes()
-    dom = max(phase_ms, key=phase_ms.get)
-    achieved = ab[dom] / (phase_ms[dom] / 1e3) / 1e9
+    roof = wl.roofline(phase_ms, peaks) if hasattr(wl, "roofline") else \
+        hbm_roofline(wl, phase_ms, peaks)
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": getattr(wl, "dtype", "f32"),
         "data": "synthetic (seeded)", "config": dict(wl.config(), parallelism=f"replica x{world}"),
         "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
-                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": round(achieved / peaks["hbm_gbs"], 4),
-                     "peak_source": peaks["source"], "alg_bytes_per_launch": ab[dom],
-                     "traffic": ncu_traffic(f"{wl.name}:{dom}")},
+        "roofline": roof,
         "e2e": {"value": round(world * wl.rays_per_step / (e_ms_max / 1e3) / 1e6, 3),
                 "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": round(e_ms_max, 4)},

@@ -298,13 +298,20 @@ typedef struct re_nsdf_config {
   uint32_t seed;                /* weight initialisation and sampling seed  */
 } re_nsdf_config;
 
+/* flags of re_nsdf_trace_params */
+#define RE_NSDF_EXACT_ONLY 1u /* skip the network: the exact phase from t = 0 */
+
 typedef struct re_nsdf_trace_params {
   float lipschitz;      /* bound on the network's gradient norm           */
   float safety;         /* step = safety * distance / lipschitz            */
   float switch_dist;    /* hand over to the exact field below this         */
   float min_step;       /* smallest network step                           */
   uint32_t max_network_steps; /* 0 = 256                                   */
-  uint32_t max_exact_steps;   /* 0 = the field's max_steps                 */
+  uint32_t max_exact_steps;   /* exact evaluations per ray; 0 = max_steps  */
+  uint32_t root_steps;  /* regula-falsi steps on a bracketed crossing; 0=4 */
+  float relax;          /* exact steps may grow along the secant up to     */
+                        /* relax x step_factor * d; <= 1: the plain rule   */
+  uint32_t flags;       /* RE_NSDF_EXACT_ONLY                              */
 } re_nsdf_trace_params;
 
 RE_API uint32_t re_nsdf_num_params(void);
@@ -344,19 +351,37 @@ RE_API re_status re_nsdf_eval(re_nsdf* s, const float* d_pts, uint32_t n,
 /* The same with the training arithmetic (SIMT FP32, BF16-rounded). */
 RE_API re_status re_nsdf_eval_reference(re_nsdf* s, const float* d_pts,
                                         uint32_t n, float* d_out, void* stream);
-/* Largest forward-difference gradient norm over `samples` training points. */
+/* Gradient-norm bound: the `quantile` (0 < q <= 1; 1 = the largest) of
+ * the forward-difference gradient norms at `samples` training points. */
 RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h,
-                                   float* out, void* stream);
-/* Neural march then exact refinement; output as re_sdf_trace (steps =
- * network steps + exact steps). */
+                                   float quantile, float* out, void* stream);
+/* Neural march inside the network's box, then the exact phase: the exact
+ * tracer's steps from the hand-over point, a bracketed crossing refined by
+ * regula falsi, the exact tracer's central-difference normal.  Output as
+ * re_sdf_trace (steps = network steps + exact evaluations). */
 RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
                                const re_nsdf_trace_params* tp,
                                const re_camera* cam, uint32_t w, uint32_t h,
                                re_sdf_hit* d_out, void* stream);
-/* Rays handed to the exact field by the last trace, and the device error
- * flag (1 = a tensor-core wait reached its bound). */
+/* The two phases of re_nsdf_trace as separate calls on the same stream
+ * (network march into the hand-over queue, then the exact phase), for
+ * timing each and for callers that interleave other work. */
+RE_API re_status re_nsdf_trace_network(re_nsdf* s, const re_sdf_params* field,
+                                       const re_nsdf_trace_params* tp,
+                                       const re_camera* cam, uint32_t w,
+                                       uint32_t h, re_sdf_hit* d_out,
+                                       void* stream);
+RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
+                                     const re_nsdf_trace_params* tp,
+                                     const re_camera* cam, uint32_t w, uint32_t h,
+                                     re_sdf_hit* d_out, void* stream);
+/* Of the last trace: rays handed to the exact phase, the device error flag
+ * (1 = a tensor-core wait reached its bound) and, when evals is not NULL,
+ * four totals: network evaluations of rays, exact-field evaluations of the
+ * march / bracket / root steps, exact normal taps, network rows computed
+ * (rays and idle rows of the 128-row tiles). */
 RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
-                                      int* error);
+                                      int* error, uint64_t* evals);
 /* Checkpoint: parameters, Adam moments and step count. */
 RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
 RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);

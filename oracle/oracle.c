@@ -691,22 +691,40 @@ double o_terrain_density_d(const uint32_t P[512], const double p[3], int octaves
 }
 
 /* March the ray (o, d promoted to double) with t += factor * d until the
- * density is below 1e-10 (the first crossing approached from outside), or
- * t > tmax.  Returns 1 and the position on a hit. */
+ * density falls below 1e-10 (the first sample at or inside the surface), or
+ * t > tmax.  On a hit the root of the density between the last outside
+ * sample and that one is refined by bisection (`refine` != 0), so a march
+ * step that overshoots into the terrain shows up as position error.
+ * Returns 1 and the position on a hit. */
 int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int octaves,
                  double scale, double amp, double factor, double tmax, int max_steps,
-                 double pos[3], double* t_out) {
-  double t = 0.0;
+                 int refine, double pos[3], double* t_out) {
+  double t = 0.0, t_prev = 0.0;
   for (int s = 0; s < max_steps; ++s) {
     double p[3] = {o[0] + t * (double)d[0], o[1] + t * (double)d[1], o[2] + t * (double)d[2]};
     double dist = o_terrain_density_d(P, p, octaves, scale, amp);
     if (dist < 1e-10) {
+      if (refine && s > 0 && dist < 0.0) {
+        double lo = t_prev, hi = t;
+        for (int it = 0; it < 80; ++it) {
+          double mid = 0.5 * (lo + hi);
+          double q[3] = {o[0] + mid * (double)d[0], o[1] + mid * (double)d[1],
+                         o[2] + mid * (double)d[2]};
+          if (o_terrain_density_d(P, q, octaves, scale, amp) < 0.0) hi = mid;
+          else lo = mid;
+        }
+        t = hi;
+        p[0] = o[0] + t * (double)d[0];
+        p[1] = o[1] + t * (double)d[1];
+        p[2] = o[2] + t * (double)d[2];
+      }
       pos[0] = p[0];
       pos[1] = p[1];
       pos[2] = p[2];
       *t_out = t;
       return 1;
     }
+    t_prev = t;
     t += factor * dist;
     if (t > tmax) return 0;
   }

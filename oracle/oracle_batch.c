@@ -208,13 +208,14 @@ double o_terrain_density_d(const uint32_t P[512], const double p[3], int octaves
                            double amp);
 int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int octaves,
                  double scale, double amp, double factor, double tmax, int max_steps,
-                 double pos[3], double* t_out);
+                 int refine, double pos[3], double* t_out);
 
-/* FP64 judge over pixels: out[i] = {x, y, z, hit} of the surface point. */
+/* FP64 judge over pixels: out[i] = {x, y, z, hit} of the surface point
+ * (refine != 0: bisected root of the first crossing the march reaches). */
 void o_batch_sdf_judge(const uint32_t perm[512], const o_camera* cam, uint32_t w, uint32_t h,
                        int octaves, double scale, double amp, double factor, double tmax,
-                       int max_steps, const uint32_t* pixels, int64_t npix, double* out,
-                       int threads) {
+                       int max_steps, int refine, const uint32_t* pixels, int64_t npix,
+                       double* out, int threads) {
   o_camera_basis b;
   o_camera_setup(cam, &b);
 #pragma omp parallel for schedule(dynamic, 8) num_threads(threads > 0 ? threads : omp_get_max_threads())
@@ -223,10 +224,17 @@ void o_batch_sdf_judge(const uint32_t perm[512], const o_camera* cam, uint32_t w
     float o[3], d[3];
     o_generate_ray(&b, w, h, p % w, p / w, o, d);
     double pos[3] = {0, 0, 0}, t = 0;
-    int hit = o_sdf_root_d(perm, o, d, octaves, scale, amp, factor, tmax, max_steps, pos, &t);
+    int hit = o_sdf_root_d(perm, o, d, octaves, scale, amp, factor, tmax, max_steps, refine, pos, &t);
     out[4 * i] = pos[0];
     out[4 * i + 1] = pos[1];
     out[4 * i + 2] = pos[2];
     out[4 * i + 3] = hit;
   }
+}
+
+/* FP64 terrain density at n points (3 doubles each). */
+void o_batch_density_d(const uint32_t perm[512], const double* pts, int64_t n, int octaves,
+                       double scale, double amp, double* out, int threads) {
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < n; ++i) out[i] = o_terrain_density_d(perm, pts + 3 * i, octaves, scale, amp);
 }

@@ -324,15 +324,18 @@ def frame_ao_bruteforce(packed, bmin, bmax, cam, w, h, light_dir, ao_length, bia
 
 
 def sdf_judge(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6, tmax=200.0,
-              max_steps=4096, nthreads=0):
-    """FP64 surface points of the given pixels' rays: (n, 3) positions and a hit mask."""
+              max_steps=4096, refine=True, nthreads=0):
+    """FP64 surface points of the given pixels' rays: (n, 3) positions and a hit mask.
+
+    The FP64 march takes the float tracer's steps (t += factor * density); with
+    `refine` the first crossing it reaches is bisected to the density's root."""
     pix = np.ascontiguousarray(pixels, np.uint32)
     out = np.zeros((pix.shape[0], 4), np.float64)
     oc = camera(cam)
     lib().o_batch_sdf_judge(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
                             ctypes.c_int(octaves), ctypes.c_double(scale), ctypes.c_double(amp),
                             ctypes.c_double(factor), ctypes.c_double(tmax), ctypes.c_int(max_steps),
-                            _p(pix), ctypes.c_int64(pix.shape[0]), _p(out), ctypes.c_int(nthreads))
+                            ctypes.c_int(1 if refine else 0), _p(pix), ctypes.c_int64(pix.shape[0]), _p(out), ctypes.c_int(nthreads))
     return out[:, :3], out[:, 3] > 0.5
 
 
@@ -345,3 +348,13 @@ def hit_errors(sdf_out, judge_pos, judge_hit, pixels):
     both = gpu_hit & judge_hit
     err = np.linalg.norm(f[both, 0:3].astype(np.float64) - judge_pos[both], axis=1)
     return err, int((gpu_hit != judge_hit).sum()), int(both.sum())
+
+
+def density_d(p, pts, octaves=8, scale=0.25, amp=3.0, nthreads=0):
+    """FP64 terrain density p.y - amp * fbm(scale * p) (the judge's field)."""
+    pts = np.ascontiguousarray(pts, np.float64)
+    out = np.zeros(pts.shape[0], np.float64)
+    lib().o_batch_density_d(_p(p), _p(pts), ctypes.c_int64(pts.shape[0]), ctypes.c_int(octaves),
+                            ctypes.c_double(scale), ctypes.c_double(amp), _p(out),
+                            ctypes.c_int(nthreads))
+    return out

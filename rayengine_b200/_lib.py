@@ -137,7 +137,13 @@ class re_nsdf_trace_params(ctypes.Structure):
         ("min_step", ctypes.c_float),
         ("max_network_steps", ctypes.c_uint32),
         ("max_exact_steps", ctypes.c_uint32),
+        ("root_steps", ctypes.c_uint32),
+        ("relax", ctypes.c_float),
+        ("flags", ctypes.c_uint32),
     ]
+
+
+NSDF_EXACT_ONLY = 1
 
 
 _P = ctypes.c_void_p
@@ -183,9 +189,11 @@ _SIGS = {
     "re_nsdf_loss_grad": (ctypes.c_int, [_P, _P, _U32, _P, _P, _P]),
     "re_nsdf_eval": (ctypes.c_int, [_P, _P, _U32, _P, _P]),
     "re_nsdf_eval_reference": (ctypes.c_int, [_P, _P, _U32, _P, _P]),
-    "re_nsdf_lipschitz": (ctypes.c_int, [_P, _U32, _F, ctypes.POINTER(_F), _P]),
+    "re_nsdf_lipschitz": (ctypes.c_int, [_P, _U32, _F, _F, ctypes.POINTER(_F), _P]),
     "re_nsdf_trace": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
-    "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int)]),
+    "re_nsdf_trace_network": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_nsdf_trace_exact": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int), _P]),
     "re_nsdf_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "re_nsdf_load": (ctypes.c_int, [_P, ctypes.c_char_p]),
 }

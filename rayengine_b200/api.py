@@ -351,11 +351,18 @@ def sphere_trace(params, cam: RCamera, w: int, h: int, out=None, stream=None):
 
 
 # ------------------------------------------------------ neural SDF surrogate
-def nsdf_trace_params(lipschitz, safety=0.9, switch_dist=0.05, min_step=1e-3,
-                      max_network_steps=256, max_exact_steps=0):
+def nsdf_trace_params(lipschitz=1.0, safety=0.9, switch_dist=0.05, min_step=1e-3,
+                      max_network_steps=256, max_exact_steps=0, root_steps=4, relax=1.0,
+                      exact_only=False):
+    """Neural march / exact phase settings (re_nsdf_trace_params).
+
+    exact_only skips the network: every ray runs the exact phase from the
+    camera (the same method without the network)."""
     p = _lib.re_nsdf_trace_params()
     p.lipschitz, p.safety, p.switch_dist, p.min_step = lipschitz, safety, switch_dist, min_step
     p.max_network_steps, p.max_exact_steps = max_network_steps, max_exact_steps
+    p.root_steps, p.relax = root_steps, relax
+    p.flags = _lib.NSDF_EXACT_ONLY if exact_only else 0
     return p
 
 
@@ -454,25 +461,36 @@ class NeuralSDF:
         call("re_nsdf_eval_reference", self._h, _dptr(pts), n, _dptr(out), _stream_ptr(stream))
         return out
 
-    def lipschitz(self, samples=200000, h=1e-2, stream=None) -> float:
+    def lipschitz(self, samples=200000, h=1e-2, quantile=1.0, stream=None) -> float:
+        """Gradient-norm bound: `quantile` of the finite-difference norms (1 = max)."""
         v = ctypes.c_float()
-        call("re_nsdf_lipschitz", self._h, samples, h, ctypes.byref(v), _stream_ptr(stream))
+        call("re_nsdf_lipschitz", self._h, samples, h, quantile, ctypes.byref(v),
+             _stream_ptr(stream))
         return float(v.value)
 
-    def trace(self, field, tp, cam, w, h, out=None, stream=None):
+    def trace(self, field, tp, cam, w, h, out=None, stream=None, phase="both"):
+        """Neural march + exact phase -> int32 CUDA tensor (h*w, 8) = re_sdf_hit.
+
+        phase "network" / "exact" runs one of the two phases (in that order)."""
         import torch
 
         if out is None:
             out = torch.empty((h * w, 8), dtype=torch.int32, device="cuda")
-        call("re_nsdf_trace", self._h, ctypes.byref(field), ctypes.byref(tp), ctypes.byref(cam),
-             w, h, _dptr(out), _stream_ptr(stream))
+        fn = {"both": "re_nsdf_trace", "network": "re_nsdf_trace_network",
+              "exact": "re_nsdf_trace_exact"}[phase]
+        call(fn, self._h, ctypes.byref(field), ctypes.byref(tp), ctypes.byref(cam), w, h,
+             _dptr(out), _stream_ptr(stream))
         return out
 
-    def trace_status(self):
+    def trace_status(self) -> dict:
+        """Counters of the last trace (see re_nsdf_trace_status)."""
         n = ctypes.c_uint32()
         e = ctypes.c_int()
-        call("re_nsdf_trace_status", self._h, ctypes.byref(n), ctypes.byref(e))
-        return int(n.value), int(e.value)
+        ev = np.zeros(4, np.uint64)
+        call("re_nsdf_trace_status", self._h, ctypes.byref(n), ctypes.byref(e), ev.ctypes.data)
+        return {"handed_over": int(n.value), "error": int(e.value),
+                "network_evals": int(ev[0]), "exact_evals": int(ev[1]),
+                "normal_evals": int(ev[2]), "network_rows": int(ev[3])}
 
     def save(self, path: str):
         call("re_nsdf_save", self._h, path.encode())

@@ -103,3 +103,52 @@ class TerrainConfig:
     def params(self):
         return api.sdf_params(self.seed, self.octaves, self.scale, self.amplitude,
                               self.step_factor, self.eps, self.tmax, self.max_steps)
+
+
+@dataclass
+class NeuralTerrainConfig:
+    """Neural SDF surrogate of the terrain field above: training set, network
+    and tracer settings."""
+    terrain: TerrainConfig = None
+    box_tmax: float = 200.0      # network box: the view frustum up to this t ...
+    box_y: tuple = (-6.0, 12.0)  # ... with y clamped to this range
+    f0: float = 2.0              # lowest feature frequency (cycles per box half-width)
+    init_seed: int = 5
+    num_points: int = 8 << 20    # 50% uniform in the box, 50% near the surface
+    data_seed: int = 11
+    train_steps: int = 20000
+    batch: int = 65536
+    lr: float = 1e-3
+    lipschitz_samples: int = 200000
+    lipschitz_h: float = 1e-2
+    lipschitz_quantile: float = 0.5
+    safety: float = 0.9
+    switch_dist: float = 0.3
+    min_step: float = 0.05
+    max_network_steps: int = 64
+    root_steps: int = 4
+
+    def __post_init__(self):
+        if self.terrain is None:
+            self.terrain = TerrainConfig()
+
+    def box(self):
+        t = self.terrain
+        return api.NeuralSDF.box_for_camera(t.camera(), t.width, t.height, self.box_tmax,
+                                            self.box_y[0], self.box_y[1])
+
+    def build(self, train_steps=None):
+        """Generate the training set, train, and return (model, trace params, losses)."""
+        t = self.terrain
+        lo, hi = self.box()
+        m = api.NeuralSDF(lo, hi, self.f0, self.init_seed)
+        m.generate(t.params(), t.camera(), t.width, t.height, self.num_points, self.data_seed)
+        losses = m.train(self.train_steps if train_steps is None else train_steps, self.batch,
+                         self.lr)
+        lip = m.lipschitz(self.lipschitz_samples, self.lipschitz_h, self.lipschitz_quantile)
+        tp = self.trace_params(lip)
+        return m, tp, losses
+
+    def trace_params(self, lipschitz):
+        return api.nsdf_trace_params(lipschitz, self.safety, self.switch_dist, self.min_step,
+                                     self.max_network_steps, 0, self.root_steps)

@@ -416,13 +416,20 @@ constexpr uint32_t kPackWh = kHidden * kHidden * 2;        // 8192
 constexpr uint32_t kPackWBytes = kPackW1 + 3 * kPackWh;    // 40960
 constexpr uint32_t kPackFloats = 4 * kHidden + kHidden + 1;
 constexpr uint32_t kPackBytes = kPackWBytes + kPackFloats * 4;
+constexpr uint32_t kBiasCol = 99;    // feature = 1.0; W1 column = BF16(b1)
+constexpr uint32_t kBiasColLo = 100; // feature = 1.0; W1 column = b1 - BF16(b1)
 
+// The inference kernels feed 1.0 at W1 columns 99 and 100 (unused by the
+// features), so those columns carry b1 as a BF16 high part and a BF16
+// remainder and the first layer's bias comes out of the MMA.
 __global__ void k_pack(const float* __restrict__ params, unsigned char* __restrict__ pack) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < (uint32_t)(kHidden * kIn)) {
     uint32_t n = i / kIn, k = i % kIn;
-    *reinterpret_cast<__nv_bfloat16*>(pack + canon_off(n, k, kIn)) =
-        __float2bfloat16_rn(params[OFF_W1 + i]);
+    float v = params[OFF_W1 + i];
+    if (k == kBiasCol) v = bf16_round(params[OFF_B1 + n]);
+    if (k == kBiasColLo) v = params[OFF_B1 + n] - bf16_round(params[OFF_B1 + n]);
+    *reinterpret_cast<__nv_bfloat16*>(pack + canon_off(n, k, kIn)) = __float2bfloat16_rn(v);
   }
   if (i < (uint32_t)(3 * kHidden * kHidden)) {
     uint32_t l = i / (kHidden * kHidden), e = i % (kHidden * kHidden);
@@ -518,106 +525,185 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
-// Shared memory of one inference CTA (256 threads = 2 threads per row).
+// ---- packed BF16x2 arithmetic (two activations per instruction)
+__device__ __forceinline__ uint32_t bf2_fma(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+__device__ __forceinline__ uint32_t bf2_mul(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ uint32_t bf2_max(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("max.bf16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+__device__ __forceinline__ uint32_t bf2_ex2(uint32_t a) {
+  uint32_t d;
+  asm("ex2.approx.ftz.bf16x2 %0, %1;" : "=r"(d) : "r"(a));
+  return d;
+}
+
+// BF16 pairs {lo, hi} of constants
+constexpr uint32_t bf2_const(uint32_t bits) { return bits | (bits << 16); }
+constexpr uint32_t kBf2Log2e = bf2_const(0x3FB9u);   // 1.4453125 ~ log2(e)
+constexpr uint32_t kBf2C1 = bf2_const(0x3F7Cu);      // 0.984375
+constexpr uint32_t kBf2C2 = bf2_const(0xBECFu);      // -0.404296875
+constexpr uint32_t kBf2C3 = bf2_const(0x3DE6u);      // 0.1123046875
+
+// softplus of two BF16 pre-activations in BF16 arithmetic:
+// max(z, 0) + u (c1 + u (c2 + u c3)) with u = 2^(-|z| log2 e), the cubic a
+// least-squares fit of log1p(u) / u on [0, 1] (coefficients rounded to
+// BF16).  Against softplus in FP32 rounded once to BF16 (the training
+// arithmetic) the pre-activation is rounded twice; the difference is at
+// most one BF16 unit in the last place of the activation.
+__device__ __forceinline__ uint32_t softplus_bf16x2(uint32_t z) {
+  uint32_t u = bf2_ex2(bf2_mul(z | 0x80008000u, kBf2Log2e));
+  uint32_t q = bf2_fma(kBf2C3, u, kBf2C2);
+  q = bf2_fma(q, u, kBf2C1);
+  return bf2_fma(q, u, bf2_max(z, 0u));
+}
+
+// Tensor-core inference: each CTA runs kGroups independent pipelines of 128
+// rows (one thread per row, 4 warps per group, one warp of every group on
+// each SM sub-partition).  A group computes its rows' features, then for
+// each layer: one elected thread issues the MMAs into the group's 64 TMEM
+// columns and commits to the group's mbarrier; the group reads its
+// accumulators back, applies bias and softplus, and writes the next
+// layer's BF16 input.  While one group waits on its MMAs the others run
+// their epilogues, which hides the tensor-core latency.
+constexpr int kGroups = 4;
+constexpr int kGroupRows = 128;
+constexpr int kTcThreads = kGroups * kGroupRows;  // 512
+constexpr uint32_t kTmemCols = 64 * kGroups;      // 256
+
 struct __align__(1024) TcSmem {
-  unsigned char w[kPackWBytes];  // W1..W4, canonical
-  unsigned char x[128 * kIn * 2];  // layer input, canonical (K = 128 or 64)
-  float bias[4][kHidden];
+  unsigned char w[kPackWBytes];               // W1..W4, canonical
+  unsigned char x[kGroups][kGroupRows * kIn * 2];  // per-group layer input (K = 128 or 64)
+  float bias[3][kHidden];                     // b2..b4 (b1 rides in W1)
   float w5[kHidden];
   float b5;
-  float half[2][128];   // partial head sums per row
-  float p[128][4];      // point (x, y, z, live) per row
-  float dist[128];
-  uint64_t bar;
+  uint64_t bar[kGroups];
   uint32_t tmem;
-  int error;
 };
 
-constexpr uint32_t kTmemCols = 64;
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+}
+__device__ __forceinline__ bool group_and(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(g + 1)
+      : "memory");
+  return r != 0u;
+}
+__device__ __forceinline__ bool group_or(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(g + 1)
+      : "memory");
+  return r != 0u;
+}
 
-// One 128-point tile through the network.  Called by all 256 threads; row
-// r = 32*(warp%4) + lane, column half ch = warp / 4.  Inputs in s.p, output
-// in s.dist.  Returns false if an MMA did not complete within the bound.
-__device__ __forceinline__ bool mlp_tile(TcSmem& s, const InputMap& m, uint32_t& phase) {
-  int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int row = 32 * (warp & 3) + lane, ch = warp >> 2;
-  // features: ch 0 -> chain 0 (chunks 0..5), ch 1 -> chain 1 (6..11) + q (12..15)
+__device__ __forceinline__ void store_chunk(unsigned char* x, int row, int k, uint32_t K, uint32_t a,
+                                            uint32_t b, uint32_t c, uint32_t d) {
+  *reinterpret_cast<uint4*>(x + canon_off(row, k, K)) = make_uint4(a, b, c, d);
+}
+
+// Network value of this thread's row (q = normalised point).  Called by the
+// 128 threads of group g together; `ok` turns false if an MMA did not
+// complete within the wait bound (the caller makes it group-uniform).
+__device__ __forceinline__ float mlp_row(TcSmem& s, const InputMap& m, int g, int row,
+                                         const float q[3], uint32_t& phase, bool& ok) {
+  unsigned char* x = s.x[g];
   {
-    float q[3];
-    normalise(m, s.p[row][0], s.p[row][1], s.p[row][2], q);
     float v[48];
-    chain_features(m, q, ch, v);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      uint4 u;
-      u.x = pack_bf16x2(v[c * 8 + 0], v[c * 8 + 1]);
-      u.y = pack_bf16x2(v[c * 8 + 2], v[c * 8 + 3]);
-      u.z = pack_bf16x2(v[c * 8 + 4], v[c * 8 + 5]);
-      u.w = pack_bf16x2(v[c * 8 + 6], v[c * 8 + 7]);
-      *reinterpret_cast<uint4*>(s.x + canon_off(row, (ch * 6 + c) * 8, kIn)) = u;
-    }
-    if (ch == 1) {
-      uint4 u;
-      u.x = pack_bf16x2(q[0], q[1]);
-      u.y = pack_bf16x2(q[2], 0.f);
-      u.z = 0u;
-      u.w = 0u;
-      *reinterpret_cast<uint4*>(s.x + canon_off(row, 96, kIn)) = u;
-      uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    for (int chain = 0; chain < 2; ++chain) {
+      chain_features(m, q, chain, v);
 #pragma unroll
-      for (int c = 13; c < 16; ++c) *reinterpret_cast<uint4*>(s.x + canon_off(row, c * 8, kIn)) = zero;
+      for (int c = 0; c < 6; ++c)
+        store_chunk(x, row, (chain * 6 + c) * 8, kIn, pack_bf16x2(v[c * 8 + 0], v[c * 8 + 1]),
+                    pack_bf16x2(v[c * 8 + 2], v[c * 8 + 3]), pack_bf16x2(v[c * 8 + 4], v[c * 8 + 5]),
+                    pack_bf16x2(v[c * 8 + 6], v[c * 8 + 7]));
     }
+    // k = 96..103: q.xyz, the two bias inputs (1.0), zeros; 104..127 zero
+    store_chunk(x, row, 96, kIn, pack_bf16x2(q[0], q[1]), pack_bf16x2(q[2], 1.0f),
+                pack_bf16x2(1.0f, 0.f), 0u);
+#pragma unroll
+    for (int c = 13; c < 16; ++c) store_chunk(x, row, c * 8, kIn, 0u, 0u, 0u, 0u);
   }
-  bool ok = true;
-  float act[32];
+  const uint32_t wq = (uint32_t)(row >> 5);  // warp within the group = TMEM lane quarter
+  const uint32_t tcol = s.tmem + ((32u * wq) << 16) + 64u * (uint32_t)g;
+  float d = 0.f;
 #pragma unroll 1
   for (int layer = 0; layer < 4; ++layer) {
-    uint32_t K = layer == 0 ? kIn : kHidden;
+    const uint32_t K = layer == 0 ? kIn : kHidden;
     fence_async_smem();
     fence_before();
-    __syncthreads();
+    group_sync(g);
     fence_after();
-    if (tid == 0) {
-      uint32_t xa = smem_addr(s.x);
+    if (row == 0) {
+      uint32_t xa = smem_addr(x);
       uint32_t wa = smem_addr(s.w + (layer == 0 ? 0u : kPackW1 + (layer - 1) * kPackWh));
 #pragma unroll 1
       for (uint32_t kk = 0; kk < K / 16; ++kk)
-        mma_bf16(s.tmem, umma_desc(xa + kk * 256u, K * 16u), umma_desc(wa + kk * 256u, K * 16u),
-                 kk > 0 ? 1u : 0u);
-      mma_commit(&s.bar);
+        mma_bf16(s.tmem + 64u * (uint32_t)g, umma_desc(xa + kk * 256u, K * 16u),
+                 umma_desc(wa + kk * 256u, K * 16u), kk > 0 ? 1u : 0u);
+      mma_commit(&s.bar[g]);
     }
-    ok = mbar_wait(&s.bar, phase) && ok;
+    ok = mbar_wait(&s.bar[g], phase) && ok;
     phase ^= 1u;
+    __syncwarp();
     fence_after();
-    tmem_ld32(s.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * ch), act);
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-      act[j] = bf16_round(softplus_approx(act[j] + s.bias[layer][32 * ch + j]));
-    if (layer < 3) {
-      // next layer's input (K = 64): this thread's 32 columns = 4 chunks
-      fence_before();
-      __syncthreads();  // every thread has read its accumulators; x is free
+    for (int half = 0; half < 2; ++half) {
+      float acc[32];
+      tmem_ld32(tcol + 32u * (uint32_t)half, acc);
+      if (layer > 0) {
+        const float4* b4 = reinterpret_cast<const float4*>(s.bias[layer - 1]) + 8 * half;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        uint4 u;
-        u.x = pack_bf16x2(act[c * 8 + 0], act[c * 8 + 1]);
-        u.y = pack_bf16x2(act[c * 8 + 2], act[c * 8 + 3]);
-        u.z = pack_bf16x2(act[c * 8 + 4], act[c * 8 + 5]);
-        u.w = pack_bf16x2(act[c * 8 + 6], act[c * 8 + 7]);
-        *reinterpret_cast<uint4*>(s.x + canon_off(row, 32 * ch + c * 8, kHidden)) = u;
+        for (int j = 0; j < 8; ++j) {
+          float4 bb = b4[j];
+          acc[4 * j] += bb.x;
+          acc[4 * j + 1] += bb.y;
+          acc[4 * j + 2] += bb.z;
+          acc[4 * j + 3] += bb.w;
+        }
+      }
+      uint32_t a[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) a[j] = softplus_bf16x2(pack_bf16x2(acc[2 * j], acc[2 * j + 1]));
+      if (layer < 3) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          store_chunk(x, row, 32 * half + 8 * c, kHidden, a[4 * c], a[4 * c + 1], a[4 * c + 2],
+                      a[4 * c + 3]);
+      } else {
+        const float4* w4 = reinterpret_cast<const float4*>(s.w5) + 8 * half;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          float4 ww = w4[j];
+          d = __fmaf_rn(__uint_as_float(a[2 * j] << 16), ww.x, d);
+          d = __fmaf_rn(__uint_as_float(a[2 * j] & 0xFFFF0000u), ww.y, d);
+          d = __fmaf_rn(__uint_as_float(a[2 * j + 1] << 16), ww.z, d);
+          d = __fmaf_rn(__uint_as_float(a[2 * j + 1] & 0xFFFF0000u), ww.w, d);
+        }
       }
     }
+    // every thread has read its accumulators before the next MMA overwrites them
+    fence_before();
   }
-  float d = 0.f;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) d = __fmaf_rn(act[j], s.w5[32 * ch + j], d);
-  s.half[ch][row] = d;
-  fence_before();
-  __syncthreads();
-  fence_after();
-  if (ch == 0) s.dist[row] = s.half[0][row] + s.half[1][row] + s.b5;
-  // block-uniform result, so every thread leaves its loop on the same trip
-  return __syncthreads_and(ok ? 1 : 0) != 0;
+  return d + s.b5;
 }
 
 __device__ __forceinline__ void tc_setup(TcSmem& s, const unsigned char* __restrict__ pack) {
@@ -625,12 +711,13 @@ __device__ __forceinline__ void tc_setup(TcSmem& s, const unsigned char* __restr
   for (uint32_t i = tid; i < kPackWBytes / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(s.w)[i] = __ldg(reinterpret_cast<const uint4*>(pack) + i);
   const float* f = reinterpret_cast<const float*>(pack + kPackWBytes);
-  for (uint32_t i = tid; i < 4 * kHidden; i += blockDim.x) s.bias[i / kHidden][i % kHidden] = f[i];
+  for (uint32_t i = tid; i < 3 * kHidden; i += blockDim.x)
+    s.bias[i / kHidden][i % kHidden] = f[kHidden + i];
   for (uint32_t i = tid; i < kHidden; i += blockDim.x) s.w5[i] = f[4 * kHidden + i];
   if (tid == 0) {
     s.b5 = f[5 * kHidden];
-    s.error = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s.bar)));
+    for (int g = 0; g < kGroups; ++g)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s.bar[g])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if ((tid >> 5) == 0) {
@@ -653,34 +740,37 @@ __device__ __forceinline__ void tc_teardown(TcSmem& s) {
                  "r"(kTmemCols));
 }
 
-// Batch evaluation: out[i] = network(pts[i]).
-__global__ void __launch_bounds__(256) k_tc_eval(InputMap m, const unsigned char* __restrict__ pack,
-                                                 const float* __restrict__ pts, uint32_t n,
-                                                 float* __restrict__ out, int* __restrict__ err) {
+__device__ __forceinline__ TcSmem& tc_smem(unsigned char* raw) {
+  return *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
+}
+
+// Batch evaluation: out[i] = network(pts[i]).  Group tiles are claimed
+// round-robin: tile = (block * kGroups + g) + k * (grid * kGroups).
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc_eval(InputMap m,
+                                                           const unsigned char* __restrict__ pack,
+                                                           const float* __restrict__ pts, uint32_t n,
+                                                           float* __restrict__ out,
+                                                           int* __restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
-  TcSmem& s = *reinterpret_cast<TcSmem*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  TcSmem& s = tc_smem(smem_raw);
   tc_setup(s, pack);
+  const int tid = threadIdx.x, g = tid >> 7, row = tid & 127;
   uint32_t phase = 0;
-  int tid = threadIdx.x;
-  uint32_t tiles = (n + 127) / 128;
+  const uint32_t tiles = (n + kGroupRows - 1) / kGroupRows;
+  const uint32_t stride = gridDim.x * kGroups;
   bool ok = true;
-  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    if (tid < 128) {
-      uint32_t i = tile * 128 + tid;
-      bool live = i < n;
-      s.p[tid][0] = live ? pts[3 * (size_t)i] : 0.f;
-      s.p[tid][1] = live ? pts[3 * (size_t)i + 1] : 0.f;
-      s.p[tid][2] = live ? pts[3 * (size_t)i + 2] : 0.f;
-    }
-    __syncthreads();
-    ok = mlp_tile(s, m, phase);
-    if (tid < 128) {
-      uint32_t i = tile * 128 + tid;
-      if (i < n) out[i] = s.dist[tid];
-    }
+  for (uint32_t tile = blockIdx.x * kGroups + g; tile < tiles; tile += stride) {
+    uint32_t i = tile * kGroupRows + row;
+    bool live = i < n;
+    float p0 = live ? pts[3 * (size_t)i] : 0.f, p1 = live ? pts[3 * (size_t)i + 1] : 0.f,
+          p2 = live ? pts[3 * (size_t)i + 2] : 0.f;
+    float q[3];
+    normalise(m, p0, p1, p2, q);
+    float dv = mlp_row(s, m, g, row, q, phase, ok);
+    if (live) out[i] = dv;
+    if (!group_and(g, ok)) break;
   }
-  if (!ok && tid == 0) atomicExch(err, 1);
+  if (!ok && row == 0) atomicExch(err, 1);
   tc_teardown(s);
 }
 
@@ -725,118 +815,197 @@ __global__ void __launch_bounds__(128) k_ref_eval(InputMap m, const float* __res
 
 // ------------------------------------------------------------- tracing
 struct MarchDev {
-  float alpha;        // step = alpha * network distance (1 / Lipschitz bound)
-  float switch_dist;  // hand over to the exact field below this distance
+  float alpha;        // network step = alpha * network distance (safety / Lipschitz bound)
+  float switch_dist;  // hand over to the exact field below this network distance
   float min_step;     // floor of a network step
   float tmax;
   uint32_t max_steps;  // network steps before handing over regardless
+  float bmin[3], bmax[3];  // the network's box; the march stays inside it
 };
 
-// Neural phase.  Rows are ray slots; a warp of row owners (warps 0-3) refills
-// its idle slots from the pixel cursor (claim order = 8x4 tiles).  Rays that
-// come within switch_dist of the surface (or exhaust their network steps)
-// are appended to the refinement queue {pixel, t, steps}; rays that leave
-// [0, tmax] are written as misses.
-__global__ void __launch_bounds__(256) k_nsdf_march(InputMap m, const unsigned char* __restrict__ pack,
-                                                    MarchDev md, CamDev cam, uint32_t w, uint32_t h,
-                                                    uint32_t* __restrict__ counters,
-                                                    uint4* __restrict__ queue,
-                                                    float4* __restrict__ out,
-                                                    int* __restrict__ err) {
+// Exact phase parameters.
+struct RefineDev {
+  uint32_t max_steps;   // exact evaluations per ray (march + bracket + root)
+  uint32_t root_steps;  // regula-falsi steps on a bracketed crossing
+  float relax;          // an exact step may grow to relax x (step_factor * d) along a secant
+  float ceiling;        // no surface above this height (bound of the field)
+};
+
+// Slab test of the ray against the box: [t0, t1] with t0 >= 0 (empty if t0 >= t1).
+__device__ __forceinline__ void box_span(const MarchDev& md, const V3& o, const V3& d, float& t0,
+                                         float& t1) {
+  float o3[3] = {o.x, o.y, o.z}, d3[3] = {d.x, d.y, d.z};
+  t0 = 0.f;
+  t1 = md.tmax;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float inv = 1.0f / d3[k];
+    float ta = (md.bmin[k] - o3[k]) * inv, tb = (md.bmax[k] - o3[k]) * inv;
+    t0 = fmaxf(t0, fminf(ta, tb));
+    t1 = fminf(t1, fmaxf(ta, tb));
+  }
+}
+
+// Appends this lane's entry to the exact-phase queue (warp-aggregated).
+__device__ __forceinline__ void queue_push(bool push, uint4 e, uint32_t* counters,
+                                           uint4* __restrict__ queue) {
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t pm = __ballot_sync(0xFFFFFFFFu, push);
+  if (pm == 0u) return;
+  uint32_t leader = __ffs(pm) - 1u, base = 0;
+  if (lane == leader) base = atomicAdd(&counters[1], (uint32_t)__popc(pm));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (push) queue[base + __popc(pm & ((1u << lane) - 1u))] = e;
+}
+
+// Neural phase.  Each group of 128 threads marches 128 rays (one per
+// thread) through the network; a warp refills its idle rows from the pixel
+// cursor (claim order = 8x4 pixel tiles) once 8 of them are idle.  A ray
+// starts where it enters the network's box and steps by
+// max(alpha * d_net, min_step).  It is queued for the exact phase as
+// {pixel, t, t_lo, steps} when d_net < switch_dist (t_lo = the previous
+// network point, a bracket candidate), when it leaves the box before tmax
+// (t = t_lo = exit), or after max_steps network steps; rays that reach tmax
+// inside the box are written as misses.
+__global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_march(InputMap m,
+                                                              const unsigned char* __restrict__ pack,
+                                                              MarchDev md, CamDev cam, uint32_t w,
+                                                              uint32_t h, uint32_t* __restrict__ counters,
+                                                              unsigned long long* __restrict__ totals,
+                                                              uint4* __restrict__ queue,
+                                                              float4* __restrict__ out,
+                                                              int* __restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
-  TcSmem& s = *reinterpret_cast<TcSmem*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ int any_live;
+  TcSmem& s = tc_smem(smem_raw);
   tc_setup(s, pack);
+  const int tid = threadIdx.x, g = tid >> 7, row = tid & 127;
+  const uint32_t lane = tid & 31u;
   uint32_t phase = 0;
-  int tid = threadIdx.x, lane = tid & 31;
-  uint32_t tiles_x = (w + 7) / 8;
-  uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
-  // ray state lives in the row owners (threads 0..127)
-  bool live = false, exhausted = false;
+  const uint32_t tiles_x = (w + 7) / 8;
+  const uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
+  bool live = false, exhausted = false, ok = true;
   uint32_t pix = 0, steps = 0;
-  V3 o = {0, 0, 0}, d = {0, 0, 1};
-  float t = 0.f;
-  bool ok = true;
-  for (uint32_t guard = 0; guard < (1u << 24) && ok; ++guard) {
-    if (tid == 0) any_live = 0;
-    __syncthreads();
-    if (tid < 128) {
-      uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
-      uint32_t nidle = __popc(idle);
-      if (!exhausted && (nidle >= 8u || nidle == 32u)) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&counters[0], nidle);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base + nidle >= total) exhausted = true;
-        if (!live) {
-          uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
-          uint32_t tile = i >> 5, l = i & 31u;
-          uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
-          if (i < total && x < w && y < h) {
-            generate_ray(cam, w, h, x, y, o, d);
-            pix = y * w + x;
-            t = 0.f;
-            steps = 0;
+  V3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+  float t = 0.f, t_lo = 0.f, t_end = 0.f;
+  uint32_t n_live = 0, n_rows = 0;  // network evaluations of rays / rows computed
+  for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
+    bool outside = false;  // a new ray that misses the box goes straight to the exact phase
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && nidle >= 8u) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&counters[0], nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= total) exhausted = true;
+      if (!live) {
+        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+        uint32_t tile = i >> 5, l = i & 31u;
+        uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
+        if (i < total && x < w && y < h) {
+          generate_ray(cam, w, h, x, y, o, d);
+          pix = y * w + x;
+          steps = 0;
+          float t0, t1;
+          box_span(md, o, d, t0, t1);
+          if (t0 < t1) {
+            t = t0;
+            t_lo = t0;
+            t_end = t1;
             live = true;
+          } else {
+            outside = true;
           }
         }
       }
-      V3 p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
-      s.p[tid][0] = p.x;
-      s.p[tid][1] = p.y;
-      s.p[tid][2] = p.z;
-      uint32_t live_b = __ballot_sync(0xFFFFFFFFu, live);
-      if (lane == 0 && (live_b != 0u || !exhausted)) atomicOr(&any_live, 1);
     }
-    __syncthreads();
-    if (!any_live) break;
-    ok = mlp_tile(s, m, phase);
-    if (tid < 128 && live) {
-      float dn = s.dist[tid];
+    queue_push(outside, make_uint4(pix, 0u, 0u, 0u), counters, queue);
+    if (!group_or(g, live || !exhausted)) break;
+    float q[3];
+    normalise(m, __fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z), q);
+    float dn = mlp_row(s, m, g, row, q, phase, ok);
+    if (!group_and(g, ok)) break;
+    ++n_rows;
+    n_live += live ? 1u : 0u;
+    bool push = false;
+    uint4 e = make_uint4(0u, 0u, 0u, 0u);
+    if (live) {
       ++steps;
-      if (dn < md.switch_dist || steps >= md.max_steps) {
-        uint32_t slot = atomicAdd(&counters[1], 1u);
-        queue[slot] = make_uint4(pix, __float_as_uint(t), steps, 0u);
-        live = false;
+      if (dn < md.switch_dist) {
+        push = true;
+        e = make_uint4(pix, __float_as_uint(t), __float_as_uint(t_lo), steps);
       } else {
+        t_lo = t;
         t += fmaxf(md.alpha * dn, md.min_step);
-        if (t > md.tmax) {
-          out[2 * (size_t)pix] = make_float4(0.f, 0.f, 0.f, 0.f);
-          out[2 * (size_t)pix + 1] =
-              make_float4(0.f, 0.f, __uint_as_float(steps), __uint_as_float(0u));
-          live = false;
+        if (t >= t_end) {
+          if (t_end >= md.tmax) {
+            out[2 * (size_t)pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+            out[2 * (size_t)pix + 1] =
+                make_float4(0.f, 0.f, __uint_as_float(steps), __uint_as_float(0u));
+            live = false;
+          } else {
+            push = true;
+            e = make_uint4(pix, __float_as_uint(t_end), __float_as_uint(t_end), steps);
+          }
+        } else if (steps >= md.max_steps) {
+          push = true;
+          e = make_uint4(pix, __float_as_uint(t), __float_as_uint(t), steps);
         }
       }
+      if (push) live = false;
     }
+    queue_push(push, e, counters, queue);
   }
-  if (!ok && tid == 0) atomicExch(err, 1);
+  n_live = __reduce_add_sync(0xFFFFFFFFu, n_live);
+  n_rows = __reduce_add_sync(0xFFFFFFFFu, n_rows);
+  if (lane == 0) {
+    atomicAdd(&totals[0], (unsigned long long)n_live);
+    atomicAdd(&totals[3], (unsigned long long)n_rows);
+  }
+  if (!ok && row == 0) atomicExch(err, 1);
   tc_teardown(s);
 }
 
-// Exact phase: continue each queued ray from its t with the exact field
-// (t += step_factor * d, hit when d < eps), then the central-difference
-// normal, as the exact tracer does.  Same state machine and lane refill as
-// k_sdf; the step count reported is network steps + exact steps.
-__global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f,
-                                                    uint32_t exact_max_steps, CamDev cam,
-                                                    uint32_t w, uint32_t h,
+// Exact phase, one lane per ray with lane refill (from the queue, or from
+// the pixel cursor when `direct`: every pixel from t = 0, the same method
+// without the network).  One field evaluation per trip of a state machine:
+//   march  t += step_factor * d (the exact tracer's rule); the step may
+//          grow along the secant through the last two samples up to relax x
+//          that (relax <= 1: plain rule).  d < eps: hit at t.  d < 0 (the
+//          sample is inside): the crossing is bracketed by the last outside
+//          sample and refined.  Going up above `ceiling`: miss.
+//   probe  the ray arrived inside from the network: check the bracket
+//          candidate t_lo; if it is outside the crossing lies in
+//          [t_lo, t], else march again from t = 0 (the network skipped
+//          over the surface).
+//   root   Illinois regula falsi on the bracket, root_steps evaluations or
+//          until |d| < 1e-6.
+//   normal the exact tracer's central differences (delta = 0.002 t).
+// The step count written is network steps + exact march/probe/root
+// evaluations (normals excluded, as in the exact tracer).
+enum : uint32_t { kMarch = 0, kProbe = 1, kRoot = 2, kNormal = 3 };
+
+__global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, RefineDev rd,
+                                                    CamDev cam, uint32_t w, uint32_t h, int direct,
                                                     const uint4* __restrict__ queue,
                                                     uint32_t* __restrict__ counters,
+                                                    unsigned long long* __restrict__ totals,
                                                     float4* __restrict__ out) {
   extern __shared__ uint32_t perm_smem[];
   load_perm(perm, perm_smem);
   Perm P = perm_view(perm_smem);
-  uint32_t lane = threadIdx.x & 31u;
-  uint32_t total = counters[1];
-  bool live = false, exhausted = false;
-  uint32_t pix = 0, steps = 0, base_steps = 0, phase = 0;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t total = direct ? w * h : counters[1];
+  bool live = false, exhausted = false, have_lo = false, restarted = false;
+  uint32_t pix = 0, steps = 0, base_steps = 0, mode = kMarch, tap = 0, iters = 0;
+  int side = 0;
   V3 o = {0, 0, 0}, d = {0, 0, 1}, p = {0, 0, 0};
-  float t = 0.f, delta = 0.f, nx = 0.f, ny = 0.f, nz = 0.f, plus = 0.f;
+  float t = 0.f, t_lo = 0.f, a = 0.f, va = 0.f, b = 0.f, vb = 0.f, delta = 0.f;
+  float nx = 0.f, ny = 0.f, nz = 0.f, plus = 0.f;
+  uint32_t n_exact = 0, n_normal = 0;  // evaluations: march/probe/root, normal taps
   for (;;) {
     uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
     uint32_t nidle = __popc(idle);
-    if (!exhausted && (nidle >= 4u || nidle == 32u)) {
+    if (!exhausted && nidle >= 4u) {
       uint32_t base = 0;
       if (lane == 0) base = atomicAdd(&counters[2], nidle);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
@@ -844,13 +1013,16 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f,
       if (!live) {
         uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
         if (i < total) {
-          uint4 q = queue[i];
-          pix = q.x;
+          uint4 e = direct ? make_uint4(i, 0u, 0u, 0u) : queue[i];
+          pix = e.x;
           generate_ray(cam, w, h, pix % w, pix / w, o, d);
-          t = __uint_as_float(q.y);
-          base_steps = q.z;
+          t = __uint_as_float(e.y);
+          t_lo = __uint_as_float(e.z);
+          base_steps = e.w;
           steps = 0;
-          phase = 0;
+          mode = kMarch;
+          have_lo = false;
+          restarted = false;
           live = true;
         }
       }
@@ -861,39 +1033,111 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f,
     }
     if (!live) continue;
     V3 qp;
-    if (phase == 0) {
+    if (mode == kMarch) {
+      qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+    } else if (mode == kProbe) {
+      qp = v3(__fmaf_rn(a, d.x, o.x), __fmaf_rn(a, d.y, o.y), __fmaf_rn(a, d.z, o.z));
+    } else if (mode == kRoot) {
       qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
     } else {
-      float sd = (phase & 1u) ? delta : -delta;
+      float sd = (tap & 1u) ? -delta : delta;
       qp = p;
-      if (phase <= 2) qp.x = p.x + sd;
-      else if (phase <= 4) qp.y = p.y + sd;
+      if (tap < 2) qp.x = p.x + sd;
+      else if (tap < 4) qp.y = p.y + sd;
       else qp.z = p.z + sd;
     }
     float v = terrain_density(P, qp, f.octaves, f.scale, f.amp);
-    uint32_t status = 3;
-    if (phase == 0) {
+    if (mode == kNormal) ++n_normal;
+    else ++n_exact;
+    uint32_t status = 3;  // 3 = still running
+    bool begin_root = false, hit_here = false;
+    if (mode == kMarch) {
       ++steps;
-      if (v < f.eps) {
-        p = qp;
-        delta = 0.002f * t;
-        phase = 1;
+      if (v < 0.f) {
+        if (have_lo) {
+          b = t;
+          vb = v;
+          begin_root = true;
+        } else if (t_lo < t && !restarted) {
+          b = t;
+          vb = v;
+          a = t_lo;
+          mode = kProbe;
+        } else {
+          hit_here = true;
+        }
+      } else if (v < f.eps) {
+        hit_here = true;
+      } else if (d.y >= 0.f && qp.y > rd.ceiling) {
+        status = 0;
       } else {
-        t = __fmaf_rn(f.step_factor, v, t);
+        float step = f.step_factor * v;
+        if (have_lo && va > v && rd.relax > 1.f) {
+          float sec = v * (t - a) / (va - v);  // distance to the secant's root
+          step = fminf(fmaxf(step, sec), rd.relax * step);
+        }
+        a = t;
+        va = v;
+        have_lo = true;
+        t += step;
         if (t > f.tmax) status = 0;
-        else if (steps >= exact_max_steps) status = 2;
+        else if (steps >= rd.max_steps) status = 2;
+      }
+    } else if (mode == kProbe) {
+      ++steps;
+      if (v > 0.f) {
+        va = v;
+        begin_root = true;
+      } else {
+        // the network passed the crossing: march again from the camera
+        t = 0.f;
+        t_lo = 0.f;
+        have_lo = false;
+        restarted = true;
+        mode = kMarch;
+        if (steps >= rd.max_steps) status = 2;
+      }
+    } else if (mode == kRoot) {
+      ++steps;
+      if (fabsf(v) < 1e-6f || ++iters >= rd.root_steps) {
+        hit_here = true;
+      } else {
+        if (v < 0.f) {
+          b = t;
+          vb = v;
+          if (side < 0) va *= 0.5f;
+          side = -1;
+        } else {
+          a = t;
+          va = v;
+          if (side > 0) vb *= 0.5f;
+          side = 1;
+        }
+        t = b - vb * (b - a) / (vb - va);
       }
     } else {
-      if (phase & 1u) {
+      if ((tap & 1u) == 0u) {
         plus = v;
       } else {
         float diff = plus - v;
-        if (phase == 2) nx = diff;
-        else if (phase == 4) ny = diff;
+        if (tap == 1) nx = diff;
+        else if (tap == 3) ny = diff;
         else nz = diff;
       }
-      if (phase == 6) status = 1;
-      else ++phase;
+      if (tap == 5) status = 1;
+      else ++tap;
+    }
+    if (begin_root) {
+      mode = kRoot;
+      side = 0;
+      iters = 0;
+      t = b - vb * (b - a) / (vb - va);
+    }
+    if (hit_here) {
+      p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+      delta = 0.002f * t;
+      mode = kNormal;
+      tap = 0;
     }
     if (status != 3) {
       float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1;
@@ -910,23 +1154,24 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f,
       live = false;
     }
   }
+  n_exact = __reduce_add_sync(0xFFFFFFFFu, n_exact);
+  n_normal = __reduce_add_sync(0xFFFFFFFFu, n_normal);
+  if (lane == 0) {
+    atomicAdd(&totals[1], (unsigned long long)n_exact);
+    atomicAdd(&totals[2], (unsigned long long)n_normal);
+  }
 }
 
-// Lipschitz estimate: max over sample points of the finite-difference
-// gradient norm of the network (points in pts, 4 evaluations each: p, p+hx,
-// p+hy, p+hz laid out by the caller).
+// Finite-difference gradient norm of the network at n sample points (vals
+// holds 4 evaluations per point: p, p+hx, p+hy, p+hz).
 __global__ void k_grad_norm(const float* __restrict__ vals, uint32_t n, float h,
-                            unsigned int* __restrict__ max_bits) {
+                            float* __restrict__ norms) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  float g = 0.f;
-  if (i < n) {
-    float v0 = vals[4 * (size_t)i];
-    float gx = (vals[4 * (size_t)i + 1] - v0) / h, gy = (vals[4 * (size_t)i + 2] - v0) / h,
-          gz = (vals[4 * (size_t)i + 3] - v0) / h;
-    g = sqrtf(gx * gx + gy * gy + gz * gz);
-  }
-  for (int off = 16; off > 0; off >>= 1) g = fmaxf(g, __shfl_xor_sync(0xFFFFFFFFu, g, off));
-  if ((threadIdx.x & 31u) == 0) atomicMax(max_bits, __float_as_uint(g));
+  if (i >= n) return;
+  float v0 = vals[4 * (size_t)i];
+  float gx = (vals[4 * (size_t)i + 1] - v0) / h, gy = (vals[4 * (size_t)i + 2] - v0) / h,
+        gz = (vals[4 * (size_t)i + 3] - v0) / h;
+  norms[i] = sqrtf(gx * gx + gy * gy + gz * gz);
 }
 
 }  // namespace nsdf
@@ -955,7 +1200,10 @@ struct re_nsdf {
   cudaGraphExec_t graph_exec = nullptr;
   float graph_lr = -1.f;
   // tracing scratch
-  uint32_t* counters = nullptr;  // [0] pixel cursor [1] queue size [2] refine cursor
+  // [0] pixel cursor [1] queue size [2] refine cursor; from byte 16, u64
+  // totals of the last trace: network evaluations of rays, exact
+  // evaluations (march/probe/root), exact normal taps, network rows computed
+  uint32_t* counters = nullptr;
   uint4* queue = nullptr;
   size_t queue_cap = 0;
   int* err = nullptr;
@@ -1067,11 +1315,11 @@ constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
 template <typename K>
 int tc_grid(K kernel) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, kTcSmemBytes) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTcThreads, kTcSmemBytes) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  per_sm = std::min(per_sm, 4);  // 4 x 64 TMEM columns of 512
+  per_sm = std::min(per_sm, 2);  // 2 x 256 TMEM columns of 512
   return per_sm * sm_count();
 }
 
@@ -1179,7 +1427,7 @@ RE_API re_status re_nsdf_create(const re_nsdf_config* cfg, re_nsdf** out) {
   if (e == cudaSuccess) e = cudaMalloc(&s->adam_v, kNumParams * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->pack, re::nsdf::kPackBytes);
   if (e == cudaSuccess) e = cudaMalloc(&s->step_ctr, 16);
-  if (e == cudaSuccess) e = cudaMalloc(&s->counters, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&s->counters, 64);
   if (e == cudaSuccess) e = cudaMalloc(&s->err, 4);
   if (e == cudaSuccess) e = cudaMemset(s->adam_m, 0, kNumParams * 4);
   if (e == cudaSuccess) e = cudaMemset(s->adam_v, 0, kNumParams * 4);
@@ -1376,9 +1624,9 @@ RE_API re_status re_nsdf_eval(re_nsdf* s, const float* d_pts, uint32_t n, float*
   if (st != RE_OK) return st;
   auto k = re::nsdf::k_tc_eval;
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)re::kTcSmemBytes));
-  int grid = std::min<int>(re::tc_grid(k), (int)((n + 127) / 128));
+  int grid = std::min<int>(re::tc_grid(k), (int)((n + 511) / 512));
   RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
-  k<<<grid, 256, re::kTcSmemBytes, cs>>>(s->map, s->pack, d_pts, n, d_out, s->err);
+  k<<<grid, re::nsdf::kTcThreads, re::kTcSmemBytes, cs>>>(s->map, s->pack, d_pts, n, d_out, s->err);
   RE_CHECK_LAUNCH("re_nsdf_eval: launch");
   int herr = 0;
   RE_CUDA(cudaMemcpyAsync(&herr, s->err, 4, cudaMemcpyDeviceToHost, cs));
@@ -1399,13 +1647,14 @@ RE_API re_status re_nsdf_eval_reference(re_nsdf* s, const float* d_pts, uint32_t
   return RE_OK;
 }
 
-// Lipschitz estimate of the network over `samples` training points:
-// max |grad| by forward differences with step h.
-RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h, float* out,
-                                   void* stream) {
+// Lipschitz estimate of the network over `samples` training points: the
+// `quantile` (1 = the maximum) of the forward-difference gradient norms
+// with step h.
+RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h, float quantile,
+                                   float* out, void* stream) {
   re_status st = re::check(s, "re_nsdf_lipschitz");
   if (st != RE_OK) return st;
-  if (!out || samples == 0 || !(h > 0.f) || !s->data)
+  if (!out || samples == 0 || !(h > 0.f) || !(quantile > 0.f && quantile <= 1.f) || !s->data)
     return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_lipschitz: bad arguments or no data");
   cudaStream_t cs = (cudaStream_t)stream;
   uint32_t n = std::min(samples, s->npts);
@@ -1417,49 +1666,60 @@ RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h, float*
     for (int k = 0; k < 4; ++k)
       for (int a = 0; a < 3; ++a) q[12 * (size_t)i + 3 * k + a] = p[a] + ((k == a + 1) ? h : 0.f);
   }
-  float *dq = nullptr, *dv = nullptr;
-  unsigned int* dm = nullptr;
+  float *dq = nullptr, *dv = nullptr, *dn = nullptr;
+  std::vector<float> norms(n);
   RE_CUDA(cudaMalloc(&dq, q.size() * 4));
   cudaError_t e = cudaMalloc(&dv, (size_t)n * 4 * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&dm, 4);
+  if (e == cudaSuccess) e = cudaMalloc(&dn, (size_t)n * 4);
   if (e == cudaSuccess) e = cudaMemcpy(dq, q.data(), q.size() * 4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(dm, 0, 4);
   if (e == cudaSuccess) {
     st = re_nsdf_eval(s, dq, 4 * n, dv, stream);
     if (st == RE_OK) {
-      re::nsdf::k_grad_norm<<<(n + 255) / 256, 256, 0, cs>>>(dv, n, h, dm);
+      re::nsdf::k_grad_norm<<<(n + 255) / 256, 256, 0, cs>>>(dv, n, h, dn);
       e = cudaGetLastError();
-      unsigned int bits = 0;
-      if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, dm, 4, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(norms.data(), dn, (size_t)n * 4, cudaMemcpyDeviceToHost, cs);
       if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
-      float v;
-      std::memcpy(&v, &bits, 4);
-      *out = v;
-      s->lipschitz = v;
     }
   }
   cudaFree(dq);
   cudaFree(dv);
-  cudaFree(dm);
+  cudaFree(dn);
   if (st != RE_OK) return st;
   if (e != cudaSuccess) return re::cuda_fail(e, "re_nsdf_lipschitz");
+  size_t k = std::min<size_t>(n - 1, (size_t)std::ceil((double)quantile * n) - 1);
+  std::nth_element(norms.begin(), norms.begin() + k, norms.end());
+  *out = norms[k];
+  s->lipschitz = norms[k];
   return RE_OK;
 }
 
-RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
-                               const re_nsdf_trace_params* tp, const re_camera* cam, uint32_t w,
-                               uint32_t h, re_sdf_hit* d_out, void* stream) {
-  re_status st = re::check(s, "re_nsdf_trace");
+namespace re {
+namespace {
+re_status trace_check(re_nsdf* s, const re_sdf_params* field, const re_nsdf_trace_params* tp,
+                      const re_camera* cam, uint32_t w, uint32_t h, re_sdf_hit* d_out,
+                      const char* fn) {
+  re_status st = check(s, fn);
   if (st != RE_OK) return st;
-  st = re::check_field(field, "re_nsdf_trace");
+  st = check_field(field, fn);
   if (st != RE_OK) return st;
-  if (!tp || !cam || !d_out || w < 2 || h < 2)
-    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace: bad arguments");
-  if ((uint64_t)w * h > (1ull << 28)) return re::fail(RE_ERR_LIMIT, "re_nsdf_trace: image > 2^28 pixels");
-  if (!(tp->lipschitz > 0.f)) return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace: lipschitz must be > 0");
+  if (!tp || !cam || !d_out || w < 2 || h < 2) return fail(RE_ERR_INVALID_ARG, "%s: bad arguments", fn);
+  if ((uint64_t)w * h > (1ull << 28)) return fail(RE_ERR_LIMIT, "%s: image > 2^28 pixels", fn);
+  if (!(tp->flags & RE_NSDF_EXACT_ONLY) && !(tp->lipschitz > 0.f && tp->safety > 0.f))
+    return fail(RE_ERR_INVALID_ARG, "%s: lipschitz and safety must be > 0", fn);
+  return RE_OK;
+}
+}  // namespace
+}  // namespace re
+
+RE_API re_status re_nsdf_trace_network(re_nsdf* s, const re_sdf_params* field,
+                                       const re_nsdf_trace_params* tp, const re_camera* cam,
+                                       uint32_t w, uint32_t h, re_sdf_hit* d_out, void* stream) {
+  re_status st = re::trace_check(s, field, tp, cam, w, h, d_out, "re_nsdf_trace_network");
+  if (st != RE_OK) return st;
   cudaStream_t cs = (cudaStream_t)stream;
+  const bool exact_only = (tp->flags & RE_NSDF_EXACT_ONLY) != 0u;
   size_t need = (size_t)w * h;
-  if (s->queue_cap < need) {
+  if (!exact_only && s->queue_cap < need) {
     RE_CUDA(cudaStreamSynchronize(cs));
     cudaFree(s->queue);
     s->queue = nullptr;
@@ -1467,23 +1727,43 @@ RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
     RE_CUDA(cudaMalloc(&s->queue, need * sizeof(uint4)));
     s->queue_cap = need;
   }
+  RE_CUDA(cudaMemsetAsync(s->counters, 0, 64, cs));
+  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
+  if (exact_only) return RE_OK;
   st = re::ensure_pack(s, cs);
   if (st != RE_OK) return st;
+  unsigned long long* totals = reinterpret_cast<unsigned long long*>(s->counters + 4);
   re::nsdf::MarchDev md;
   md.alpha = tp->safety / tp->lipschitz;
   md.switch_dist = tp->switch_dist;
   md.min_step = tp->min_step;
   md.tmax = field->tmax;
   md.max_steps = tp->max_network_steps ? tp->max_network_steps : 256;
-  re::CamDev cd = re::cam_dev(*cam);
-  RE_CUDA(cudaMemsetAsync(s->counters, 0, 16, cs));
-  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
+  for (int k = 0; k < 3; ++k) {
+    float half = 1.0f / s->map.inv_half[k];
+    md.bmin[k] = s->map.center[k] - half;
+    md.bmax[k] = s->map.center[k] + half;
+  }
   auto k = re::nsdf::k_nsdf_march;
-  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)re::kTcSmemBytes));
-  k<<<re::tc_grid(k), 256, re::kTcSmemBytes, cs>>>(s->map, s->pack, md, cd, w, h, s->counters,
-                                                   s->queue, reinterpret_cast<float4*>(d_out),
-                                                   s->err);
-  RE_CHECK_LAUNCH("re_nsdf_trace: march launch");
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)re::kTcSmemBytes));
+  k<<<re::tc_grid(k), re::nsdf::kTcThreads, re::kTcSmemBytes, cs>>>(
+      s->map, s->pack, md, re::cam_dev(*cam), w, h, s->counters, totals, s->queue,
+      reinterpret_cast<float4*>(d_out), s->err);
+  RE_CHECK_LAUNCH("re_nsdf_trace_network: march launch");
+  return RE_OK;
+}
+
+RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
+                                     const re_nsdf_trace_params* tp, const re_camera* cam,
+                                     uint32_t w, uint32_t h, re_sdf_hit* d_out, void* stream) {
+  re_status st = re::trace_check(s, field, tp, cam, w, h, d_out, "re_nsdf_trace_exact");
+  if (st != RE_OK) return st;
+  const bool exact_only = (tp->flags & RE_NSDF_EXACT_ONLY) != 0u;
+  if (!exact_only && s->queue_cap < (size_t)w * h)
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace_exact: no network phase for this image");
+  cudaStream_t cs = (cudaStream_t)stream;
+  unsigned long long* totals = reinterpret_cast<unsigned long long*>(s->counters + 4);
   auto kr = re::nsdf::k_sdf_refine;
   RE_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)re::kPermSmemBytes));
@@ -1492,23 +1772,41 @@ RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  uint32_t exact_steps = tp->max_exact_steps ? tp->max_exact_steps : field->max_steps;
+  re::nsdf::RefineDev rd;
+  rd.max_steps = tp->max_exact_steps ? tp->max_exact_steps : field->max_steps;
+  rd.root_steps = tp->root_steps ? tp->root_steps : 4;
+  rd.relax = tp->relax;
+  // |Perlin| <= 2 (each corner term |g . r| <= |r_x| + |r_y| <= 2 and the
+  // interpolation is convex), so fBm <= 2 (2 - 2^(1 - octaves)) and the
+  // density is positive above this height
+  rd.ceiling =
+      2.0f * std::fabs(field->amplitude) * (2.0f - std::ldexp(1.0f, 1 - (int)field->octaves)) + 1e-3f;
   kr<<<per_sm * re::sm_count(), 256, re::kPermSmemBytes, cs>>>(
-      re::perm_of(field->seed), re::field_of(*field), exact_steps, cd, w, h, s->queue, s->counters,
-      reinterpret_cast<float4*>(d_out));
-  RE_CHECK_LAUNCH("re_nsdf_trace: refine launch");
+      re::perm_of(field->seed), re::field_of(*field), rd, re::cam_dev(*cam), w, h,
+      exact_only ? 1 : 0, s->queue, s->counters, totals, reinterpret_cast<float4*>(d_out));
+  RE_CHECK_LAUNCH("re_nsdf_trace_exact: refine launch");
   return RE_OK;
 }
 
-RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined, int* error) {
+RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
+                               const re_nsdf_trace_params* tp, const re_camera* cam, uint32_t w,
+                               uint32_t h, re_sdf_hit* d_out, void* stream) {
+  re_status st = re_nsdf_trace_network(s, field, tp, cam, w, h, d_out, stream);
+  if (st != RE_OK) return st;
+  return re_nsdf_trace_exact(s, field, tp, cam, w, h, d_out, stream);
+}
+
+RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined, int* error,
+                                      uint64_t* evals) {
   re_status st = re::check(s, "re_nsdf_trace_status");
   if (st != RE_OK) return st;
-  uint32_t c[4] = {0, 0, 0, 0};
+  uint32_t c[16] = {};
   int e = 0;
-  RE_CUDA(cudaMemcpy(c, s->counters, 16, cudaMemcpyDeviceToHost));
+  RE_CUDA(cudaMemcpy(c, s->counters, 64, cudaMemcpyDeviceToHost));
   RE_CUDA(cudaMemcpy(&e, s->err, 4, cudaMemcpyDeviceToHost));
   if (num_refined) *num_refined = c[1];
   if (error) *error = e;
+  if (evals) std::memcpy(evals, c + 4, 4 * sizeof(uint64_t));
   return RE_OK;
 }
 

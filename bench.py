@@ -526,6 +526,120 @@ class NeuralTerrainSDF:
         return TerrainSDF.cpu_baseline(self, budget_s)
 
 
+class BatchWavefront:
+    """32 seeded scenes (soups of 10k-2M triangles and volumetric terrains)
+    at 640x360 / 1280x720 / 1920x1080, 1 spp path tracing to depth 4, one
+    persistent launch per frame replayed from a CUDA graph, autotuned."""
+    name = "batch32"
+
+    def __init__(self, torch):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.cfg = rb.configs.BatchConfig()
+        t0 = time.perf_counter()
+        self.batch, self.meshes = self.cfg.build()
+        self.build_s = time.perf_counter() - t0
+        self.out = torch.empty(self.batch.total_pixels, dtype=torch.float32, device="cuda")
+        self.tuning = self.batch.autotune(self.out)
+        self.work = self.batch.counts(self.out)
+        self.batch.render(self.out, graph=True)
+        torch.cuda.synchronize()
+        st = self.batch.stats()
+        if st["error"]:
+            raise RuntimeError("batch frame reported a wait-bound error")
+        self.rays = st["rays"]
+        self.rays_per_step = int(self.rays.sum())
+        self.kernels_per_step = 1
+
+    def config(self):
+        sp = self.cfg.specs()
+        return {"workload": f"batched wavefront path tracing: {len(sp)} seeded scenes "
+                            f"({sum(s['kind'] == 'soup' for s in sp)} soups, "
+                            f"{sum(s['kind'] == 'terrain' for s in sp)} fBm terrains), resolutions "
+                            "from {640x360, 1280x720, 1920x1080}, 1 spp, depth 4 Lambertian; one "
+                            "persistent launch per frame from a captured CUDA graph",
+                "pixels": self.batch.total_pixels,
+                "triangles": int(sum(s.get("num_tris", 0) for s in sp)),
+                "rays_per_bounce": {"mesh": [int(x) for x in self.rays[:, 0]],
+                                    "terrain": [int(x) for x in self.rays[:, 1]]},
+                "work": self.work, "tuning": self.tuning,
+                "scene_build_s": round(self.build_s, 2),
+                "rays_per_step": self.rays_per_step, "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        return [("batch", lambda: self.batch.render(self.out, stream=stream, graph=True))]
+
+    def alg_bytes(self):
+        w = self.work
+        cont = int(self.rays[1:].sum())
+        return {"batch": 16 * w["inner"] + 48 * w["leaf"] + 52 * w["tests"] + 64 * cont +
+                4 * self.batch.total_pixels}
+
+    def host_buffers(self, torch):
+        return (torch.empty(self.batch.total_pixels, dtype=torch.float32, pin_memory=True), None)
+
+    def e2e_step(self, torch, stream, host_out, _):
+        self.batch.render(self.out, stream=stream, graph=True)
+        host_out.copy_(self.out, non_blocking=True)
+
+    def e2e_bytes(self):
+        return (0, 4 * self.batch.total_pixels)
+
+    def cpu_baseline(self, budget_s=12.0):
+        from oracle import pyoracle as po
+
+        scenes, offsets, _ = reference_batch_scenes(self.cfg)
+        rng = np.random.default_rng(0)
+        n = 64
+        while True:
+            g = np.sort(rng.choice(self.batch.total_pixels, n, replace=False)).astype(np.uint32)
+            t0 = time.perf_counter()
+            _, _, nr = po.batch_path(scenes, offsets, g, self.cfg.max_depth, self.cfg.path_seed,
+                                     self.cfg.mesh_bias)
+            dt = time.perf_counter() - t0
+            if dt > budget_s / 4 or n >= 1 << 16:
+                break
+            n = min(1 << 16, int(n * min(8.0, budget_s / max(dt, 1e-3))))
+        return {"value": round(int(nr.sum()) / dt / 1e6, 6), "unit": "Mrays/s",
+                "cores": po.threads(), "kind": "port",
+                "sample": f"{n} seeded-random pixels of the batch ({int(nr.sum())} rays); oracle "
+                          "path tracer with brute-force Moller-Trumbore (the reference's one-leaf "
+                          "tree) and the exact SDF march, OpenMP"}
+
+
+def reference_batch_scenes(cfg):
+    """The batch's scenes for the CPU path (oracle generators only):
+    (oracle scene dicts, first-pixel offsets, total pixels)."""
+    from oracle import pyoracle as po
+    import rayengine_b200.configs as C
+    from rayengine_b200 import api
+
+    scenes, offsets, off = [], [], 0
+    for s in cfg.specs():
+        w, h = s["width"], s["height"]
+        offsets.append(off)
+        off += w * h
+        if s["kind"] == "soup":
+            sc = C.SoupConfig(num_tris=s["num_tris"], seed=s["seed"], width=w, height=h)
+            tri = po.soup(sc.seed, sc.num_tris)
+            verts = tri.reshape(-1, 3)
+            faces = np.arange(verts.shape[0], dtype=np.uint32).reshape(-1, 3)
+            packed = api.pack_triangles(verts, faces)
+            v = np.concatenate([packed[:, 0:3], packed[:, 0:3] + packed[:, 4:7],
+                                packed[:, 0:3] + packed[:, 8:11]])
+            cam = api.build_camera(sc.campos, sc.lookat, (60.0, api.vertical_fov(60.0, w, h)))
+            scenes.append(dict(kind=0, tris=packed, bmin=v.min(0), bmax=v.max(0), cam=cam, w=w,
+                               h=h, albedo=s["albedo"]))
+        else:
+            tc = C.TerrainConfig(seed=s["seed"], amplitude=s["amplitude"], width=w, height=h)
+            scenes.append(dict(kind=1, seed=tc.seed, octaves=tc.octaves, scale=tc.scale,
+                               amp=tc.amplitude, step_factor=tc.step_factor, eps=tc.eps,
+                               tmax=tc.tmax, max_steps=tc.max_steps, cam=tc.camera(), w=w, h=h,
+                               albedo=s["albedo"]))
+    return scenes, np.array(offsets, np.uint64), off
+
+
 # ---------------------------------------------------- the reference's path
 def reference_workload(name):
     """(workload description, built-by note, step(npix) -> rays traced) for the
@@ -537,6 +651,18 @@ def reference_workload(name):
     from rayengine_b200 import api
 
     rng = np.random.default_rng(1)
+    if name == "batch32":
+        cfg = C.BatchConfig()
+        scenes, offsets, total = reference_batch_scenes(cfg)
+
+        def step(npix):
+            g = np.sort(rng.choice(total, npix, replace=False)).astype(np.uint32)
+            _, _, nr = po.batch_path(scenes, offsets, g, cfg.max_depth, cfg.path_seed,
+                                     cfg.mesh_bias)
+            return int(nr.sum())
+        return ("batched path tracing of the 32-scene batch (depth 4, 1 spp), seeded-random "
+                "pixels", "restated single-leaf build (brute-force Moller-Trumbore) and the "
+                "restated exact SDF march", step)
     if name in ("terrain_sdf", "nsdf_terrain"):
         cfg = C.TerrainConfig()
         W, H = cfg.width, cfg.height
@@ -594,6 +720,7 @@ WORKLOADS = {
     "soup1m": lambda torch: SoupPrimary(torch, num_tris=1 << 20),
     "terrain_sdf": TerrainSDF,
     "nsdf_terrain": NeuralTerrainSDF,
+    "batch32": BatchWavefront,
 }
 
 METRIC = "Mrays/s on 1 B200: plain rope-kd/exact-SDF vs wavefront+neural SDF @<=1e-3 err"

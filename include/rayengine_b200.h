@@ -386,6 +386,74 @@ RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
 RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
 RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);
 
+/* ---- batched wavefront path tracing ----------------------------------
+ * No single counterpart in the reference, which renders one scene per
+ * frame (cuda_render_frame, renderer.cu:702-738; bounce rays in
+ * trace_secondary_rays, renderer.cu:435-492).  Many scenes of uneven size
+ * (rope kd-tree meshes and exact-SDF terrains, each with its own camera and
+ * resolution) are path traced (1 sample per pixel, Lambertian bounces) by
+ * one persistent kernel launch that pulls rays from per-bounce queues.
+ * Radiance of pixel i of scene s is out[offset(s) + i]: albedo^b * sky(d)
+ * for a path that leaves the scene at bounce b with direction d, sky(d) =
+ * 0.5 (1 + d.y); 0 for a path still on a surface after max_depth rays. */
+#define RE_BATCH_MESH 0u
+#define RE_BATCH_TERRAIN 1u
+typedef struct re_batch re_batch;
+
+typedef struct re_batch_scene {
+  uint32_t kind;          /* RE_BATCH_MESH or RE_BATCH_TERRAIN              */
+  const re_scene* mesh;   /* MESH: a built scene, used in place (must       */
+                          /* outlive the batch); two-sided triangles        */
+  re_sdf_params field;    /* TERRAIN: the exact field and its march         */
+  re_camera camera;
+  uint32_t width, height;
+  float albedo;           /* Lambertian reflectance in [0, 1]               */
+} re_batch_scene;
+
+typedef struct re_path_params {
+  uint32_t max_depth;     /* rays per path, the primary included (4); <= 8  */
+  uint32_t seed;          /* bounce directions: hash(seed, pixel, bounce)   */
+  float mesh_bias;        /* bounce origin offset along a mesh normal       */
+} re_path_params;
+
+typedef struct re_batch_tuning {
+  uint32_t block_threads; /* 32..512, multiple of 32 (256)                  */
+  uint32_t refill_min;    /* idle lanes a warp waits for before claiming    */
+  uint32_t stage_nodes;   /* top nodes per mesh scene in shared memory      */
+  uint32_t reserved;
+} re_batch_tuning;
+
+RE_API re_status re_batch_create(const re_batch_scene* scenes, uint32_t num_scenes,
+                                 const re_path_params* pp, re_batch** out);
+RE_API re_status re_batch_destroy(re_batch* b);
+/* Total pixels of the batch and each scene's first pixel (num_scenes
+ * values; offsets may be NULL). */
+RE_API re_status re_batch_pixels(const re_batch* b, uint64_t* total,
+                                 uint64_t* offsets);
+/* One frame, one launch.  d_radiance: total pixels floats; d_primary (may
+ * be NULL): the primary ray's hit per pixel (mesh: id, t, u, v; terrain:
+ * id 0 on a hit, -1 otherwise, t). */
+RE_API re_status re_batch_render(re_batch* b, float* d_radiance, re_hit* d_primary,
+                                 void* stream);
+/* The same frame from a CUDA graph captured on the first call (and again
+ * when the buffers, the stream or the tuning change), then replayed. */
+RE_API re_status re_batch_render_graph(re_batch* b, float* d_radiance,
+                                       re_hit* d_primary, void* stream);
+/* Rays traced in the last frame: rays[2 * bounce + kind] (bounce 0: all
+ * primary rays under kind 0), 2 * max_depth values; error = 1 if a wait
+ * bound was reached (rays dropped). */
+RE_API re_status re_batch_stats_get(re_batch* b, uint64_t* rays, int* error);
+/* One frame with work counters: totals[0..3] = inner-node visits, leaf
+ * visits, triangle tests, terrain field evaluations (host array). */
+RE_API re_status re_batch_counts(re_batch* b, float* d_radiance, void* stream,
+                                 uint64_t* totals);
+RE_API re_status re_batch_get_tuning(const re_batch* b, re_batch_tuning* out);
+RE_API re_status re_batch_set_tuning(re_batch* b, const re_batch_tuning* t);
+/* Times one frame per candidate (block size x refill threshold x staged
+ * nodes) and keeps the fastest. */
+RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
+                                   re_batch_tuning* out, float* best_ms);
+
 #ifdef __cplusplus
 }
 #endif

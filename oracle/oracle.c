@@ -730,3 +730,104 @@ int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int 
   }
   return 0;
 }
+
+/* ------------------------------------------------- batched path tracing */
+/* One pixel's path of the batched wavefront renderer: closest hits by
+ * brute force (two-sided, equal to the rope traversal's hits), the exact
+ * SDF march for terrains, cosine-weighted Lambertian bounces. */
+static void cosine_dir(const float n[3], uint32_t seed, uint32_t pixel, uint32_t j, float d[3]) {
+  float nt[3], nb[3];
+  if (fabsf(n[0]) > fabsf(n[1])) {
+    float inv = 1.0f / sqrtf(fmaf(n[2], n[2], n[0] * n[0]));
+    nt[0] = n[2] * inv; nt[1] = 0.0f; nt[2] = -n[0] * inv;
+  } else {
+    float inv = 1.0f / sqrtf(fmaf(n[2], n[2], n[1] * n[1]));
+    nt[0] = 0.0f; nt[1] = -n[2] * inv; nt[2] = n[1] * inv;
+  }
+  cross3(n, nt, nb);
+  uint32_t h1 = o_hash_u32(seed, pixel, 2 * j), h2 = o_hash_u32(seed, pixel, 2 * j + 1);
+  float u1 = (float)(h1 >> 8) * 0x1.0p-24f;
+  float u2 = (float)(h2 >> 8) * 0x1.0p-24f;
+  float r = sqrtf(u1);
+  float sn, cs;
+  o_sincos_2pi(u2, &sn, &cs);
+  float lx = r * cs, ly = sqrtf(1.0f - u1), lz = r * sn;
+  for (int k = 0; k < 3; ++k) d[k] = fmaf(lz, nt[k], fmaf(ly, n[k], lx * nb[k]));
+}
+
+uint32_t o_path_pixel(const o_path_scene* s, uint32_t gpix, uint32_t local_pix, uint32_t depth,
+                      uint32_t seed, float mesh_bias, float* radiance, o_hit* primary) {
+  o_camera_basis cb;
+  o_camera_setup(&s->cam, &cb);
+  float o[3], d[3];
+  o_generate_ray(&cb, s->w, s->h, local_pix % s->w, local_pix / s->w, o, d);
+  for (uint32_t b = 0; b < depth; ++b) {
+    int hit = 0;
+    float n[3] = {0, 0, 1}, hp[3] = {0, 0, 0};
+    o_hit ph = {-1, K_INFINITY, 0.f, 0.f};
+    if (s->kind == 0) {
+      o_hit h;
+      o_trace_bruteforce(s->tris, s->ntris, s->bmin, s->bmax, o, d, 0, &h);
+      if (h.id >= 0) {
+        hit = 1;
+        ph = h;
+        const float* T = s->tris + 12 * (size_t)h.id;
+        cross3(T + 4, T + 8, n);
+        normalize3(n);
+        if (dot3(n, d) > 0.0f) {
+          n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2];
+        }
+        for (int k = 0; k < 3; ++k) hp[k] = fmaf(n[k], mesh_bias, fmaf(h.t, d[k], o[k]));
+      }
+    } else {
+      float t = 0.0f, v = 0.0f, p[3];
+      uint32_t steps = 0;
+      for (;;) {
+        for (int k = 0; k < 3; ++k) p[k] = fmaf(t, d[k], o[k]);
+        v = o_terrain_density(s->perm, p, s->octaves, s->scale, s->amp);
+        ++steps;
+        if (v < s->eps) {
+          hit = 1;
+          break;
+        }
+        t = fmaf(s->step_factor, v, t);
+        if (t > s->tmax || steps >= s->max_steps) break;
+      }
+      if (hit) {
+        float delta = fmaxf(0.002f * t, 1e-3f), g[3];
+        for (int k = 0; k < 3; ++k) {
+          float q[3] = {p[0], p[1], p[2]};
+          q[k] = p[k] + delta;
+          float plus = o_terrain_density(s->perm, q, s->octaves, s->scale, s->amp);
+          q[k] = p[k] - delta;
+          g[k] = plus - o_terrain_density(s->perm, q, s->octaves, s->scale, s->amp);
+        }
+        float gl = sqrtf(fmaf(g[2], g[2], fmaf(g[1], g[1], g[0] * g[0])));
+        n[0] = g[0]; n[1] = g[1]; n[2] = g[2];
+        normalize3(n);
+        float off = fmaxf(-v, 0.0f) / (gl / (2.0f * delta)) + 2e-3f;
+        for (int k = 0; k < 3; ++k) hp[k] = fmaf(n[k], off, p[k]);
+        ph.id = 0;
+        ph.t = t;
+      }
+    }
+    if (b == 0 && primary) *primary = ph;
+    if (!hit) {
+      float pw = 1.0f;
+      for (uint32_t i = 0; i < b; ++i) pw *= s->albedo;
+      *radiance = pw * (0.5f * (1.0f + d[1]));
+      return b + 1;
+    }
+    if (b + 1 == depth) {
+      *radiance = 0.0f;
+      return b + 1;
+    }
+    float nd[3];
+    cosine_dir(n, seed, gpix, b, nd);
+    for (int k = 0; k < 3; ++k) {
+      o[k] = hp[k];
+      d[k] = nd[k];
+    }
+  }
+  return depth;
+}

@@ -125,6 +125,23 @@ void o_secondary_rays(const float hitp[3], const float n[3], uint32_t seed,
                       uint32_t pixel, const float light_dir[3], float bias,
                       float o_out[5][3], float d_out[5][3], float tmax_out[5]);
 
+/* --- batched path tracing (one pixel of the wavefront renderer) -------- */
+typedef struct {
+  uint32_t kind;              /* 0 mesh, 1 terrain                         */
+  const float* tris;          /* mesh: n x 12 floats in triangle-id order  */
+  int32_t ntris;
+  float bmin[3], bmax[3];     /* mesh: root box of the scene               */
+  const uint32_t* perm;       /* terrain                                   */
+  int octaves;
+  float scale, amp, step_factor, eps, tmax;
+  uint32_t max_steps;
+  o_camera cam;
+  uint32_t w, h;
+  float albedo;
+} o_path_scene;
+/* returns the number of rays the path traced */
+uint32_t o_path_pixel(const o_path_scene* s, uint32_t gpix, uint32_t local_pix, uint32_t depth,
+                      uint32_t seed, float mesh_bias, float* radiance, o_hit* primary);
 #ifdef __cplusplus
 }
 #endif

@@ -238,3 +238,20 @@ void o_batch_density_d(const uint32_t perm[512], const double* pts, int64_t n, i
 #pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : omp_get_max_threads())
   for (int64_t i = 0; i < n; ++i) out[i] = o_terrain_density_d(perm, pts + 3 * i, octaves, scale, amp);
 }
+
+/* Batched path tracing over `npix` global pixels of `nscenes` scenes
+ * (offsets[s] = first global pixel of scene s). */
+void o_batch_path(const o_path_scene* scenes, int nscenes, const uint64_t* offsets,
+                  const uint32_t* gpix, int64_t npix, uint32_t depth, uint32_t seed,
+                  float mesh_bias, float* radiance, o_hit* primary, uint32_t* nrays,
+                  int threads) {
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < npix; ++i) {
+    uint32_t g = gpix[i];
+    int s = 0;
+    while (s + 1 < nscenes && offsets[s + 1] <= g) ++s;
+    uint32_t r = o_path_pixel(&scenes[s], g, (uint32_t)(g - offsets[s]), depth, seed, mesh_bias,
+                              &radiance[i], primary ? &primary[i] : NULL);
+    if (nrays) nrays[i] = r;
+  }
+}

@@ -358,3 +358,51 @@ def density_d(p, pts, octaves=8, scale=0.25, amp=3.0, nthreads=0):
                             ctypes.c_double(scale), ctypes.c_double(amp), _p(out),
                             ctypes.c_int(nthreads))
     return out
+
+
+class OPathScene(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("tris", ctypes.c_void_p), ("ntris", ctypes.c_int32),
+                ("bmin", ctypes.c_float * 3), ("bmax", ctypes.c_float * 3),
+                ("perm", ctypes.c_void_p), ("octaves", ctypes.c_int),
+                ("scale", ctypes.c_float), ("amp", ctypes.c_float),
+                ("step_factor", ctypes.c_float), ("eps", ctypes.c_float),
+                ("tmax", ctypes.c_float), ("max_steps", ctypes.c_uint32),
+                ("cam", OCamera), ("w", ctypes.c_uint32), ("h", ctypes.c_uint32),
+                ("albedo", ctypes.c_float)]
+
+
+def batch_path(scenes, offsets, gpix, depth, seed, mesh_bias, nthreads=0):
+    """Oracle radiance, primary hits and rays per path of the batched path tracer.
+
+    scenes: dicts with kind 0 {tris (n,12) float32 in id order, bmin, bmax}
+    or kind 1 {seed, octaves, scale, amp, step_factor, eps, tmax, max_steps},
+    plus cam (product re_camera), w, h, albedo."""
+    keep = []
+    arr = (OPathScene * len(scenes))()
+    for i, s in enumerate(scenes):
+        o = arr[i]
+        o.kind = s["kind"]
+        if s["kind"] == 0:
+            tris = np.ascontiguousarray(s["tris"], np.float32)
+            keep.append(tris)
+            o.tris, o.ntris = tris.ctypes.data, tris.shape[0]
+            o.bmin[:] = [float(x) for x in s["bmin"]]
+            o.bmax[:] = [float(x) for x in s["bmax"]]
+        else:
+            P = np.ascontiguousarray(perm(s["seed"]), np.uint32)
+            keep.append(P)
+            o.perm = P.ctypes.data
+            o.octaves, o.scale, o.amp = s["octaves"], s["scale"], s["amp"]
+            o.step_factor, o.eps, o.tmax, o.max_steps = (s["step_factor"], s["eps"], s["tmax"],
+                                                         s["max_steps"])
+        o.cam = camera(s["cam"])
+        o.w, o.h, o.albedo = s["w"], s["h"], s["albedo"]
+    offs = np.ascontiguousarray(offsets, np.uint64)
+    g = np.ascontiguousarray(gpix, np.uint32)
+    rad = np.zeros(g.shape[0], np.float32)
+    prim = np.zeros((g.shape[0], 4), np.int32)
+    nrays = np.zeros(g.shape[0], np.uint32)
+    lib().o_batch_path(arr, ctypes.c_int(len(scenes)), _p(offs), _p(g), ctypes.c_int64(g.shape[0]),
+                       ctypes.c_uint32(depth), ctypes.c_uint32(seed), ctypes.c_float(mesh_bias),
+                       _p(rad), _p(prim), _p(nrays), ctypes.c_int(nthreads))
+    return rad, prim, nrays

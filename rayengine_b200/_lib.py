@@ -146,6 +146,31 @@ class re_nsdf_trace_params(ctypes.Structure):
 NSDF_EXACT_ONLY = 1
 
 
+class re_batch_scene(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_uint32),
+        ("mesh", ctypes.c_void_p),
+        ("field", re_sdf_params),
+        ("camera", re_camera),
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("albedo", ctypes.c_float),
+    ]
+
+
+class re_path_params(ctypes.Structure):
+    _fields_ = [("max_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32),
+                ("mesh_bias", ctypes.c_float)]
+
+
+class re_batch_tuning(ctypes.Structure):
+    _fields_ = [("block_threads", ctypes.c_uint32), ("refill_min", ctypes.c_uint32),
+                ("stage_nodes", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+BATCH_MESH, BATCH_TERRAIN = 0, 1
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _F = ctypes.c_float
@@ -194,6 +219,16 @@ _SIGS = {
     "re_nsdf_trace_network": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_exact": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int), _P]),
+    "re_batch_create": (ctypes.c_int, [ctypes.POINTER(re_batch_scene), _U32, ctypes.POINTER(re_path_params), ctypes.POINTER(ctypes.c_void_p)]),
+    "re_batch_destroy": (ctypes.c_int, [_P]),
+    "re_batch_pixels": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),
+    "re_batch_render": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_batch_render_graph": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_batch_stats_get": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_int)]),
+    "re_batch_counts": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_batch_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_batch_tuning)]),
+    "re_batch_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_batch_tuning)]),
+    "re_batch_autotune": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(re_batch_tuning), ctypes.POINTER(_F)]),
     "re_nsdf_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "re_nsdf_load": (ctypes.c_int, [_P, ctypes.c_char_p]),
 }

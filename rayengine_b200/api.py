@@ -497,3 +497,104 @@ class NeuralSDF:
 
     def load(self, path: str):
         call("re_nsdf_load", self._h, path.encode())
+
+
+# ------------------------------------------------- batched path tracing
+class Batch:
+    """Many scenes of uneven size path traced by one persistent launch.
+
+    scenes: dicts with either "mesh" (a KDScene) or "terrain" (sdf_params),
+    plus "camera", "width", "height" and "albedo"."""
+
+    def __init__(self, scenes, max_depth=4, seed=0, mesh_bias=1e-4):
+        arr = (_lib.re_batch_scene * len(scenes))()
+        self._meshes = []
+        for i, sc in enumerate(scenes):
+            e = arr[i]
+            if "mesh" in sc:
+                e.kind = _lib.BATCH_MESH
+                e.mesh = sc["mesh"]._h.value
+                self._meshes.append(sc["mesh"])
+            else:
+                e.kind = _lib.BATCH_TERRAIN
+                e.field = sc["terrain"]
+            e.camera = sc["camera"]
+            e.width, e.height, e.albedo = sc["width"], sc["height"], sc["albedo"]
+        pp = _lib.re_path_params(max_depth, seed, mesh_bias)
+        h = ctypes.c_void_p()
+        call("re_batch_create", arr, len(scenes), ctypes.byref(pp), ctypes.byref(h))
+        self._h = h
+        self.max_depth = max_depth
+        total = ctypes.c_uint64()
+        offs = np.zeros(len(scenes), np.uint64)
+        call("re_batch_pixels", self._h, ctypes.byref(total), offs.ctypes.data)
+        self.total_pixels = int(total.value)
+        self.offsets = offs
+
+    def close(self):
+        if self._h:
+            lib.re_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, out=None, primary=None, stream=None, graph=False):
+        """One frame -> float32 CUDA tensor of total_pixels radiances."""
+        import torch
+
+        if out is None:
+            out = torch.empty(self.total_pixels, dtype=torch.float32, device="cuda")
+        fn = "re_batch_render_graph" if graph else "re_batch_render"
+        call(fn, self._h, _dptr(out), _dptr(primary) if primary is not None else None,
+             _stream_ptr(stream))
+        return out
+
+    def stats(self) -> dict:
+        rays = np.zeros(2 * self.max_depth, np.uint64)
+        err = ctypes.c_int()
+        call("re_batch_stats_get", self._h, rays.ctypes.data, ctypes.byref(err))
+        return {"rays": rays.reshape(self.max_depth, 2).astype(np.int64), "error": int(err.value)}
+
+    def counts(self, out=None, stream=None) -> dict:
+        """Traversal and field-evaluation work of one frame."""
+        import torch
+
+        if out is None:
+            out = torch.empty(self.total_pixels, dtype=torch.float32, device="cuda")
+        v = np.zeros(4, np.uint64)
+        call("re_batch_counts", self._h, _dptr(out), _stream_ptr(stream), v.ctypes.data)
+        return {"inner": int(v[0]), "leaf": int(v[1]), "tests": int(v[2]),
+                "field_evals": int(v[3])}
+
+    @property
+    def tuning(self) -> dict:
+        t = _lib.re_batch_tuning()
+        call("re_batch_get_tuning", self._h, ctypes.byref(t))
+        return {"block_threads": t.block_threads, "refill_min": t.refill_min,
+                "stage_nodes": t.stage_nodes}
+
+    def set_tuning(self, block_threads, refill_min, stage_nodes):
+        t = _lib.re_batch_tuning(block_threads, refill_min, stage_nodes, 0)
+        call("re_batch_set_tuning", self._h, ctypes.byref(t))
+
+    def autotune(self, out=None, stream=None) -> dict:
+        import torch
+
+        if out is None:
+            out = torch.empty(self.total_pixels, dtype=torch.float32, device="cuda")
+        t = _lib.re_batch_tuning()
+        ms = ctypes.c_float()
+        call("re_batch_autotune", self._h, _dptr(out), _stream_ptr(stream), ctypes.byref(t),
+             ctypes.byref(ms))
+        return {"block_threads": t.block_threads, "refill_min": t.refill_min,
+                "stage_nodes": t.stage_nodes, "frame_ms": round(ms.value, 4)}

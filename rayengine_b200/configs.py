@@ -152,3 +152,56 @@ class NeuralTerrainConfig:
     def trace_params(self, lipschitz):
         return api.nsdf_trace_params(lipschitz, self.safety, self.switch_dist, self.min_step,
                                      self.max_network_steps, 0, self.root_steps)
+
+
+@dataclass
+class BatchConfig:
+    """Batched wavefront workload: seeded scenes of uneven size, soups
+    (triangle counts log-uniform in tri_range, cameras as SoupConfig) and
+    volumetric terrains (TerrainConfig with a per-scene seed and
+    amplitude), each at a resolution drawn from `resolutions`."""
+    num_scenes: int = 32
+    seed: int = 4
+    terrain_fraction: float = 0.25
+    tri_range: tuple = (10_000, 2_000_000)
+    resolutions: tuple = ((640, 360), (1280, 720), (1920, 1080))
+    max_depth: int = 4
+    path_seed: int = 11
+    mesh_bias: float = 1e-4
+
+    def specs(self):
+        """Scene descriptions (no device work): dicts with kind, size and seeds."""
+        rng = np.random.default_rng(self.seed)
+        out = []
+        for i in range(self.num_scenes):
+            w, h = self.resolutions[int(rng.integers(len(self.resolutions)))]
+            albedo = float(rng.uniform(0.5, 0.8))
+            if rng.random() < self.terrain_fraction:
+                out.append(dict(kind="terrain", seed=PERLIN_SEED + i,
+                                amplitude=float(rng.uniform(2.0, 3.5)), width=w, height=h,
+                                albedo=albedo))
+            else:
+                lo, hi = np.log(self.tri_range[0]), np.log(self.tri_range[1])
+                n = int(round(float(np.exp(rng.uniform(lo, hi)))))
+                out.append(dict(kind="soup", num_tris=n, seed=1000 + i, width=w, height=h,
+                                albedo=albedo))
+        return out
+
+    def build(self):
+        """(Batch, [KDScene]) on the current device."""
+        scenes, meshes = [], []
+        for s in self.specs():
+            w, h = s["width"], s["height"]
+            if s["kind"] == "soup":
+                sc = SoupConfig(num_tris=s["num_tris"], seed=s["seed"], width=w, height=h)
+                m = api.KDScene.from_packed(sc.packed())
+                meshes.append(m)
+                cam = api.build_camera(sc.campos, sc.lookat,
+                                       (60.0, api.vertical_fov(60.0, w, h)))
+                scenes.append(dict(mesh=m, camera=cam, width=w, height=h, albedo=s["albedo"]))
+            else:
+                tc = TerrainConfig(seed=s["seed"], amplitude=s["amplitude"], width=w, height=h)
+                scenes.append(dict(terrain=tc.params(), camera=tc.camera(), width=w, height=h,
+                                   albedo=s["albedo"]))
+        b = api.Batch(scenes, self.max_depth, self.path_seed, self.mesh_bias)
+        return b, meshes

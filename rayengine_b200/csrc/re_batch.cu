@@ -1,0 +1,907 @@
+// Batched wavefront path tracer: many scenes of uneven size (rope kd-tree
+// meshes and exact-SDF terrains, each with its own camera and resolution)
+// rendered by ONE persistent launch that pulls rays from per-bounce queues.
+//
+// The reference renders one scene per frame (cuda_render_frame,
+// RE/cuda-src/renderer.cu:702-738, with trace_secondary_rays :435-492 for
+// the bounce rays); batching is new.  Ray queries restate the reference's
+// traversal (re_kd.cuh) and the exact SDF march (sphere_tracing.cuh:183-216,
+// re_noise.cuh).
+//
+// Path (per pixel, 1 sample): ray 0 from the scene's camera; at a hit with
+// bounce b < depth - 1 the path continues with a cosine-weighted Lambertian
+// direction about the normal (createCoordinateSystem /
+// uniformSampleHemisphere, RE/cuda-src/cuda_helper_functions.h:197-216, with
+// cosine weighting), so the throughput after b bounces is albedo^b.  A miss
+// at bounce b writes albedo^b * sky(d), sky(d) = 0.5 (1 + d.y); a hit at the
+// last bounce writes 0.  Each pixel is written exactly once.
+//
+// Work distribution (no grid-wide barrier):
+//   * primary rays come from a global pixel cursor over all scenes' pixels;
+//   * a ray that continues is appended to the queue of (next bounce, scene
+//     kind): a warp reserves slots with one atomic per distinct queue, writes
+//     the 32-byte records and publishes each slot with a release store of the
+//     frame's epoch into the slot's flag;
+//   * idle lanes refill from the deepest non-empty queue (preferring the kind
+//     the warp is already running, so meshes and terrains rarely share a
+//     warp), claiming only published-or-reserved slots (compare-and-swap up to
+//     the reserved count) and waiting, without blocking the warp, for a
+//     claimed slot's flag;
+//   * a warp leaves when the cursor is exhausted and every created ray has
+//     finished (children are counted as created before their parent counts
+//     as finished, so finished == created means nothing is in flight);
+//   * the last block to leave resets the counters and advances the epoch, so
+//     the same launch can be replayed from a CUDA graph.
+// Every wait has an iteration bound after which the kernel sets the error
+// flag and drops the ray.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "re_common.hpp"
+#include "re_kd.cuh"
+#include "re_math.cuh"
+#include "re_noise.cuh"
+#include "re_scene.hpp"
+
+namespace re {
+namespace batch {
+
+constexpr uint32_t kMaxScenes = 64;
+constexpr uint32_t kMaxDepth = 8;
+constexpr uint32_t kMaxQueues = 2 * (kMaxDepth - 1);
+constexpr uint32_t kMesh = RE_BATCH_MESH, kTerrain = RE_BATCH_TERRAIN;
+
+// counters (uint32): cursor, created, finished, epoch, blocks done, error,
+// then reserved[q] at kReserved + q and claimed[q] at kClaimed + q; the last
+// frame's per-queue ray counts are copied to kStats + q before the reset.
+enum : uint32_t {
+  kCursor = 0,
+  kCreated = 1,
+  kFinished = 2,
+  kEpoch = 3,
+  kDone = 4,
+  kError = 5,
+  kPrimaryRays = 6,
+  kReserved = 8,
+  kClaimed = kReserved + kMaxQueues,
+  kStats = kClaimed + kMaxQueues,
+  kStatsPrimary = kStats + kMaxQueues,
+  kStatsError = kStatsPrimary + 1,
+  kNumCounters = 64
+};
+static_assert(kStatsError < kNumCounters, "counter layout");
+
+struct __align__(16) SceneDev {
+  const uint2* nodes;
+  const float4* leaves;
+  const float4* tris;
+  float bmin[3], bmax[3];
+  uint32_t max_visits, stage, stage_off;
+  uint32_t perm_slot, octaves, max_steps;
+  float scale, amp, step_factor, eps, tmax;
+  CamDev cam;
+  uint32_t w, h, kind, pix_off;
+  float albedo;
+};
+
+struct BatchDev {
+  const SceneDev* scenes;
+  const uint8_t* perms;  // perm_count tables of 512 bytes
+  uint32_t num_scenes, perm_count, stage_total, total_pixels;
+  uint32_t depth, seed, refill_min;
+  float mesh_bias;
+  float4* queue;        // records: 2 float4 per slot
+  uint32_t* flags;      // one per slot
+  uint64_t qoff[kMaxQueues];  // first slot of queue q
+  uint32_t* ctr;
+  float* radiance;
+  int4* primary;        // optional re_hit per pixel
+  unsigned long long* totals;  // COUNT: inner nodes, leaves, triangle tests, field evaluations
+};
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Claim up to `want` reserved slots of queue q; returns the count (base in
+// `base`).  Never claims past the reserved count.
+__device__ __forceinline__ uint32_t claim(uint32_t* ctr, uint32_t q, uint32_t want, uint32_t& base) {
+  for (int tries = 0; tries < 4; ++tries) {
+    uint32_t c = ld_relaxed(&ctr[kClaimed + q]);
+    uint32_t r = ld_relaxed(&ctr[kReserved + q]);
+    if (c >= r) return 0u;
+    uint32_t k = min(want, r - c);
+    if (atomicCAS(&ctr[kClaimed + q], c, c + k) == c) {
+      base = c;
+      return k;
+    }
+  }
+  return 0u;
+}
+
+__device__ __forceinline__ uint32_t scene_of(const SceneDev* sc, uint32_t n, uint32_t gpix) {
+  uint32_t lo = 0, hi = n - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (sc[mid].pix_off <= gpix) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ KdDev kd_of(const SceneDev& s) {
+  KdDev kd;
+  kd.nodes = s.nodes;
+  kd.leaves = s.leaves;
+  kd.tris = s.tris;
+  kd.bmin = v3(s.bmin[0], s.bmin[1], s.bmin[2]);
+  kd.bmax = v3(s.bmax[0], s.bmax[1], s.bmax[2]);
+  kd.max_visits = s.max_visits;
+  kd.stage = s.stage;
+  return kd;
+}
+
+// cosine-weighted direction about n (the AO frame's construction)
+__device__ __forceinline__ V3 cosine_dir(V3 n, uint32_t seed, uint32_t gpix, uint32_t bounce) {
+  V3 nt;
+  if (fabsf(n.x) > fabsf(n.y)) {
+    float iv = 1.0f / sqrtf(__fmaf_rn(n.z, n.z, n.x * n.x));
+    nt = v3(n.z * iv, 0.0f, -n.x * iv);
+  } else {
+    float iv = 1.0f / sqrtf(__fmaf_rn(n.z, n.z, n.y * n.y));
+    nt = v3(0.0f, -n.z * iv, n.y * iv);
+  }
+  V3 nb = cross(n, nt);
+  uint32_t h1 = hash_u32(seed, gpix, 2u * bounce), h2 = hash_u32(seed, gpix, 2u * bounce + 1u);
+  float u1 = (float)(h1 >> 8) * 5.9604644775390625e-08f;
+  float u2 = (float)(h2 >> 8) * 5.9604644775390625e-08f;
+  float r = sqrtf(u1);
+  float sn, cs;
+  sincos_2pi(u2, sn, cs);
+  float lx = r * cs, ly = sqrtf(1.0f - u1), lz = r * sn;
+  return v3(__fmaf_rn(lz, nt.x, __fmaf_rn(ly, n.x, lx * nb.x)),
+            __fmaf_rn(lz, nt.y, __fmaf_rn(ly, n.y, lx * nb.y)),
+            __fmaf_rn(lz, nt.z, __fmaf_rn(ly, n.z, lx * nb.z)));
+}
+
+__device__ __forceinline__ float miss_radiance(float albedo, uint32_t bounce, V3 d) {
+  float pw = 1.0f;
+  for (uint32_t i = 0; i < bounce; ++i) pw *= albedo;
+  return pw * (0.5f * (1.0f + d.y));
+}
+
+enum : uint32_t { kIdle = 0, kPending = 1, kLive = 2 };
+enum : uint32_t { kMarch = 0, kNormal = 1 };
+constexpr uint32_t kPendingBound = 1u << 22;  // polls of one slot flag
+constexpr uint32_t kLoopBound = 1u << 24;     // trips of the persistent loop
+
+template <bool COUNT>
+__global__ void __launch_bounds__(512) k_batch(BatchDev B) {
+  extern __shared__ uint4 smem_u4[];
+  SceneDev* sc = reinterpret_cast<SceneDev*>(smem_u4);
+  uint8_t* sperm = reinterpret_cast<uint8_t*>(sc + B.num_scenes);
+  uint2* snodes = reinterpret_cast<uint2*>(sperm + 512u * B.perm_count);
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(B.scenes);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
+    for (uint32_t i = threadIdx.x; i < B.num_scenes * (uint32_t)(sizeof(SceneDev) / 4); i += blockDim.x)
+      dst[i] = src[i];
+    for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) sperm[i] = B.perms[i];
+    __syncthreads();
+    for (uint32_t s = 0; s < B.num_scenes; ++s)
+      for (uint32_t i = threadIdx.x; i < sc[s].stage; i += blockDim.x)
+        snodes[sc[s].stage_off + i] = __ldg(&sc[s].nodes[i]);
+    __syncthreads();
+  }
+  uint32_t* ctr = B.ctr;
+  const uint32_t epoch = ld_relaxed(&ctr[kEpoch]);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t nq = 2u * (B.depth - 1u);
+
+  uint32_t state = kIdle, pq = 0, pslot = 0, polls = 0;
+  uint32_t gpix = 0, scene = 0, bounce = 0, kind = kMesh;
+  Trav tr;
+  tr.live = false;
+  // terrain march state
+  float t = 0.f, v_hit = 0.f, delta = 0.f, plus = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
+  uint32_t steps = 0, mode = kMarch, tap = 0;
+  V3 p = {0.f, 0.f, 0.f};
+  Counters cnt = {0, 0, 0, 0};
+  uint32_t errors = 0;
+
+  uint32_t trip = 0;
+  for (; trip < kLoopBound; ++trip) {
+    // ---- pending claims: the slot's record is published once its flag holds this epoch
+    if (state == kPending) {
+      if (ld_acquire(&B.flags[B.qoff[pq] + pslot]) == epoch) {
+        const float4* rec = B.queue + 2 * (B.qoff[pq] + pslot);
+        float4 A = __ldcg(rec), Bv = __ldcg(rec + 1);
+        uint32_t tag = __float_as_uint(Bv.w);
+        gpix = tag & 0x0FFFFFFFu;
+        bounce = tag >> 28;
+        scene = scene_of(sc, B.num_scenes, gpix);
+        kind = sc[scene].kind;
+        V3 o = v3(A.x, A.y, A.z), d = v3(Bv.x, Bv.y, Bv.z);
+        if (kind == kMesh) {
+          trav_init(tr, kd_of(sc[scene]), o, d, K_INF, __float_as_uint(A.w));
+        } else {
+          tr.o = o;
+          tr.d = d;
+          t = 0.f;
+          steps = 0;
+          mode = kMarch;
+        }
+        state = kLive;
+      } else if (++polls >= kPendingBound) {
+        errors = 1;
+        state = kIdle;  // dropped: counted as finished below
+      }
+    }
+    // ---- refill idle lanes
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, state == kIdle);
+    uint32_t live_mesh = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kMesh);
+    uint32_t live_terr = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kTerrain);
+    uint32_t nidle = __popc(idle);
+    if (nidle != 0u && (nidle >= B.refill_min || nidle == 32u)) {
+      uint32_t src = 0xFFFFFFFFu, base = 0, k = 0;
+      if (lane == 0) {
+        uint32_t first = live_terr > live_mesh ? kTerrain : kMesh;
+        for (int b = (int)B.depth - 1; b >= 1 && k == 0; --b) {
+          for (uint32_t j = 0; j < 2 && k == 0; ++j) {
+            uint32_t q = 2u * (uint32_t)(b - 1) + (j == 0 ? first : 1u - first);
+            k = claim(ctr, q, nidle, base);
+            if (k) src = q;
+          }
+        }
+        if (k == 0 && ld_relaxed(&ctr[kCursor]) < B.total_pixels) {
+          base = atomicAdd(&ctr[kCursor], nidle);
+          k = base < B.total_pixels ? min(nidle, B.total_pixels - base) : 0u;
+          if (k) {
+            atomicAdd(&ctr[kCreated], k);
+            src = 0xFFFFFFFEu;
+          }
+        }
+      }
+      src = __shfl_sync(0xFFFFFFFFu, src, 0);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      k = __shfl_sync(0xFFFFFFFFu, k, 0);
+      uint32_t rank = __popc(idle & lt_mask);
+      if (state == kIdle && rank < k) {
+        if (src == 0xFFFFFFFEu) {
+          gpix = base + rank;
+          bounce = 0;
+          scene = scene_of(sc, B.num_scenes, gpix);
+          kind = sc[scene].kind;
+          const SceneDev& S = sc[scene];
+          uint32_t lp = gpix - S.pix_off;
+          V3 o, d;
+          generate_ray(S.cam, S.w, S.h, lp % S.w, lp / S.w, o, d);
+          if (kind == kMesh) {
+            trav_init(tr, kd_of(S), o, d, K_INF, 0u);
+          } else {
+            tr.o = o;
+            tr.d = d;
+            t = 0.f;
+            steps = 0;
+            mode = kMarch;
+          }
+          state = kLive;
+        } else {
+          pq = src;
+          pslot = base + rank;
+          polls = 0;
+          state = kPending;
+          kind = src & 1u;
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, state != kIdle) == 0u) {
+      // nothing in this warp: leave once nothing can be created any more
+      uint32_t leave = 0;
+      if (lane == 0) {
+        if (ld_relaxed(&ctr[kCursor]) >= B.total_pixels) {
+          uint32_t f = ld_acquire(&ctr[kFinished]);
+          uint32_t c = ld_acquire(&ctr[kCreated]);
+          leave = f == c ? 1u : 0u;
+        }
+        if (!leave) __nanosleep(64);
+      }
+      if (__shfl_sync(0xFFFFFFFFu, leave, 0)) break;
+      continue;
+    }
+    // ---- one step of every live ray
+    bool done = false, hit = false;
+    V3 n = {0.f, 0.f, 1.f}, hp = {0.f, 0.f, 0.f};
+    uint32_t start_leaf = 0;
+    float hit_t = 0.f, hit_u = 0.f, hit_v = 0.f;
+    int32_t hit_id = -1;
+    if (state == kLive) {
+      const SceneDev& S = sc[scene];
+      if (kind == kMesh) {
+        KdDev kd = kd_of(S);
+        trav_step<0, false, COUNT>(tr, kd, snodes + S.stage_off, cnt);
+        if (!tr.live) {
+          done = true;
+          hit = tr.best_id >= 0;
+          if (hit) {
+            hit_t = tr.best_t;
+            hit_u = tr.best_u;
+            hit_v = tr.best_v;
+            hit_id = tr.best_id;
+            start_leaf = tr.best_leaf;
+            const float4* T = S.tris + 3 * (size_t)tr.best_ref;
+            float4 T1 = __ldg(T + 1), T2 = __ldg(T + 2);
+            n = normalize(cross(v3(T1.x, T1.y, T1.z), v3(T2.x, T2.y, T2.z)));
+            if (dot(n, tr.d) > 0.0f) n = v3(-n.x, -n.y, -n.z);
+            V3 q = v3(__fmaf_rn(hit_t, tr.d.x, tr.o.x), __fmaf_rn(hit_t, tr.d.y, tr.o.y),
+                      __fmaf_rn(hit_t, tr.d.z, tr.o.z));
+            hp = v3(__fmaf_rn(n.x, B.mesh_bias, q.x), __fmaf_rn(n.y, B.mesh_bias, q.y),
+                    __fmaf_rn(n.z, B.mesh_bias, q.z));
+          }
+        }
+      } else {
+        PermBytes P{sperm + 512u * S.perm_slot};
+        V3 qp;
+        if (mode == kMarch) {
+          qp = v3(__fmaf_rn(t, tr.d.x, tr.o.x), __fmaf_rn(t, tr.d.y, tr.o.y),
+                  __fmaf_rn(t, tr.d.z, tr.o.z));
+        } else {
+          float sd = (tap & 1u) ? -delta : delta;
+          qp = p;
+          if (tap < 2) qp.x = p.x + sd;
+          else if (tap < 4) qp.y = p.y + sd;
+          else qp.z = p.z + sd;
+        }
+        float v = terrain_density(P, qp, S.octaves, S.scale, S.amp);
+        if (COUNT) ++cnt.status;  // field evaluations
+        if (mode == kMarch) {
+          ++steps;
+          if (v < S.eps) {
+            p = qp;
+            v_hit = v;
+            delta = fmaxf(0.002f * t, 1e-3f);
+            mode = kNormal;
+            tap = 0;
+          } else {
+            t = __fmaf_rn(S.step_factor, v, t);
+            if (t > S.tmax || steps >= S.max_steps) done = true;
+          }
+        } else {
+          if ((tap & 1u) == 0u) {
+            plus = v;
+          } else {
+            float diff = plus - v;
+            if (tap == 1) nx = diff;
+            else if (tap == 3) ny = diff;
+            else nz = diff;
+          }
+          if (tap == 5) {
+            done = true;
+            hit = true;
+            hit_t = t;
+            hit_id = 0;
+            float gl = sqrtf(__fmaf_rn(nz, nz, __fmaf_rn(ny, ny, nx * nx)));
+            n = normalize(v3(nx, ny, nz));
+            // leave the surface: the march may stop inside (v_hit < 0)
+            float off = fmaxf(-v_hit, 0.0f) / (gl / (2.0f * delta)) + 2e-3f;
+            hp = v3(__fmaf_rn(n.x, off, p.x), __fmaf_rn(n.y, off, p.y), __fmaf_rn(n.z, off, p.z));
+          } else {
+            ++tap;
+          }
+        }
+      }
+    }
+    // ---- finished rays: write or continue the path
+    bool push = false;
+    float4 R0 = make_float4(0.f, 0.f, 0.f, 0.f), R1 = R0;
+    uint32_t qn = 0;
+    if (done) {
+      const SceneDev& S = sc[scene];
+      if (bounce == 0 && B.primary)
+        B.primary[gpix] = make_int4(hit_id, __float_as_int(hit ? hit_t : K_INF),
+                                    __float_as_int(hit_u), __float_as_int(hit_v));
+      if (hit && bounce + 1u < B.depth) {
+        V3 nd = cosine_dir(n, B.seed, gpix, bounce);
+        push = true;
+        qn = 2u * bounce + kind;
+        R0 = make_float4(hp.x, hp.y, hp.z, __uint_as_float(start_leaf));
+        R1 = make_float4(nd.x, nd.y, nd.z, __uint_as_float(gpix | ((bounce + 1u) << 28)));
+      } else {
+        B.radiance[gpix] = hit ? 0.0f : miss_radiance(S.albedo, bounce, tr.d);
+      }
+      state = kIdle;
+    }
+    // dropped pending claims also finish (error path)
+    bool finished = done || (errors && state == kIdle && polls >= kPendingBound);
+    if (finished && !done) polls = 0;
+    // ---- append continuations, one atomic per distinct queue
+    uint32_t pushers = __ballot_sync(0xFFFFFFFFu, push);
+    if (pushers) {
+      uint32_t slot = 0;
+      if (push) {
+        uint32_t peers = __match_any_sync(pushers, qn);
+        uint32_t leader = __ffs(peers) - 1u;
+        uint32_t b0 = 0;
+        if (lane == leader) b0 = atomicAdd(&ctr[kReserved + qn], (uint32_t)__popc(peers));
+        b0 = __shfl_sync(peers, b0, leader);
+        slot = b0 + __popc(peers & lt_mask);
+        float4* rec = B.queue + 2 * (B.qoff[qn] + slot);
+        __stcg(rec, R0);
+        __stcg(rec + 1, R1);
+      }
+      if (lane == 0) atomicAdd(&ctr[kCreated], (uint32_t)__popc(pushers));
+      __threadfence();
+      if (push) st_release(&B.flags[B.qoff[qn] + slot], epoch);
+    }
+    uint32_t fin = __ballot_sync(0xFFFFFFFFu, finished);
+    if (fin) {
+      __threadfence();
+      if (lane == 0) atomicAdd(&ctr[kFinished], (uint32_t)__popc(fin));
+    }
+  }
+  if (trip >= kLoopBound) errors = 1;
+  if (COUNT) {
+    uint32_t v4[4] = {cnt.inner, cnt.leaf, cnt.tests, cnt.status};
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      uint32_t x = __reduce_add_sync(0xFFFFFFFFu, v4[f]);
+      if (lane == 0) atomicAdd(&B.totals[f], (unsigned long long)x);
+    }
+  }
+  if (errors) atomicExch(&ctr[kError], 1u);
+  // ---- the last block resets the counters for the next frame
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    uint32_t d = atomicAdd(&ctr[kDone], 1u);
+    if (d == gridDim.x - 1u) {
+      __threadfence();
+      for (uint32_t q = 0; q < nq; ++q) {
+        ctr[kStats + q] = ctr[kReserved + q];
+        ctr[kReserved + q] = 0u;
+        ctr[kClaimed + q] = 0u;
+      }
+      ctr[kStatsPrimary] = min(ctr[kCursor], B.total_pixels);
+      ctr[kStatsError] = ctr[kError];
+      ctr[kCursor] = 0u;
+      ctr[kCreated] = 0u;
+      ctr[kFinished] = 0u;
+      ctr[kError] = 0u;
+      ctr[kDone] = 0u;
+      __threadfence();
+      ctr[kEpoch] = epoch + 1u;
+    }
+  }
+}
+
+}  // namespace batch
+}  // namespace re
+
+// ------------------------------------------------------------------ host
+struct re_batch {
+  int device = 0;
+  uint32_t num_scenes = 0, depth = 4, seed = 0;
+  float mesh_bias = 1e-4f;
+  std::vector<re::batch::SceneDev> host_scenes;
+  std::vector<const re_scene*> meshes;
+  std::vector<uint8_t> perms;
+  uint64_t total_pixels = 0;
+  std::vector<uint64_t> offsets;
+  uint64_t cap[2] = {0, 0};  // pixels of mesh / terrain scenes (queue capacity)
+  re::batch::SceneDev* d_scenes = nullptr;
+  uint8_t* d_perms = nullptr;
+  float4* d_queue = nullptr;
+  uint32_t* d_flags = nullptr;
+  uint32_t* d_ctr = nullptr;
+  uint64_t qoff[re::batch::kMaxQueues] = {};
+  re_batch_tuning tune = {256, 8, 0, 0};
+  // captured frame
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float* g_radiance = nullptr;
+  re_hit* g_primary = nullptr;
+  re_batch_tuning g_tune = {0, 0, 0, 0};
+  cudaStream_t g_stream = nullptr;
+};
+
+namespace re {
+namespace {
+
+using namespace batch;
+
+CamDev cam_of(const re_camera& c) {
+  CamBasis b;
+  camera_basis(c, b);
+  CamDev d;
+  d.campos = {b.campos[0], b.campos[1], b.campos[2]};
+  d.middle = {b.middle[0], b.middle[1], b.middle[2]};
+  d.horizontal = {b.horizontal[0], b.horizontal[1], b.horizontal[2]};
+  d.vertical = {b.vertical[0], b.vertical[1], b.vertical[2]};
+  d.focal = b.focal;
+  return d;
+}
+
+void free_graph(re_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+// Staging: the first `stage_nodes` nodes (breadth-first top of the tree) of
+// every mesh scene are copied to shared memory.
+uint32_t layout_stage(re_batch* b, uint32_t stage_nodes) {
+  uint32_t off = 0;
+  for (uint32_t i = 0; i < b->num_scenes; ++i) {
+    SceneDev& s = b->host_scenes[i];
+    if (s.kind != kMesh) {
+      s.stage = 0;
+      s.stage_off = 0;
+      continue;
+    }
+    uint32_t n = (uint32_t)std::min<size_t>(stage_nodes, b->meshes[i]->host.nodes.size());
+    s.stage = n;
+    s.stage_off = off;
+    off += n;
+  }
+  return off;
+}
+
+size_t smem_bytes(const re_batch* b, uint32_t stage_total) {
+  return b->num_scenes * sizeof(SceneDev) + 512u * (b->perms.size() / 512) +
+         (size_t)stage_total * sizeof(uint2);
+}
+
+// Scene table (with this tuning's staging offsets) to the device and the
+// kernel's shared-memory limit; outside any stream capture.
+re_status prepare(re_batch* b, const re_batch_tuning& tn, cudaStream_t st) {
+  uint32_t stage_total = layout_stage(b, tn.stage_nodes);
+  RE_CUDA(cudaMemcpyAsync(b->d_scenes, b->host_scenes.data(), b->num_scenes * sizeof(SceneDev),
+                          cudaMemcpyHostToDevice, st));
+  RE_CUDA(cudaStreamSynchronize(st));
+  RE_CUDA(cudaFuncSetAttribute(k_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes(b, stage_total)));
+  RE_CUDA(cudaFuncSetAttribute(k_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes(b, stage_total)));
+  return RE_OK;
+}
+
+// One frame: a single launch of the persistent kernel (prepare() first).
+re_status launch(re_batch* b, float* d_radiance, re_hit* d_primary, cudaStream_t st,
+                 const re_batch_tuning& tn, unsigned long long* totals = nullptr) {
+  uint32_t stage_total = layout_stage(b, tn.stage_nodes);
+  size_t smem = smem_bytes(b, stage_total);
+  int per_sm = 0;
+  auto kern = totals ? k_batch<true> : k_batch<false>;
+  RE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)tn.block_threads,
+                                                        smem));
+  if (per_sm < 1) return fail(RE_ERR_LIMIT, "re_batch: tuning does not fit on an SM");
+  BatchDev B;
+  B.scenes = b->d_scenes;
+  B.perms = b->d_perms;
+  B.num_scenes = b->num_scenes;
+  B.perm_count = (uint32_t)(b->perms.size() / 512);
+  B.stage_total = stage_total;
+  B.total_pixels = (uint32_t)b->total_pixels;
+  B.depth = b->depth;
+  B.seed = b->seed;
+  B.refill_min = tn.refill_min;
+  B.mesh_bias = b->mesh_bias;
+  B.queue = b->d_queue;
+  B.flags = b->d_flags;
+  for (uint32_t q = 0; q < kMaxQueues; ++q) B.qoff[q] = b->qoff[q];
+  B.ctr = b->d_ctr;
+  B.radiance = d_radiance;
+  B.primary = reinterpret_cast<int4*>(d_primary);
+  B.totals = totals;
+  kern<<<per_sm * sm_count(), tn.block_threads, smem, st>>>(B);
+  RE_CHECK_LAUNCH("re_batch: launch");
+  return RE_OK;
+}
+
+re_status check_tuning(const re_batch_tuning& t) {
+  if (t.block_threads == 0 || t.block_threads % 32 != 0 || t.block_threads > 512)
+    return fail(RE_ERR_INVALID_ARG, "re_batch: block_threads must be a multiple of 32 in [32, 512]");
+  if (t.refill_min == 0 || t.refill_min > 32)
+    return fail(RE_ERR_INVALID_ARG, "re_batch: refill_min must be in [1, 32]");
+  if (t.stage_nodes > 4096) return fail(RE_ERR_INVALID_ARG, "re_batch: stage_nodes > 4096");
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API re_status re_batch_create(const re_batch_scene* scenes, uint32_t n, const re_path_params* pp,
+                                 re_batch** out) {
+  using namespace re::batch;
+  if (!scenes || !pp || !out || n == 0) return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: bad arguments");
+  *out = nullptr;
+  if (n > kMaxScenes) return re::fail(RE_ERR_LIMIT, "re_batch_create: more than %u scenes", kMaxScenes);
+  if (pp->max_depth < 1 || pp->max_depth > kMaxDepth)
+    return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: max_depth must be in [1, %u]", kMaxDepth);
+  re_batch* b = new (std::nothrow) re_batch();
+  if (!b) return re::fail(RE_ERR_OUT_OF_MEMORY, "re_batch_create: host allocation");
+  RE_CUDA(cudaGetDevice(&b->device));
+  b->num_scenes = n;
+  b->depth = pp->max_depth;
+  b->seed = pp->seed;
+  b->mesh_bias = pp->mesh_bias;
+  b->host_scenes.resize(n);
+  b->meshes.assign(n, nullptr);
+  b->offsets.resize(n);
+  std::vector<uint32_t> perm_seeds;
+  uint64_t off = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const re_batch_scene& s = scenes[i];
+    SceneDev d;
+    std::memset(&d, 0, sizeof(d));
+    if (s.width < 2 || s.height < 2 || !(s.albedo >= 0.f && s.albedo <= 1.f)) {
+      delete b;
+      return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: scene %u: bad size or albedo", i);
+    }
+    d.cam = re::cam_of(s.camera);
+    d.w = s.width;
+    d.h = s.height;
+    d.kind = s.kind;
+    d.albedo = s.albedo;
+    d.pix_off = (uint32_t)off;
+    if (s.kind == RE_BATCH_MESH) {
+      const re_scene* m = s.mesh;
+      int dev = -1;
+      if (!m || !m->d_nodes || (cudaGetDevice(&dev), dev != m->device)) {
+        delete b;
+        return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: scene %u: no mesh on this device", i);
+      }
+      b->meshes[i] = m;
+      d.nodes = m->d_nodes;
+      d.leaves = m->d_leaves;
+      d.tris = m->d_tris;
+      for (int k = 0; k < 3; ++k) {
+        d.bmin[k] = m->host.bmin[k];
+        d.bmax[k] = m->host.bmax[k];
+      }
+      d.max_visits = m->max_visits;
+      b->cap[0] += (uint64_t)s.width * s.height;
+    } else if (s.kind == RE_BATCH_TERRAIN) {
+      const re_sdf_params& f = s.field;
+      if (f.octaves < 1 || f.octaves > 16 || !(f.step_factor > 0.f) || !(f.tmax > 0.f) ||
+          f.max_steps == 0) {
+        delete b;
+        return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: scene %u: bad field", i);
+      }
+      auto it = std::find(perm_seeds.begin(), perm_seeds.end(), f.seed);
+      d.perm_slot = (uint32_t)(it - perm_seeds.begin());
+      if (it == perm_seeds.end()) {
+        perm_seeds.push_back(f.seed);
+        uint32_t full[512];
+        re::perlin_permutation(f.seed, full);
+        for (int k = 0; k < 512; ++k) b->perms.push_back((uint8_t)full[k]);
+      }
+      d.octaves = f.octaves;
+      d.max_steps = f.max_steps;
+      d.scale = f.scale;
+      d.amp = f.amplitude;
+      d.step_factor = f.step_factor;
+      d.eps = f.eps;
+      d.tmax = f.tmax;
+      b->cap[1] += (uint64_t)s.width * s.height;
+    } else {
+      delete b;
+      return re::fail(RE_ERR_INVALID_ARG, "re_batch_create: scene %u: unknown kind", i);
+    }
+    b->offsets[i] = off;
+    off += (uint64_t)s.width * s.height;
+    b->host_scenes[i] = d;
+  }
+  if (off >= (1ull << 28)) {
+    delete b;
+    return re::fail(RE_ERR_LIMIT, "re_batch_create: more than 2^28 pixels in the batch");
+  }
+  b->total_pixels = off;
+  // queue q = 2 * (bounce - 1) + kind holds at most one ray per pixel of that kind
+  uint64_t slots = 0;
+  uint32_t nq = 2 * (b->depth - 1);
+  for (uint32_t q = 0; q < nq; ++q) {
+    b->qoff[q] = slots;
+    slots += b->cap[q & 1u];
+  }
+  cudaError_t e = cudaMalloc(&b->d_scenes, n * sizeof(SceneDev));
+  if (e == cudaSuccess && !b->perms.empty()) e = cudaMalloc(&b->d_perms, b->perms.size());
+  if (e == cudaSuccess && slots) e = cudaMalloc(&b->d_queue, slots * 2 * sizeof(float4));
+  if (e == cudaSuccess && slots) e = cudaMalloc(&b->d_flags, slots * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_ctr, kNumCounters * sizeof(uint32_t));
+  if (e == cudaSuccess && !b->perms.empty())
+    e = cudaMemcpy(b->d_perms, b->perms.data(), b->perms.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && slots) e = cudaMemset(b->d_flags, 0, slots * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(b->d_ctr, 0, kNumCounters * sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    uint32_t one = 1;  // epoch of the first frame (flags start at 0)
+    e = cudaMemcpy(b->d_ctr + kEpoch, &one, 4, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    re_batch_destroy(b);
+    return re::cuda_fail(e, "re_batch_create");
+  }
+  *out = b;
+  return RE_OK;
+}
+
+RE_API re_status re_batch_destroy(re_batch* b) {
+  if (!b) return RE_OK;
+  re::free_graph(b);
+  cudaFree(b->d_scenes);
+  cudaFree(b->d_perms);
+  cudaFree(b->d_queue);
+  cudaFree(b->d_flags);
+  cudaFree(b->d_ctr);
+  delete b;
+  return RE_OK;
+}
+
+RE_API re_status re_batch_pixels(const re_batch* b, uint64_t* total, uint64_t* offsets) {
+  if (!b || !total) return re::fail(RE_ERR_INVALID_ARG, "re_batch_pixels: bad arguments");
+  *total = b->total_pixels;
+  if (offsets) std::memcpy(offsets, b->offsets.data(), b->num_scenes * sizeof(uint64_t));
+  return RE_OK;
+}
+
+RE_API re_status re_batch_render(re_batch* b, float* d_radiance, re_hit* d_primary, void* stream) {
+  if (!b || !d_radiance) return re::fail(RE_ERR_INVALID_ARG, "re_batch_render: bad arguments");
+  re_status s = re::prepare(b, b->tune, (cudaStream_t)stream);
+  if (s != RE_OK) return s;
+  return re::launch(b, d_radiance, d_primary, (cudaStream_t)stream, b->tune);
+}
+
+RE_API re_status re_batch_render_graph(re_batch* b, float* d_radiance, re_hit* d_primary,
+                                       void* stream) {
+  if (!b || !d_radiance) return re::fail(RE_ERR_INVALID_ARG, "re_batch_render_graph: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  bool same = b->exec && b->g_radiance == d_radiance && b->g_primary == d_primary &&
+              b->g_stream == st && std::memcmp(&b->g_tune, &b->tune, sizeof(b->tune)) == 0;
+  if (!same) {
+    re::free_graph(b);
+    // the scene table and shared-memory limit are set outside the capture
+    re_status ps = re::prepare(b, b->tune, st);
+    if (ps != RE_OK) return ps;
+    cudaStream_t cap = nullptr;
+    RE_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    re_status s = RE_OK;
+    if (e == cudaSuccess) {
+      s = re::launch(b, d_radiance, d_primary, cap, b->tune);
+      cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
+      if (e == cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess && s == RE_OK) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    cudaStreamDestroy(cap);
+    if (s != RE_OK) return s;
+    if (e != cudaSuccess) {
+      re::free_graph(b);
+      return re::cuda_fail(e, "re_batch_render_graph: capture");
+    }
+    b->g_radiance = d_radiance;
+    b->g_primary = d_primary;
+    b->g_stream = st;
+    b->g_tune = b->tune;
+  }
+  RE_CUDA(cudaGraphLaunch(b->exec, st));
+  return RE_OK;
+}
+
+// A frame with the work counters on: totals[0..3] = inner-node visits, leaf
+// visits, triangle tests, terrain field evaluations.
+RE_API re_status re_batch_counts(re_batch* b, float* d_radiance, void* stream, uint64_t* totals) {
+  if (!b || !d_radiance || !totals) return re::fail(RE_ERR_INVALID_ARG, "re_batch_counts: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* d = nullptr;
+  RE_CUDA(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(d, 0, 4 * sizeof(unsigned long long), st);
+  re_status s = e == cudaSuccess ? re::prepare(b, b->tune, st) : re::cuda_fail(e, "re_batch_counts");
+  if (s == RE_OK) s = re::launch(b, d_radiance, nullptr, st, b->tune, d);
+  if (s == RE_OK) {
+    e = cudaMemcpyAsync(totals, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = re::cuda_fail(e, "re_batch_counts");
+  }
+  cudaFree(d);
+  return s;
+}
+
+RE_API re_status re_batch_stats_get(re_batch* b, uint64_t* rays, int* error) {
+  using namespace re::batch;
+  if (!b || !rays) return re::fail(RE_ERR_INVALID_ARG, "re_batch_stats_get: bad arguments");
+  uint32_t c[kNumCounters];
+  RE_CUDA(cudaMemcpy(c, b->d_ctr, sizeof(c), cudaMemcpyDeviceToHost));
+  // rays[2 * bounce + kind]: bounce 0 counts every primary ray under kind 0
+  for (uint32_t i = 0; i < 2 * b->depth; ++i) rays[i] = 0;
+  rays[0] = c[kStatsPrimary];
+  for (uint32_t q = 0; q < 2 * (b->depth - 1); ++q) rays[2 + q] = c[kStats + q];
+  if (error) *error = (int)c[kStatsError];
+  return RE_OK;
+}
+
+RE_API re_status re_batch_get_tuning(const re_batch* b, re_batch_tuning* out) {
+  if (!b || !out) return re::fail(RE_ERR_INVALID_ARG, "re_batch_get_tuning: bad arguments");
+  *out = b->tune;
+  return RE_OK;
+}
+
+RE_API re_status re_batch_set_tuning(re_batch* b, const re_batch_tuning* t) {
+  if (!b || !t) return re::fail(RE_ERR_INVALID_ARG, "re_batch_set_tuning: bad arguments");
+  re_status s = re::check_tuning(*t);
+  if (s != RE_OK) return s;
+  b->tune = *t;
+  return RE_OK;
+}
+
+// Times one frame per candidate (after a warm-up frame) and keeps the
+// fastest: block size x refill threshold x staged nodes per mesh scene.
+RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
+                                   re_batch_tuning* out, float* best_ms) {
+  if (!b || !d_radiance) return re::fail(RE_ERR_INVALID_ARG, "re_batch_autotune: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const uint32_t blocks[] = {128, 256, 512};
+  const uint32_t refills[] = {4, 8, 16, 32};
+  const uint32_t stages[] = {0, 64, 512};
+  cudaEvent_t e0, e1;
+  RE_CUDA(cudaEventCreate(&e0));
+  RE_CUDA(cudaEventCreate(&e1));
+  re_batch_tuning best = b->tune;
+  float best_t = 1e30f;
+  re_status s = RE_OK;
+  for (uint32_t bt : blocks)
+    for (uint32_t rf : refills)
+      for (uint32_t sg : stages) {
+        re_batch_tuning t = {bt, rf, sg, 0};
+        size_t smem = re::smem_bytes(b, re::layout_stage(b, sg));
+        if (smem > 200 * 1024) continue;
+        s = re::prepare(b, t, st);
+        if (s != RE_OK) break;
+        s = re::launch(b, d_radiance, nullptr, st, t);  // warm-up
+        if (s != RE_OK) break;
+        cudaEventRecord(e0, st);
+        s = re::launch(b, d_radiance, nullptr, st, t);
+        if (s != RE_OK) break;
+        cudaEventRecord(e1, st);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+          s = re::cuda_fail(e, "re_batch_autotune");
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_t) {
+          best_t = ms;
+          best = t;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s != RE_OK) return s;
+  b->tune = best;
+  s = re::prepare(b, best, st);
+  if (s != RE_OK) return s;
+  if (out) *out = best;
+  if (best_ms) *best_ms = best_t;
+  return RE_OK;
+}
+
+}  // extern "C"

@@ -37,6 +37,13 @@ struct Perm {
 
 __device__ __forceinline__ Perm perm_view(const uint32_t* s) { return Perm{s, threadIdx.x & 31u}; }
 
+// One 512-byte table (several tables fit in shared memory at once; lookups
+// may share banks).
+struct PermBytes {
+  const uint8_t* __restrict__ s;
+  __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return s[j]; }
+};
+
 // gradientDotV (sdf_functions.cuh:26-47) without branches: each case is a
 // sum of two signed coordinates, picked here with selects from bit masks
 // (bit h set = property holds for case h).  The operands and their signs are
@@ -59,7 +66,10 @@ __device__ __forceinline__ float quintic(float t) {
   return ((t * t) * t) * in;
 }
 
-__device__ __forceinline__ float perlin(const Perm& P, float x, float y, float z) {
+// PT: a permutation-table view with operator[] (Perm: per-lane shared
+// copies; PermBytes: one byte table).
+template <class PT>
+__device__ __forceinline__ float perlin(const PT& P, float x, float y, float z) {
   float fx = floorf(x), fy = floorf(y), fz = floorf(z);
   uint32_t xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
   uint32_t xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
@@ -94,7 +104,8 @@ __device__ __forceinline__ float perlin(const Perm& P, float x, float y, float z
   return r;
 }
 
-__device__ __forceinline__ float fbm(const Perm& P, float x, float y, float z,
+template <class PT>
+__device__ __forceinline__ float fbm(const PT& P, float x, float y, float z,
                                      uint32_t octaves, float lacunarity, float gain) {
   float sum = 0.0f, amp = 1.0f;
 #pragma unroll 4
@@ -109,7 +120,8 @@ __device__ __forceinline__ float fbm(const Perm& P, float x, float y, float z,
 }
 
 // d(p) = p.y - amp * fbm(scale * p), lacunarity 2, gain 0.5
-__device__ __forceinline__ float terrain_density(const Perm& P, V3 p,
+template <class PT>
+__device__ __forceinline__ float terrain_density(const PT& P, V3 p,
                                                  uint32_t octaves, float scale, float amp) {
   float f = fbm(P, scale * p.x, scale * p.y, scale * p.z, octaves, 2.0f, 0.5f);
   return __fmaf_rn(-amp, f, p.y);

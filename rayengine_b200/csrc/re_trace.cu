@@ -32,250 +32,11 @@
 
 #include "kd_build.hpp"
 #include "re_common.hpp"
+#include "re_kd.cuh"
+#include "re_scene.hpp"
 #include "re_math.cuh"
 
 namespace re {
-
-constexpr float K_INF = 1e20f;  // RE/RayEngine/RayEngine.h:24
-
-struct KdDev {
-  const uint2* __restrict__ nodes;
-  const float4* __restrict__ leaves;
-  const float4* __restrict__ tris;
-  V3 bmin, bmax;
-  uint32_t max_visits;
-  uint32_t stage;  // nodes [0, stage) are read from shared memory
-};
-
-struct Counters {
-  uint32_t inner, leaf, tests, status;
-};
-
-// gpu_ray_box_intersect (ray_functions.cuh:62-92)
-__device__ __forceinline__ bool ray_box(V3 lo, V3 hi, V3 o, V3 inv, float& tn, float& tf) {
-  float t1 = (lo.x - o.x) * inv.x, t2 = (hi.x - o.x) * inv.x;
-  float t3 = (lo.y - o.y) * inv.y, t4 = (hi.y - o.y) * inv.y;
-  float t5 = (lo.z - o.z) * inv.z, t6 = (hi.z - o.z) * inv.z;
-  float tmin = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
-  float tmax = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
-  if (tmax < 0.0f) return false;
-  if (tmin > tmax) return false;
-  tn = tmin >= 0.0f ? tmin : 0.0f;
-  tf = tmax;
-  return true;
-}
-
-// Moller-Trumbore.  MODE 0: two-sided (KDTree.cpp:909-949), MODE 1:
-// back faces culled (ray_functions.cuh:174-223).
-template <int MODE>
-__device__ __forceinline__ bool ray_tri(V3 o, V3 d, float4 T0, float4 T1, float4 T2,
-                                        float& t, float& u, float& v) {
-  V3 v0 = {T0.x, T0.y, T0.z}, e1 = {T1.x, T1.y, T1.z}, e2 = {T2.x, T2.y, T2.z};
-  V3 h = cross(d, e2);
-  float a = dot(e1, h);
-  if (MODE == 0) {
-    if (a > -0.00001f && a < 0.00001f) return false;
-  } else {
-    if (a < 1e-4f) return false;
-  }
-  float f = 1.0f / a;
-  V3 s = sub(o, v0);
-  float uu = f * dot(s, h);
-  if (uu < 0.0f || uu > 1.0f) return false;
-  V3 q = cross(s, e1);
-  float vv = f * dot(d, q);
-  if (vv < 0.0f || uu + vv > 1.0f) return false;
-  float tt = f * dot(e2, q);
-  if (!(tt > (MODE == 0 ? 0.00001f : 1e-4f))) return false;
-  t = tt;
-  u = uu;
-  v = vv;
-  return true;
-}
-
-struct HitState {
-  float t, u, v;
-  int32_t id;
-  uint32_t ref;        // leaf-order triangle slot of the best hit
-  uint32_t leaf_node;  // node index of the leaf the best hit was found in
-};
-
-__device__ __forceinline__ uint2 load_node(const KdDev& kd, const uint2* snodes, uint32_t i) {
-  return i < kd.stage ? snodes[i] : __ldg(&kd.nodes[i]);
-}
-
-// Stackless rope traversal (stackless_kdtree_traversal,
-// ray_functions.cuh:231-360) with the exit face taken from the slab test and
-// split decisions made on the ray parameter so that a point on a split plane
-// goes to the side the ray moves into.
-//
-// The walk is a per-lane state machine: trav_init() clips the ray to the
-// root box, each trav_step() descends to one leaf, tests its triangles and
-// follows one rope.  Kernels either run a ray to completion (traverse()) or
-// interleave steps of many rays and refill finished lanes (k_ao_secondary).
-//
-// start: a leaf node to begin in instead of descending from the root (a
-// secondary ray starts where its primary ray hit); used only when the ray
-// origin lies in that leaf's region, otherwise the walk starts at the root.
-// Either way every leaf the ray crosses is visited, so hits are unchanged.
-struct Trav {
-  V3 o, d, inv;
-  float t_entry, best_t, best_u, best_v;
-  int32_t best_id;
-  uint32_t best_ref, best_leaf, node, visits;
-  bool live;
-};
-
-__device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, float tmax,
-                                          uint32_t start) {
-  s.o = o;
-  s.d = d;
-  s.inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
-  s.best_id = -1;
-  s.best_u = 0.f;
-  s.best_v = 0.f;
-  s.best_ref = 0xFFFFFFFFu;
-  s.best_leaf = 0;
-  s.node = 0;
-  s.visits = 0;
-  float t_root_exit;
-  s.live = ray_box(kd.bmin, kd.bmax, o, s.inv, s.t_entry, t_root_exit);
-  if (!s.live) return;
-  s.best_t = fminf(t_root_exit, tmax);
-  s.live = s.t_entry < s.best_t;
-  if (s.live && start != 0) {
-    uint2 sn = __ldg(&kd.nodes[start]);
-    if ((sn.y & 3u) == 3u) {
-      const float4* SL = kd.leaves + 4 * (size_t)(sn.y >> 2);
-      float4 A = __ldg(SL), B = __ldg(SL + 1);
-      if (o.x >= A.x && o.x <= A.w && o.y >= A.y && o.y <= B.x && o.z >= A.z && o.z <= B.y)
-        s.node = start;
-    }
-  }
-}
-
-template <int MODE, bool ANYHIT, bool COUNT>
-__device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2* snodes,
-                                          Counters& c) {
-  const V3 o = s.o, d = s.d, inv = s.inv;
-  const float t_entry = s.t_entry;
-  uint32_t node = s.node;
-  uint2 nd = load_node(kd, snodes, node);
-  while ((nd.y & 3u) != 3u) {
-    uint32_t k = nd.y & 3u;
-    float split = __uint_as_float(nd.x);
-    float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
-    bool left;
-    if (dk > 0.0f)
-      left = t_entry < (split - ok) * ik;
-    else if (dk < 0.0f)
-      left = t_entry >= (split - ok) * ik;
-    else
-      left = ok < split;
-    node = (nd.y >> 2) + (left ? 0u : 1u);
-    nd = load_node(kd, snodes, node);
-    if (COUNT) c.inner++;
-  }
-  const float4* L = kd.leaves + 4 * (size_t)(nd.y >> 2);
-  float4 A = __ldg(L), B = __ldg(L + 1);
-  if (COUNT) c.leaf++;
-  uint32_t first = __float_as_uint(B.z), count = __float_as_uint(B.w);
-  for (uint32_t i = first; i < first + count; ++i) {
-    const float4* T = kd.tris + 3 * (size_t)i;
-    float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
-    int32_t id = __float_as_int(T0.w);
-    float t, u, v;
-    if (COUNT) c.tests++;
-    if (ray_tri<MODE>(o, d, T0, T1, T2, t, u, v)) {
-      if (t < s.best_t || (t == s.best_t && id < s.best_id && s.best_id >= 0)) {
-        s.best_t = t;
-        s.best_id = id;
-        s.best_u = u;
-        s.best_v = v;
-        s.best_ref = i;
-        s.best_leaf = node;
-        if (ANYHIT) {
-          s.live = false;
-          return;
-        }
-      }
-    }
-  }
-  float texit = __int_as_float(0x7f800000);
-  int face = -1;
-  {
-    float tk;
-    if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
-    else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
-    if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
-    else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
-    if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
-    else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
-  }
-  if (face < 0) {
-    s.live = false;
-    return;
-  }
-  s.t_entry = fmaxf(t_entry, texit);
-  if (!(s.t_entry < s.best_t)) {
-    s.live = false;
-    return;
-  }
-  int32_t rope = __ldg(reinterpret_cast<const int32_t*>(L + 2) + face);
-  if (rope < 0) {
-    s.live = false;
-    return;
-  }
-  s.node = (uint32_t)rope;
-  if (++s.visits >= kd.max_visits) {
-    c.status = 1;
-    s.live = false;
-  }
-}
-
-__device__ __forceinline__ void trav_result(const Trav& s, HitState& hs) {
-  if (s.best_id >= 0) {
-    hs.t = s.best_t;
-    hs.u = s.best_u;
-    hs.v = s.best_v;
-    hs.id = s.best_id;
-    hs.ref = s.best_ref;
-    hs.leaf_node = s.best_leaf;
-  } else {
-    hs.t = K_INF;
-    hs.u = 0.f;
-    hs.v = 0.f;
-    hs.id = -1;
-    hs.ref = 0xFFFFFFFFu;
-    hs.leaf_node = 0;
-  }
-}
-
-template <int MODE, bool ANYHIT, bool COUNT>
-__device__ __forceinline__ void traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
-                                         float tmax, uint32_t start, HitState& hs, Counters& c) {
-  Trav s;
-  trav_init(s, kd, o, d, tmax, start);
-  while (s.live) trav_step<MODE, ANYHIT, COUNT>(s, kd, snodes, c);
-  trav_result(s, hs);
-}
-
-__device__ __forceinline__ void stage_nodes(const KdDev& kd, uint2* snodes) {
-  for (uint32_t i = threadIdx.x; i < kd.stage; i += blockDim.x) snodes[i] = __ldg(&kd.nodes[i]);
-  __syncthreads();
-}
-
-__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter) {
-  uint32_t lane = threadIdx.x & 31u;
-  uint32_t t = 0;
-  if (lane == 0) t = atomicAdd(counter, 1u);
-  return __shfl_sync(0xFFFFFFFFu, t, 0);
-}
-
-__device__ __forceinline__ void store_hit(re_hit* out, size_t i, const HitState& hs) {
-  reinterpret_cast<int4*>(out)[i] =
-      make_int4(hs.id, __float_as_int(hs.t), __float_as_int(hs.u), __float_as_int(hs.v));
-}
 
 // --------------------------------------------------------------- kernels
 // Primary rays, persistent warps over 8x4 pixel tiles.
@@ -521,23 +282,6 @@ __global__ void __launch_bounds__(256, 5) k_ao_secondary(KdDev kd, AoDev ao, AoQ
 }  // namespace re
 
 // ------------------------------------------------------------------ host
-struct re_scene {
-  int device = 0;
-  re::FlatTree host;
-  uint2* d_nodes = nullptr;
-  float4* d_leaves = nullptr;
-  float4* d_tris = nullptr;
-  uint32_t* d_counters = nullptr;  // [0] tiles, [1] queue size, [2] queue chunks
-  float4* d_queue = nullptr;
-  size_t queue_cap = 0;  // rays
-  uint32_t max_visits = 16384;
-  uint32_t stage = 0;
-  int blocks_per_sm = 0;
-  float ao_length = 1.0f;    // AO ray length of the last primary pass
-  uint32_t queue_stride = 0;  // record capacity per ray kind in d_queue
-  re_tuning tune = {0, 0, 32, 0};
-};
-
 namespace re {
 namespace {
 

@@ -430,11 +430,13 @@ class NeuralTerrainSDF:
     name = "nsdf_terrain"
     dtype = "bf16 (network, FP32 accumulate) + f32 (exact field)"
 
-    def __init__(self, torch):
+    def __init__(self, torch, train_steps=None):
         import rayengine_b200 as rb
 
         self.rb = rb
         self.ncfg = rb.configs.NeuralTerrainConfig()
+        if train_steps:
+            self.ncfg.train_steps = train_steps
         self.cfg = cfg = self.ncfg.terrain
         self.cam = cfg.camera()
         self.params = cfg.params()
@@ -532,11 +534,13 @@ class BatchWavefront:
     persistent launch per frame replayed from a CUDA graph, autotuned."""
     name = "batch32"
 
-    def __init__(self, torch):
+    def __init__(self, torch, num_scenes=None):
         import rayengine_b200 as rb
 
         self.rb = rb
         self.cfg = rb.configs.BatchConfig()
+        if num_scenes:
+            self.cfg.num_scenes = num_scenes
         t0 = time.perf_counter()
         self.batch, self.meshes = self.cfg.build()
         self.build_s = time.perf_counter() - t0
@@ -773,7 +777,12 @@ def run_ours(args):
     torch.cuda.set_device(local)
     init_dist(world)
     dev = torch.device("cuda", local)
-    wl = WORKLOADS[args.config](torch)
+    opts = {}
+    if args.config == "nsdf_terrain" and args.train_steps:
+        opts["train_steps"] = args.train_steps
+    if args.config == "batch32" and args.scenes:
+        opts["num_scenes"] = args.scenes
+    wl = WORKLOADS[args.config](torch, **opts)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     phases = wl.phases(stream)
@@ -783,10 +792,14 @@ def run_ours(args):
             fn()
 
     if args.profile:
-        # for ncu captures: one warm-up step, one flushed step, no timing
+        # for ncu captures: one warm-up step, then one flushed step inside the
+        # NVTX range "profile" (ncu --nvtx --nvtx-include "profile/"), no timing
         step()
         flush.fill_(1)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profile")
         step()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         print(json.dumps({"profile": wl.name, "kernels_per_step": wl.kernels_per_step}))
         return 0
@@ -875,6 +888,10 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS), default="heightfield_ao")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--train-steps", type=int, default=0,
+                    help="nsdf_terrain: training steps at set-up (default: the config's 20000)")
+    ap.add_argument("--scenes", type=int, default=0,
+                    help="batch32: number of scenes (default: the config's 32)")
     ap.add_argument("--profile", action="store_true",
                     help="one warm-up and one flushed step, untimed (for ncu captures)")
     args = ap.parse_args(argv)

@@ -386,6 +386,54 @@ RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
 RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
 RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);
 
+/* ---- mesh ingestion (host) ---------------------------------------------
+ * Replaces RStaticMesh::LoadFromFile (RE/Objects/RStaticMesh.cpp:68-128,
+ * PLY through rply) and WavefrontOBJ::loadObjFromFile
+ * (RayEngine/includes/ObjFileReader.h:65-180).  PLY: ascii or binary, any
+ * numeric property types, vertex x/y/z and face vertex_indices; faces with
+ * more corners are fan-triangulated unless RE_MESH_FIRST_TRIANGLE (the
+ * reference's reader keeps the first three corners).  OBJ: v and f with
+ * p, p/t, p//n, p/t/n corners; one vertex per distinct corner in order of
+ * first use, quads split as the reference does, larger polygons fanned. */
+#define RE_MESH_FIRST_TRIANGLE 1u
+typedef struct re_mesh re_mesh;
+RE_API re_status re_mesh_load(const char* path, uint32_t flags, re_mesh** out);
+RE_API re_status re_mesh_info(const re_mesh* m, uint32_t* num_verts,
+                              uint32_t* num_faces);
+/* verts: 3 floats per vertex; faces: 3 indices per triangle. */
+RE_API re_status re_mesh_copy(const re_mesh* m, float* verts, uint32_t* faces);
+RE_API re_status re_mesh_destroy(re_mesh* m);
+
+/* ---- shaded frame (the reference's render call) ----------------------
+ * Replaces cuda_render_frame (renderer.cu:702-738) with its per-pixel
+ * shading (trace_secondary_rays :435-492, phong_light / shade
+ * material_functions.cuh:69-119, illuminate cuda_helper_functions.h:90-102)
+ * and rgbaFloatToInt (cuda_helper_functions.h:61-68): primary closest hits,
+ * Phong with one shadow ray per point light, a sky gradient for misses,
+ * packed RGBA8 (R in the low byte, alpha 255) in a W x H device buffer. */
+typedef struct re_light {
+  float pos[3];
+  float intensity;        /* the reference's scene uses 20000               */
+} re_light;
+
+typedef struct re_shade_params {
+  float albedo[3];        /* material colour, the base of every hit         */
+  float sky_zenith[3];    /* miss colour = lerp(horizon, zenith, max(d.y,0))*/
+  float sky_horizon[3];
+  uint32_t flags;         /* RE_TRACE_ONE_SIDED for the primary rays        */
+} re_shade_params;
+
+RE_API re_status re_render_frame(re_scene* s, const re_camera* cam,
+                                 const re_light* lights, uint32_t num_lights,
+                                 const re_shade_params* sp, uint32_t w, uint32_t h,
+                                 uint32_t* d_rgba, void* stream);
+/* State for cuda_render_frame(), which keeps the reference's signature
+ * (scene, camera and lights are globals there); animate_light != 0 moves
+ * light 0 after every frame as the reference's Craze kernel does. */
+RE_API re_status re_frame_bind(re_scene* s, const re_camera* cam,
+                               const re_light* lights, uint32_t num_lights,
+                               const re_shade_params* sp, int animate_light);
+
 /* ---- batched wavefront path tracing ----------------------------------
  * No single counterpart in the reference, which renders one scene per
  * frame (cuda_render_frame, renderer.cu:702-738; bounce rays in
@@ -456,5 +504,10 @@ RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
 
 #ifdef __cplusplus
 }
+/* The reference's render call, same C++ signature (renderer.cu:701):
+ * renders the state bound by re_frame_bind into `output` (device, W x H
+ * RGBA8) and waits; errors go to re_last_error(). */
+void cuda_render_frame(unsigned int* output, const unsigned int& width,
+                       const unsigned int& heigth);
 #endif
 #endif

@@ -831,3 +831,67 @@ uint32_t o_path_pixel(const o_path_scene* s, uint32_t gpix, uint32_t local_pix, 
   }
   return depth;
 }
+
+/* ------------------------------------------------------- shaded frame */
+/* One pixel of the shaded frame (Phong with shadow rays, sky gradient,
+ * rgbaFloatToInt pack): brute-force closest hits (mode for the primary
+ * ray, two-sided shadow rays). */
+static uint32_t pack_rgba(const float c[3]) {
+  float v[3];
+  for (int k = 0; k < 3; ++k) v[k] = c[k] < 0.0f ? 0.0f : (c[k] > 1.0f ? 1.0f : c[k]);
+  return (255u << 24) | ((uint32_t)(v[2] * 255.0f) << 16) | ((uint32_t)(v[1] * 255.0f) << 8) |
+         (uint32_t)(v[0] * 255.0f);
+}
+
+uint32_t o_frame_pixel(const float* tris, int32_t n, const float bmin[3], const float bmax[3],
+                       const o_camera_basis* cb, uint32_t w, uint32_t h, uint32_t x, uint32_t y,
+                       int mode, const float* light_pos, const float* light_int,
+                       uint32_t num_lights, const float albedo[3], const float zenith[3],
+                       const float horizon[3]) {
+  float o[3], d[3], col[3];
+  o_generate_ray(cb, w, h, x, y, o, d);
+  o_hit hit;
+  o_trace_bruteforce(tris, n, bmin, bmax, o, d, mode, &hit);
+  if (hit.id < 0) {
+    float s = d[1] > 0.0f ? d[1] : 0.0f;
+    for (int k = 0; k < 3; ++k) col[k] = fmaf(s, zenith[k] - horizon[k], horizon[k]);
+    return pack_rgba(col);
+  }
+  const float* T = tris + 12 * (size_t)hit.id;
+  float nn[3], p[3], org[3];
+  cross3(T + 4, T + 8, nn);
+  normalize3(nn);
+  if (dot3(nn, d) > 0.0f) {
+    nn[0] = -nn[0]; nn[1] = -nn[1]; nn[2] = -nn[2];
+  }
+  for (int k = 0; k < 3; ++k) {
+    p[k] = fmaf(hit.t, d[k], o[k]);
+    org[k] = fmaf(nn[k], 1e-4f, p[k]);
+    col[k] = albedo[k];
+  }
+  for (uint32_t i = 0; i < num_lights; ++i) {
+    const float* L = light_pos + 3 * i;
+    float pl[3] = {p[0] - L[0], p[1] - L[1], p[2] - L[2]};
+    float r2 = dot3(pl, pl);
+    float dist = sqrtf(r2);
+    float l[3] = {pl[0] / dist, pl[1] / dist, pl[2] / dist};
+    float kk = light_int[i] / (4.0f * 3.14159265358979f * r2);
+    float li[3] = {0.86f * kk, 0.80f * kk, 0.45f * kk};
+    float toward[3] = {-l[0], -l[1], -l[2]};
+    o_hit sh;
+    o_trace_bruteforce(tris, n, bmin, bmax, org, toward, 0, &sh);
+    if (sh.id >= 0 && sh.t < dist) continue;
+    float nl = dot3(nn, toward);
+    nl = nl > 0.0f ? nl : 0.0f;
+    float dn = dot3(nn, l);
+    float R[3];
+    for (int k = 0; k < 3; ++k) R[k] = fmaf(-2.0f * dn, nn[k], l[k]);
+    float rv = -dot3(R, d);
+    rv = rv > 0.0f ? rv : 0.0f;
+    float r2v = rv * rv, r4 = r2v * r2v, r8 = r4 * r4;
+    float spec = r8 * r2v;
+    float dfac = 0.8f * (0.18f * nl), sfac = 0.2f * spec;
+    for (int k = 0; k < 3; ++k) col[k] = fmaf(li[k], sfac, fmaf(li[k], dfac, col[k]));
+  }
+  return pack_rgba(col);
+}

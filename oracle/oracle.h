@@ -142,6 +142,12 @@ typedef struct {
 /* returns the number of rays the path traced */
 uint32_t o_path_pixel(const o_path_scene* s, uint32_t gpix, uint32_t local_pix, uint32_t depth,
                       uint32_t seed, float mesh_bias, float* radiance, o_hit* primary);
+/* --- shaded frame: one pixel, packed RGBA8 ------------------------------ */
+uint32_t o_frame_pixel(const float* tris, int32_t n, const float bmin[3], const float bmax[3],
+                       const o_camera_basis* cb, uint32_t w, uint32_t h, uint32_t x, uint32_t y,
+                       int mode, const float* light_pos, const float* light_int,
+                       uint32_t num_lights, const float albedo[3], const float zenith[3],
+                       const float horizon[3]);
 #ifdef __cplusplus
 }
 #endif

@@ -255,3 +255,19 @@ void o_batch_path(const o_path_scene* scenes, int nscenes, const uint64_t* offse
     if (nrays) nrays[i] = r;
   }
 }
+
+/* Shaded frame over the given pixels (or all when pixels == NULL). */
+void o_batch_frame(const float* tris, int32_t n, const float bmin[3], const float bmax[3],
+                   const o_camera* cam, uint32_t w, uint32_t h, int mode, const float* light_pos,
+                   const float* light_int, uint32_t num_lights, const float albedo[3],
+                   const float zenith[3], const float horizon[3], const uint32_t* pixels,
+                   int64_t npix, uint32_t* out, int threads) {
+  o_camera_basis b;
+  o_camera_setup(cam, &b);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < npix; ++i) {
+    uint32_t p = pixels ? pixels[i] : (uint32_t)i;
+    out[i] = o_frame_pixel(tris, n, bmin, bmax, &b, w, h, p % w, p / w, mode, light_pos, light_int,
+                           num_lights, albedo, zenith, horizon);
+  }
+}

@@ -406,3 +406,53 @@ def batch_path(scenes, offsets, gpix, depth, seed, mesh_bias, nthreads=0):
                        ctypes.c_uint32(depth), ctypes.c_uint32(seed), ctypes.c_float(mesh_bias),
                        _p(rad), _p(prim), _p(nrays), ctypes.c_int(nthreads))
     return rad, prim, nrays
+
+
+def frame_rgba(packed, bmin, bmax, cam, w, h, lights, albedo, zenith, horizon, mode=0,
+               pixels=None, nthreads=0):
+    """Packed RGBA8 of the shaded frame. lights: list of (pos xyz, intensity)."""
+    tris = np.ascontiguousarray(packed, np.float32)
+    lp = np.ascontiguousarray([l[0] for l in lights], np.float32).reshape(-1)
+    li = np.ascontiguousarray([l[1] for l in lights], np.float32)
+    f3 = lambda v: np.ascontiguousarray(v, np.float32)
+    bmin, bmax, albedo, zenith, horizon = map(f3, (bmin, bmax, albedo, zenith, horizon))
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, np.uint32)
+    oc = camera(cam)
+    lib().o_batch_frame(_p(tris), ctypes.c_int32(tris.shape[0]), _p(bmin), _p(bmax),
+                        ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h), ctypes.c_int(mode),
+                        _p(lp) if len(lights) else None, _p(li) if len(lights) else None,
+                        ctypes.c_uint32(len(lights)), _p(albedo), _p(zenith), _p(horizon),
+                        _p(pix), ctypes.c_int64(n), _p(out), ctypes.c_int(nthreads))
+    return out
+
+
+def ref_ply_lib():
+    """oracle/_ref/libre_ply.so (the reference's rply + loader shim) or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libre_ply.so")
+    if not os.path.exists(path):
+        return None
+    lib_ = ctypes.CDLL(path)
+    lib_.ref_ply_load.restype = ctypes.c_int
+    lib_.ref_ply_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p),
+                                  ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_void_p),
+                                  ctypes.POINTER(ctypes.c_long)]
+    lib_.ref_ply_free.argtypes = [ctypes.c_void_p]
+    return lib_
+
+
+def ref_ply_load(path):
+    """(ok, vertices (V,3) float32, faces (F,3) uint32) read the reference's way."""
+    lib_ = ref_ply_lib()
+    v, f = ctypes.c_void_p(), ctypes.c_void_p()
+    nv, nf = ctypes.c_long(), ctypes.c_long()
+    ok = lib_.ref_ply_load(str(path).encode(), ctypes.byref(v), ctypes.byref(nv), ctypes.byref(f),
+                           ctypes.byref(nf))
+    verts = np.ctypeslib.as_array((ctypes.c_float * (3 * nv.value)).from_address(v.value)).copy() \
+        if nv.value else np.zeros(0, np.float32)
+    faces = np.ctypeslib.as_array((ctypes.c_uint32 * (3 * nf.value)).from_address(f.value)).copy() \
+        if nf.value else np.zeros(0, np.uint32)
+    lib_.ref_ply_free(v)
+    lib_.ref_ply_free(f)
+    return bool(ok), verts.reshape(-1, 3), faces.reshape(-1, 3)

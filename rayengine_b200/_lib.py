@@ -146,6 +146,15 @@ class re_nsdf_trace_params(ctypes.Structure):
 NSDF_EXACT_ONLY = 1
 
 
+class re_light(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_float * 3), ("intensity", ctypes.c_float)]
+
+
+class re_shade_params(ctypes.Structure):
+    _fields_ = [("albedo", ctypes.c_float * 3), ("sky_zenith", ctypes.c_float * 3),
+                ("sky_horizon", ctypes.c_float * 3), ("flags", ctypes.c_uint32)]
+
+
 class re_batch_scene(ctypes.Structure):
     _fields_ = [
         ("kind", ctypes.c_uint32),
@@ -219,6 +228,12 @@ _SIGS = {
     "re_nsdf_trace_network": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_exact": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int), _P]),
+    "re_mesh_load": (ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(ctypes.c_void_p)]),
+    "re_mesh_info": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "re_mesh_copy": (ctypes.c_int, [_P, _P, _P]),
+    "re_mesh_destroy": (ctypes.c_int, [_P]),
+    "re_render_frame": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), ctypes.POINTER(re_light), _U32, ctypes.POINTER(re_shade_params), _U32, _U32, _P, _P]),
+    "re_frame_bind": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), ctypes.POINTER(re_light), _U32, ctypes.POINTER(re_shade_params), ctypes.c_int]),
     "re_batch_create": (ctypes.c_int, [ctypes.POINTER(re_batch_scene), _U32, ctypes.POINTER(re_path_params), ctypes.POINTER(ctypes.c_void_p)]),
     "re_batch_destroy": (ctypes.c_int, [_P]),
     "re_batch_pixels": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _P]),

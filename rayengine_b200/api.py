@@ -305,6 +305,25 @@ class KDScene:
         return {"stage_nodes": t.stage_nodes, "queue_kind_major": t.queue_kind_major,
                 "refill_min": t.refill_min, "frame_ms": round(ms.value, 4)}
 
+    def render_frame(self, cam: RCamera, w: int, h: int, lights, shade, out=None, stream=None):
+        """Shaded RGBA8 frame -> uint32-valued int32 CUDA tensor (h*w,).
+
+        lights: [(pos xyz, intensity)]; shade: shade_params(...)."""
+        import torch
+
+        if out is None:
+            out = torch.empty(h * w, dtype=torch.int32, device="cuda")
+        arr = _light_array(lights)
+        call("re_render_frame", self._h, ctypes.byref(cam), arr, len(lights),
+             ctypes.byref(shade), w, h, _dptr(out), _stream_ptr(stream))
+        return out
+
+    def bind_frame(self, cam: RCamera, lights, shade, animate_light=False):
+        """State for the reference-style cuda_render_frame(output, w, h)."""
+        arr = _light_array(lights)
+        call("re_frame_bind", self._h, ctypes.byref(cam), arr, len(lights), ctypes.byref(shade),
+             1 if animate_light else 0)
+
     def render_ao_counts(self, cam: RCamera, w: int, h: int, params, stream=None) -> dict:
         """Traversal work of the AO frame (sums over all rays of each pass)."""
         import torch
@@ -598,3 +617,54 @@ class Batch:
              ctypes.byref(ms))
         return {"block_threads": t.block_threads, "refill_min": t.refill_min,
                 "stage_nodes": t.stage_nodes, "frame_ms": round(ms.value, 4)}
+
+
+# ------------------------------------------------------------ shaded frame
+def shade_params(albedo=(0.6, 0.6, 0.6), sky_zenith=(0.35, 0.55, 0.95),
+                 sky_horizon=(0.85, 0.9, 1.0), one_sided=False):
+    p = _lib.re_shade_params()
+    p.albedo[:] = [float(x) for x in albedo]
+    p.sky_zenith[:] = [float(x) for x in sky_zenith]
+    p.sky_horizon[:] = [float(x) for x in sky_horizon]
+    p.flags = TRACE_ONE_SIDED if one_sided else 0
+    return p
+
+
+def _light_array(lights):
+    arr = (_lib.re_light * max(1, len(lights)))()
+    for i, (pos, inten) in enumerate(lights):
+        arr[i].pos[:] = [float(x) for x in pos]
+        arr[i].intensity = float(inten)
+    return arr
+
+
+def cuda_render_frame(output, width: int, height: int) -> str:
+    """The reference's render call (C++ symbol cuda_render_frame(uint*, const
+    uint&, const uint&)) on a CUDA tensor of width*height 32-bit pixels."""
+    fn = getattr(lib, "_Z17cuda_render_framePjRKjS1_")
+    fn.restype = None
+    fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    w, h = ctypes.c_uint32(width), ctypes.c_uint32(height)
+    fn(_dptr(output), ctypes.byref(w), ctypes.byref(h))
+    err = lib.re_last_error()
+    return err.decode() if err else ""
+
+
+# ------------------------------------------------------------ mesh files
+MESH_FIRST_TRIANGLE = 1
+
+
+def load_mesh(path: str, first_triangle_only: bool = False):
+    """(vertices float32 (V,3), faces uint32 (F,3)) from a .ply or .obj file."""
+    h = ctypes.c_void_p()
+    call("re_mesh_load", str(path).encode(), MESH_FIRST_TRIANGLE if first_triangle_only else 0,
+         ctypes.byref(h))
+    try:
+        nv, nf = ctypes.c_uint32(), ctypes.c_uint32()
+        call("re_mesh_info", h, ctypes.byref(nv), ctypes.byref(nf))
+        verts = np.empty((nv.value, 3), np.float32)
+        faces = np.empty((nf.value, 3), np.uint32)
+        call("re_mesh_copy", h, verts.ctypes.data, faces.ctypes.data)
+    finally:
+        lib.re_mesh_destroy(h)
+    return verts, faces

@@ -386,6 +386,42 @@ RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
 RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
 RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);
 
+/* ---- voxel SDF ----------------------------------------------------------
+ * Replaces the reference's voxel-SDF path: the bake kernel generate_noise
+ * (renderer.cu:106-126), the .rsdf file (Grid.cpp:23-64, save_map
+ * renderer.cu:839-870) and get_distance's LOW / MEDIUM / HIGH sampling
+ * (sdf_functions.cuh:394-419).  A grid is dim[0] x dim[1] x dim[2] voxels
+ * of 2 floats {distance, material}, x fastest; voxel (i, j, k) holds the
+ * field at origin + (i, j, k) * spacing; lookups clamp to the edge. */
+#define RE_VOXEL_LOW 0u    /* nearest voxel                                  */
+#define RE_VOXEL_MEDIUM 1u /* trilinear                                      */
+#define RE_VOXEL_HIGH 2u   /* tricubic B-spline over 4 x 4 x 4 voxels        */
+typedef struct re_voxel_grid {
+  uint32_t dim[3];
+  float spacing[3];
+  float origin[3];
+} re_voxel_grid;
+/* d_grid: 2 * voxels floats; distance = the field's density, material 0. */
+RE_API re_status re_voxel_bake(const re_sdf_params* field, const re_voxel_grid* g,
+                               float* d_grid, void* stream);
+RE_API re_status re_voxel_sample(const float* d_grid, const re_voxel_grid* g,
+                                 uint32_t quality, const float* d_pts, uint32_t n,
+                                 float* d_out, void* stream);
+/* Sphere tracing inside the grid's box with march's step_factor, eps, tmax
+ * and max_steps; output as re_sdf_trace (normal: central differences with
+ * half the smallest spacing). */
+RE_API re_status re_voxel_trace(const float* d_grid, const re_voxel_grid* g,
+                                uint32_t quality, const re_sdf_params* march,
+                                const re_camera* cam, uint32_t w, uint32_t h,
+                                re_sdf_hit* d_out, void* stream);
+/* .rsdf files: int32 dim[3], float spacing[3], {distance, material} per
+ * voxel, x fastest.  re_voxel_load fills g (origin 0) and, when host_grid
+ * is not NULL, up to capacity_voxels voxels. */
+RE_API re_status re_voxel_save(const char* path, const re_voxel_grid* g,
+                               const float* host_grid);
+RE_API re_status re_voxel_load(const char* path, re_voxel_grid* g, float* host_grid,
+                               uint64_t capacity_voxels);
+
 /* ---- mesh ingestion (host) ---------------------------------------------
  * Replaces RStaticMesh::LoadFromFile (RE/Objects/RStaticMesh.cpp:68-128,
  * PLY through rply) and WavefrontOBJ::loadObjFromFile

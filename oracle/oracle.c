@@ -895,3 +895,113 @@ uint32_t o_frame_pixel(const float* tris, int32_t n, const float bmin[3], const 
   }
   return pack_rgba(col);
 }
+
+/* ------------------------------------------------------------ voxel SDF */
+/* Grid lookups and the voxel sphere tracer (LOW nearest, MEDIUM trilinear,
+ * HIGH tricubic B-spline), edge-clamped. */
+static float vox_fetch(const o_voxel* g, int x, int y, int z) {
+  x = x < 0 ? 0 : (x > g->dim[0] - 1 ? g->dim[0] - 1 : x);
+  y = y < 0 ? 0 : (y > g->dim[1] - 1 ? g->dim[1] - 1 : y);
+  z = z < 0 ? 0 : (z > g->dim[2] - 1 ? g->dim[2] - 1 : z);
+  return g->v[2 * ((size_t)x + (size_t)g->dim[0] * ((size_t)y + (size_t)g->dim[1] * z))];
+}
+
+static float vox_bspline(float t) {
+  t = fabsf(t);
+  const float a = 2.0f - t;
+  if (t < 1.0f) return 2.0f / 3.0f - 0.5f * t * t * a;
+  if (t < 2.0f) return a * a * a / 6.0f;
+  return 0.0f;
+}
+
+static float vox_bilerp(float tx, float ty, float c00, float c10, float c01, float c11) {
+  return (1.0f - tx) * (1.0f - ty) * c00 + tx * (1.0f - ty) * c10 + (1.0f - tx) * ty * c01 +
+         tx * ty * c11;
+}
+
+float o_voxel_sample(const o_voxel* g, uint32_t quality, const float p[3]) {
+  float u[3];
+  for (int k = 0; k < 3; ++k) u[k] = (p[k] - g->origin[k]) / g->spacing[k];
+  if (quality == 0) return vox_fetch(g, (int)floorf(u[0]), (int)floorf(u[1]), (int)floorf(u[2]));
+  if (quality == 1) {
+    float fx = floorf(u[0]), fy = floorf(u[1]), fz = floorf(u[2]);
+    int x = (int)fx, y = (int)fy, z = (int)fz;
+    float tx = u[0] - fx, ty = u[1] - fy, tz = u[2] - fz;
+    float e = vox_bilerp(tx, ty, vox_fetch(g, x, y, z), vox_fetch(g, x + 1, y, z),
+                         vox_fetch(g, x, y + 1, z), vox_fetch(g, x + 1, y + 1, z));
+    float f = vox_bilerp(tx, ty, vox_fetch(g, x, y, z + 1), vox_fetch(g, x + 1, y, z + 1),
+                         vox_fetch(g, x, y + 1, z + 1), vox_fetch(g, x + 1, y + 1, z + 1));
+    return e * (1.0f - tz) + f * tz;
+  }
+  float cg[3] = {u[0] - 0.5f, u[1] - 0.5f, u[2] - 0.5f};
+  float idx[3] = {floorf(cg[0]), floorf(cg[1]), floorf(cg[2])};
+  float fr[3] = {cg[0] - idx[0], cg[1] - idx[1], cg[2] - idx[2]};
+  int ix = (int)idx[0], iy = (int)idx[1], iz = (int)idx[2];
+  float result = 0.0f;
+  for (int z = -1; z <= 2; ++z) {
+    float bz = vox_bspline((float)z - fr[2]);
+    for (int y = -1; y <= 2; ++y) {
+      float byz = vox_bspline((float)y - fr[1]) * bz;
+      for (int x = -1; x <= 2; ++x) {
+        float bxyz = vox_bspline((float)x - fr[0]) * byz;
+        result += bxyz * vox_fetch(g, ix + x, iy + y, iz + z);
+      }
+    }
+  }
+  return result;
+}
+
+void o_voxel_trace_pixel(const o_voxel* g, uint32_t quality, float step_factor, float eps,
+                         float tmax, uint32_t max_steps, const o_camera_basis* cb, uint32_t w,
+                         uint32_t h, uint32_t pix, o_sdf_hit* out) {
+  float o[3], d[3];
+  o_generate_ray(cb, w, h, pix % w, pix / w, o, d);
+  float t0 = 0.0f, t1 = tmax;
+  for (int k = 0; k < 3; ++k) {
+    float lo = g->origin[k], hi = fmaf((float)(g->dim[k] - 1), g->spacing[k], g->origin[k]);
+    float inv = 1.0f / d[k];
+    float ta = (lo - o[k]) * inv, tb = (hi - o[k]) * inv;
+    float mn = fminf(ta, tb), mx = fmaxf(ta, tb);
+    t0 = fmaxf(t0, mn);
+    t1 = fminf(t1, mx);
+  }
+  uint32_t steps = 0, status = 0;
+  float p[3] = {0, 0, 0};
+  if (t0 < t1) {
+    float t = t0;
+    for (;;) {
+      for (int k = 0; k < 3; ++k) p[k] = fmaf(t, d[k], o[k]);
+      float v = o_voxel_sample(g, quality, p);
+      ++steps;
+      if (v < eps) {
+        status = 1;
+        break;
+      }
+      t = fmaf(step_factor, v, t);
+      if (t > t1) break;
+      if (steps >= max_steps) {
+        status = 2;
+        break;
+      }
+    }
+  }
+  memset(out, 0, sizeof(*out));
+  out->steps = steps;
+  out->status = status;
+  if (status == 1) {
+    float s01 = g->spacing[1] < g->spacing[2] ? g->spacing[1] : g->spacing[2];
+    float delta = 0.5f * (g->spacing[0] < s01 ? g->spacing[0] : s01);
+    float n[3];
+    for (int k = 0; k < 3; ++k) {
+      float a[3] = {p[0], p[1], p[2]}, b[3] = {p[0], p[1], p[2]};
+      a[k] = p[k] + delta;
+      b[k] = p[k] - delta;
+      n[k] = o_voxel_sample(g, quality, a) - o_voxel_sample(g, quality, b);
+    }
+    normalize3(n);
+    for (int k = 0; k < 3; ++k) {
+      out->pos[k] = p[k];
+      out->normal[k] = n[k];
+    }
+  }
+}

@@ -148,6 +148,16 @@ uint32_t o_frame_pixel(const float* tris, int32_t n, const float bmin[3], const 
                        int mode, const float* light_pos, const float* light_int,
                        uint32_t num_lights, const float albedo[3], const float zenith[3],
                        const float horizon[3]);
+/* --- voxel SDF (grid lookups, voxel sphere tracer) --------------------- */
+typedef struct {
+  const float* v;   /* 2 floats per voxel {distance, material}, x fastest */
+  int dim[3];
+  float spacing[3], origin[3];
+} o_voxel;
+float o_voxel_sample(const o_voxel* g, uint32_t quality, const float p[3]);
+void o_voxel_trace_pixel(const o_voxel* g, uint32_t quality, float step_factor, float eps,
+                         float tmax, uint32_t max_steps, const o_camera_basis* cb, uint32_t w,
+                         uint32_t h, uint32_t pix, o_sdf_hit* out);
 #ifdef __cplusplus
 }
 #endif

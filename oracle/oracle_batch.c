@@ -271,3 +271,36 @@ void o_batch_frame(const float* tris, int32_t n, const float bmin[3], const floa
                            num_lights, albedo, zenith, horizon);
   }
 }
+
+void o_batch_voxel_sample(const o_voxel* g, uint32_t quality, const float* pts, int64_t n,
+                          float* out, int threads) {
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < n; ++i) out[i] = o_voxel_sample(g, quality, pts + 3 * i);
+}
+
+void o_batch_voxel_trace(const o_voxel* g, uint32_t quality, float step_factor, float eps,
+                         float tmax, uint32_t max_steps, const o_camera* cam, uint32_t w,
+                         uint32_t h, const uint32_t* pixels, int64_t npix, o_sdf_hit* out,
+                         int threads) {
+  o_camera_basis b;
+  o_camera_setup(cam, &b);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < npix; ++i)
+    o_voxel_trace_pixel(g, quality, step_factor, eps, tmax, max_steps, &b, w, h,
+                        pixels ? pixels[i] : (uint32_t)i, &out[i]);
+}
+
+/* FP32 density at grid points origin + (i, j, k) * spacing (the bake). */
+void o_batch_voxel_bake(const uint32_t perm[512], int octaves, float scale, float amp,
+                        const int dim[3], const float spacing[3], const float origin[3],
+                        float* out, int threads) {
+  int64_t n = (int64_t)dim[0] * dim[1] * dim[2];
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < n; ++i) {
+    int x = (int)(i % dim[0]), y = (int)((i / dim[0]) % dim[1]), z = (int)(i / ((int64_t)dim[0] * dim[1]));
+    float p[3] = {fmaf((float)x, spacing[0], origin[0]), fmaf((float)y, spacing[1], origin[1]),
+                  fmaf((float)z, spacing[2], origin[2])};
+    out[2 * i] = o_terrain_density(perm, p, octaves, scale, amp);
+    out[2 * i + 1] = 0.0f;
+  }
+}

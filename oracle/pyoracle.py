@@ -456,3 +456,56 @@ def ref_ply_load(path):
     lib_.ref_ply_free(v)
     lib_.ref_ply_free(f)
     return bool(ok), verts.reshape(-1, 3), faces.reshape(-1, 3)
+
+
+class OVoxel(ctypes.Structure):
+    _fields_ = [("v", ctypes.c_void_p), ("dim", ctypes.c_int * 3), ("spacing", ctypes.c_float * 3),
+                ("origin", ctypes.c_float * 3)]
+
+
+def _ovoxel(grid, dim, spacing, origin):
+    g = OVoxel()
+    g.v = grid.ctypes.data
+    g.dim[:] = [int(x) for x in dim]
+    g.spacing[:] = [float(x) for x in spacing]
+    g.origin[:] = [float(x) for x in origin]
+    return g
+
+
+def voxel_bake(p, octaves, scale, amp, dim, spacing, origin, nthreads=0):
+    """(2 * voxels) float32: FP32 density at the grid points, material 0."""
+    n = int(dim[0]) * int(dim[1]) * int(dim[2])
+    out = np.zeros(2 * n, np.float32)
+    d = np.ascontiguousarray(dim, np.int32)
+    s = np.ascontiguousarray(spacing, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    lib().o_batch_voxel_bake(_p(p), ctypes.c_int(octaves), ctypes.c_float(scale),
+                             ctypes.c_float(amp), _p(d), _p(s), _p(o), _p(out),
+                             ctypes.c_int(nthreads))
+    return out
+
+
+def voxel_sample(grid, dim, spacing, origin, quality, pts, nthreads=0):
+    grid = np.ascontiguousarray(grid, np.float32)
+    pts = np.ascontiguousarray(pts, np.float32)
+    out = np.zeros(pts.shape[0], np.float32)
+    g = _ovoxel(grid, dim, spacing, origin)
+    lib().o_batch_voxel_sample(ctypes.byref(g), ctypes.c_uint32(quality), _p(pts),
+                               ctypes.c_int64(pts.shape[0]), _p(out), ctypes.c_int(nthreads))
+    return out
+
+
+def voxel_trace(grid, dim, spacing, origin, quality, step_factor, eps, tmax, max_steps, cam, w,
+                h, pixels=None, nthreads=0):
+    """Records like sdf_image: pos, normal, steps, status."""
+    grid = np.ascontiguousarray(grid, np.float32)
+    g = _ovoxel(grid, dim, spacing, origin)
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, SDF_DTYPE)
+    oc = camera(cam)
+    lib().o_batch_voxel_trace(ctypes.byref(g), ctypes.c_uint32(quality), ctypes.c_float(step_factor),
+                              ctypes.c_float(eps), ctypes.c_float(tmax), ctypes.c_uint32(max_steps),
+                              ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h), _p(pix),
+                              ctypes.c_int64(n), _p(out), ctypes.c_int(nthreads))
+    return out

@@ -146,6 +146,11 @@ class re_nsdf_trace_params(ctypes.Structure):
 NSDF_EXACT_ONLY = 1
 
 
+class re_voxel_grid(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_uint32 * 3), ("spacing", ctypes.c_float * 3),
+                ("origin", ctypes.c_float * 3)]
+
+
 class re_light(ctypes.Structure):
     _fields_ = [("pos", ctypes.c_float * 3), ("intensity", ctypes.c_float)]
 
@@ -228,6 +233,11 @@ _SIGS = {
     "re_nsdf_trace_network": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_exact": (ctypes.c_int, [_P, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_nsdf_trace_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_nsdf_trace_status": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_int), _P]),
+    "re_voxel_bake": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_voxel_grid), _P, _P]),
+    "re_voxel_sample": (ctypes.c_int, [_P, ctypes.POINTER(re_voxel_grid), _U32, _P, _U32, _P, _P]),
+    "re_voxel_trace": (ctypes.c_int, [_P, ctypes.POINTER(re_voxel_grid), _U32, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_voxel_save": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(re_voxel_grid), _P]),
+    "re_voxel_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(re_voxel_grid), _P, ctypes.c_uint64]),
     "re_mesh_load": (ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(ctypes.c_void_p)]),
     "re_mesh_info": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "re_mesh_copy": (ctypes.c_int, [_P, _P, _P]),

@@ -668,3 +668,63 @@ def load_mesh(path: str, first_triangle_only: bool = False):
     finally:
         lib.re_mesh_destroy(h)
     return verts, faces
+
+
+# -------------------------------------------------------------- voxel SDF
+VOXEL_LOW, VOXEL_MEDIUM, VOXEL_HIGH = 0, 1, 2
+
+
+class VoxelGrid:
+    """A voxel SDF on the device: 2 floats {distance, material} per voxel."""
+
+    def __init__(self, dim, spacing, origin=(0.0, 0.0, 0.0), data=None):
+        import torch
+
+        self.desc = _lib.re_voxel_grid()
+        self.desc.dim[:] = [int(x) for x in dim]
+        self.desc.spacing[:] = [float(x) for x in spacing]
+        self.desc.origin[:] = [float(x) for x in origin]
+        n = int(dim[0]) * int(dim[1]) * int(dim[2])
+        if data is None:
+            self.data = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
+        else:
+            self.data = torch.as_tensor(np.ascontiguousarray(data, np.float32).reshape(-1)).cuda()
+
+    @classmethod
+    def bake(cls, field, dim, spacing, origin=(0.0, 0.0, 0.0), stream=None):
+        g = cls(dim, spacing, origin)
+        call("re_voxel_bake", ctypes.byref(field), ctypes.byref(g.desc), _dptr(g.data),
+             _stream_ptr(stream))
+        return g
+
+    @classmethod
+    def load(cls, path: str, origin=(0.0, 0.0, 0.0)):
+        d = _lib.re_voxel_grid()
+        call("re_voxel_load", str(path).encode(), ctypes.byref(d), None, 0)
+        n = d.dim[0] * d.dim[1] * d.dim[2]
+        host = np.empty(2 * n, np.float32)
+        call("re_voxel_load", str(path).encode(), ctypes.byref(d), host.ctypes.data, n)
+        return cls(list(d.dim), list(d.spacing), origin, host)
+
+    def save(self, path: str):
+        host = np.ascontiguousarray(self.data.cpu().numpy())
+        call("re_voxel_save", str(path).encode(), ctypes.byref(self.desc), host.ctypes.data)
+
+    def sample(self, pts, quality, out=None, stream=None):
+        import torch
+
+        n = pts.shape[0]
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device="cuda")
+        call("re_voxel_sample", _dptr(self.data), ctypes.byref(self.desc), quality, _dptr(pts), n,
+             _dptr(out), _stream_ptr(stream))
+        return out
+
+    def trace(self, quality, march, cam, w, h, out=None, stream=None):
+        import torch
+
+        if out is None:
+            out = torch.empty((h * w, 8), dtype=torch.int32, device="cuda")
+        call("re_voxel_trace", _dptr(self.data), ctypes.byref(self.desc), quality,
+             ctypes.byref(march), ctypes.byref(cam), w, h, _dptr(out), _stream_ptr(stream))
+        return out

@@ -386,6 +386,25 @@ RE_API re_status re_nsdf_trace_status(re_nsdf* s, uint32_t* num_refined,
 RE_API re_status re_nsdf_save(const re_nsdf* s, const char* path);
 RE_API re_status re_nsdf_load(re_nsdf* s, const char* path);
 
+/* ---- instanced scenes --------------------------------------------------
+ * Replaces the reference's per-object ray transform and closest-hit loop
+ * (ray_functions.cuh:236-267,377-396; objects in RTScene.cpp:40-62): each
+ * instance is a built scene seen through a yaw rotation and a location,
+ * object-space ray d' = normalize(Ry d), o' = Ry o + location. */
+typedef struct re_instance {
+  const re_scene* mesh;
+  float yaw;              /* radians, about +y                              */
+  float location[3];
+} re_instance;
+/* Primary rays against all instances: re_hit per pixel and the index of
+ * the instance hit (-1 for none); one-sided with RE_TRACE_ONE_SIDED. */
+RE_API re_status re_trace_instances(const re_instance* instances, uint32_t n,
+                                    const re_camera* cam, uint32_t w, uint32_t h,
+                                    uint32_t flags, re_hit* d_out, int32_t* d_instance,
+                                    void* stream);
+/* cos and sin of a yaw exactly as re_trace_instances computes them. */
+RE_API void re_instance_trig(float yaw, float* c, float* s);
+
 /* ---- voxel SDF ----------------------------------------------------------
  * Replaces the reference's voxel-SDF path: the bake kernel generate_noise
  * (renderer.cu:106-126), the .rsdf file (Grid.cpp:23-64, save_map
@@ -414,6 +433,22 @@ RE_API re_status re_voxel_trace(const float* d_grid, const re_voxel_grid* g,
                                 uint32_t quality, const re_sdf_params* march,
                                 const re_camera* cam, uint32_t w, uint32_t h,
                                 re_sdf_hit* d_out, void* stream);
+/* Brush edits of a grid (insert_sphere_to_texture, renderer.cu:31-92) at a
+ * world-space centre: sphere add (smooth union with k = smooth, the
+ * reference uses 0.1) / subtract, cube add / subtract (half-extents). */
+#define RE_BRUSH_SPHERE_ADD 0u
+#define RE_BRUSH_SPHERE_SUBTRACT 1u
+#define RE_BRUSH_CUBE_ADD 2u
+#define RE_BRUSH_CUBE_SUBTRACT 3u
+typedef struct re_voxel_brush_params {
+  uint32_t type;
+  float center[3];
+  float extent[3];        /* sphere: radius in extent[0]                    */
+  float material;
+  float smooth;
+} re_voxel_brush_params;
+RE_API re_status re_voxel_brush(float* d_grid, const re_voxel_grid* g,
+                                const re_voxel_brush_params* b, void* stream);
 /* .rsdf files: int32 dim[3], float spacing[3], {distance, material} per
  * voxel, x fastest.  re_voxel_load fills g (origin 0) and, when host_grid
  * is not NULL, up to capacity_voxels voxels. */

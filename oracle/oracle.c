@@ -1005,3 +1005,73 @@ void o_voxel_trace_pixel(const o_voxel* g, uint32_t quality, float step_factor, 
     }
   }
 }
+
+/* ------------------------------------------------------------ instances */
+/* Closest hit over instances (object-space ray d' = normalize(Ry d),
+ * o' = Ry o + location), brute force per instance; c, s = cos / sin of
+ * each yaw as the library computes them. */
+void o_trace_instances_pixel(const float* const* tris, const int32_t* ntris, const float* bmin,
+                             const float* bmax, const float* cs, const float* loc, int32_t n,
+                             const float o[3], const float d[3], int mode, o_hit* out,
+                             int32_t* inst) {
+  out->id = -1;
+  out->t = K_INFINITY;
+  out->u = out->v = 0.0f;
+  *inst = -1;
+  float best = INFINITY;
+  for (int32_t k = 0; k < n; ++k) {
+    float c = cs[2 * k], s = cs[2 * k + 1];
+    float nd[3] = {d[0] * c + d[2] * s, d[1], -d[0] * s + d[2] * c};
+    normalize3(nd);
+    float no[3] = {o[0] * c + o[2] * s + loc[3 * k], o[1] + loc[3 * k + 1],
+                   -o[0] * s + o[2] * c + loc[3 * k + 2]};
+    o_hit h;
+    o_trace_bruteforce(tris[k], ntris[k], bmin + 3 * k, bmax + 3 * k, no, nd, mode, &h);
+    if (h.id >= 0 && h.t < best) {
+      best = h.t;
+      *out = h;
+      *inst = k;
+    }
+  }
+}
+
+/* ---------------------------------------------------------- voxel brush */
+static float len3f(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+
+void o_voxel_brush(float* v, const int dim[3], const float spacing[3], const float origin[3],
+                   uint32_t type, const float c[3], const float e[3], float mat, float k) {
+  int64_t n = (int64_t)dim[0] * dim[1] * dim[2];
+  for (int64_t i = 0; i < n; ++i) {
+    int x = (int)(i % dim[0]), y = (int)((i / dim[0]) % dim[1]), z = (int)(i / ((int64_t)dim[0] * dim[1]));
+    float qx = fmaf((float)x, spacing[0], origin[0]) - c[0];
+    float qy = fmaf((float)y, spacing[1], origin[1]) - c[1];
+    float qz = fmaf((float)z, spacing[2], origin[2]) - c[2];
+    float ax = v[2 * i], ay = v[2 * i + 1], rx = ax, ry = ay;
+    if (type <= 1) {
+      float sd = len3f(qx, qy, qz) - e[0];
+      if (type == 0) {
+        float h = fmaxf(k - fabsf(ax - sd), 0.0f) / k;
+        float mx = ax < sd ? ax : sd, my = ax < sd ? ay : mat;
+        float cc = h * h * k * 0.25f;
+        rx = mx - cc;
+        ry = my;
+      } else if (!(ax > -sd)) {
+        rx = -sd;
+        ry = mat;
+      }
+    } else {
+      float dx = fabsf(qx) - e[0], dy = fabsf(qy) - e[1], dz = fabsf(qz) - e[2];
+      float bd = len3f(fmaxf(dx, 0.0f), fmaxf(dy, 0.0f), fmaxf(dz, 0.0f)) +
+                 fminf(fmaxf(dx, fmaxf(dy, dz)), 0.0f);
+      if (type == 2) {
+        rx = fminf(ax, bd);
+        ry = fminf(ay, mat);
+      } else if (!(ax > -bd)) {
+        rx = -bd;
+        ry = mat;
+      }
+    }
+    v[2 * i] = rx;
+    v[2 * i + 1] = ry;
+  }
+}

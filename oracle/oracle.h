@@ -158,6 +158,13 @@ float o_voxel_sample(const o_voxel* g, uint32_t quality, const float p[3]);
 void o_voxel_trace_pixel(const o_voxel* g, uint32_t quality, float step_factor, float eps,
                          float tmax, uint32_t max_steps, const o_camera_basis* cb, uint32_t w,
                          uint32_t h, uint32_t pix, o_sdf_hit* out);
+/* --- instances and voxel brush ------------------------------------------ */
+void o_trace_instances_pixel(const float* const* tris, const int32_t* ntris, const float* bmin,
+                             const float* bmax, const float* cs, const float* loc, int32_t n,
+                             const float o[3], const float d[3], int mode, o_hit* out,
+                             int32_t* inst);
+void o_voxel_brush(float* v, const int dim[3], const float spacing[3], const float origin[3],
+                   uint32_t type, const float c[3], const float e[3], float mat, float k);
 #ifdef __cplusplus
 }
 #endif

@@ -304,3 +304,17 @@ void o_batch_voxel_bake(const uint32_t perm[512], int octaves, float scale, floa
     out[2 * i + 1] = 0.0f;
   }
 }
+
+void o_batch_instances(const float* const* tris, const int32_t* ntris, const float* bmin,
+                       const float* bmax, const float* cs, const float* loc, int32_t n,
+                       const o_camera* cam, uint32_t w, uint32_t h, int mode, o_hit* out,
+                       int32_t* inst, int threads) {
+  o_camera_basis b;
+  o_camera_setup(cam, &b);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < (int64_t)w * h; ++i) {
+    float o[3], d[3];
+    o_generate_ray(&b, w, h, (uint32_t)(i % w), (uint32_t)(i / w), o, d);
+    o_trace_instances_pixel(tris, ntris, bmin, bmax, cs, loc, n, o, d, mode, &out[i], &inst[i]);
+  }
+}

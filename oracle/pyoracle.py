@@ -509,3 +509,35 @@ def voxel_trace(grid, dim, spacing, origin, quality, step_factor, eps, tmax, max
                               ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h), _p(pix),
                               ctypes.c_int64(n), _p(out), ctypes.c_int(nthreads))
     return out
+
+
+def trace_instances(instances, cam, w, h, mode=0, nthreads=0):
+    """instances: [(packed (n,12), bmin, bmax, (cos, sin), location)] ->
+    (hits HIT_DTYPE (w*h,), instance index (w*h,))."""
+    n = len(instances)
+    keep = [np.ascontiguousarray(x[0], np.float32) for x in instances]
+    ptrs = (ctypes.c_void_p * n)(*[k.ctypes.data for k in keep])
+    nt = np.array([k.shape[0] for k in keep], np.int32)
+    bmin = np.ascontiguousarray([x[1] for x in instances], np.float32)
+    bmax = np.ascontiguousarray([x[2] for x in instances], np.float32)
+    cs = np.ascontiguousarray([x[3] for x in instances], np.float32)
+    loc = np.ascontiguousarray([x[4] for x in instances], np.float32)
+    out = np.zeros(w * h, HIT_DTYPE)
+    inst = np.zeros(w * h, np.int32)
+    oc = camera(cam)
+    lib().o_batch_instances(ptrs, _p(nt), _p(bmin), _p(bmax), _p(cs), _p(loc), ctypes.c_int32(n),
+                            ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                            ctypes.c_int(mode), _p(out), _p(inst), ctypes.c_int(nthreads))
+    return out, inst
+
+
+def voxel_brush(grid, dim, spacing, origin, kind, center, extent, material=0.0, smooth=0.1):
+    g = np.ascontiguousarray(grid, np.float32).copy()
+    d = np.ascontiguousarray(dim, np.int32)
+    s = np.ascontiguousarray(spacing, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    c = np.ascontiguousarray(center, np.float32)
+    e = np.ascontiguousarray(extent if hasattr(extent, "__len__") else [extent] * 3, np.float32)
+    lib().o_voxel_brush(_p(g), _p(d), _p(s), _p(o), ctypes.c_uint32(kind), _p(c), _p(e),
+                        ctypes.c_float(material), ctypes.c_float(smooth))
+    return g

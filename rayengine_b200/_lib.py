@@ -151,6 +151,17 @@ class re_voxel_grid(ctypes.Structure):
                 ("origin", ctypes.c_float * 3)]
 
 
+class re_instance(ctypes.Structure):
+    _fields_ = [("mesh", ctypes.c_void_p), ("yaw", ctypes.c_float),
+                ("location", ctypes.c_float * 3)]
+
+
+class re_voxel_brush_params(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_uint32), ("center", ctypes.c_float * 3),
+                ("extent", ctypes.c_float * 3), ("material", ctypes.c_float),
+                ("smooth", ctypes.c_float)]
+
+
 class re_light(ctypes.Structure):
     _fields_ = [("pos", ctypes.c_float * 3), ("intensity", ctypes.c_float)]
 
@@ -238,6 +249,9 @@ _SIGS = {
     "re_voxel_trace": (ctypes.c_int, [_P, ctypes.POINTER(re_voxel_grid), _U32, ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
     "re_voxel_save": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(re_voxel_grid), _P]),
     "re_voxel_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(re_voxel_grid), _P, ctypes.c_uint64]),
+    "re_voxel_brush": (ctypes.c_int, [_P, ctypes.POINTER(re_voxel_grid), ctypes.POINTER(re_voxel_brush_params), _P]),
+    "re_trace_instances": (ctypes.c_int, [ctypes.POINTER(re_instance), _U32, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P, _P]),
+    "re_instance_trig": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
     "re_mesh_load": (ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(ctypes.c_void_p)]),
     "re_mesh_info": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "re_mesh_copy": (ctypes.c_int, [_P, _P, _P]),

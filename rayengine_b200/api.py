@@ -672,6 +672,7 @@ def load_mesh(path: str, first_triangle_only: bool = False):
 
 # -------------------------------------------------------------- voxel SDF
 VOXEL_LOW, VOXEL_MEDIUM, VOXEL_HIGH = 0, 1, 2
+BRUSH_SPHERE_ADD, BRUSH_SPHERE_SUBTRACT, BRUSH_CUBE_ADD, BRUSH_CUBE_SUBTRACT = 0, 1, 2, 3
 
 
 class VoxelGrid:
@@ -720,6 +721,17 @@ class VoxelGrid:
              _dptr(out), _stream_ptr(stream))
         return out
 
+    def brush(self, kind, center, extent, material=0.0, smooth=0.1, stream=None):
+        """Edit every voxel: kind in BRUSH_SPHERE_ADD / _SUBTRACT, BRUSH_CUBE_ADD / _SUBTRACT."""
+        b = _lib.re_voxel_brush_params()
+        b.type = kind
+        b.center[:] = [float(x) for x in center]
+        ext = list(extent) if hasattr(extent, "__len__") else [extent, extent, extent]
+        b.extent[:] = [float(x) for x in ext]
+        b.material, b.smooth = float(material), float(smooth)
+        call("re_voxel_brush", _dptr(self.data), ctypes.byref(self.desc), ctypes.byref(b),
+             _stream_ptr(stream))
+
     def trace(self, quality, march, cam, w, h, out=None, stream=None):
         import torch
 
@@ -728,3 +740,28 @@ class VoxelGrid:
         call("re_voxel_trace", _dptr(self.data), ctypes.byref(self.desc), quality,
              ctypes.byref(march), ctypes.byref(cam), w, h, _dptr(out), _stream_ptr(stream))
         return out
+
+
+# ------------------------------------------------------------ instances
+def instance_trig(yaw: float):
+    """(cos, sin) of a yaw as the instanced tracer computes them."""
+    c, s_ = ctypes.c_float(), ctypes.c_float()
+    lib.re_instance_trig(ctypes.c_float(yaw), ctypes.byref(c), ctypes.byref(s_))
+    return c.value, s_.value
+
+
+def trace_instances(instances, cam, w, h, flags=TRACE_TWO_SIDED, stream=None):
+    """instances: [(KDScene, yaw, location xyz)] -> (re_hit (h*w, 4) int32,
+    instance index (h*w,) int32) CUDA tensors."""
+    import torch
+
+    arr = (_lib.re_instance * len(instances))()
+    for i, (sc, yaw, loc) in enumerate(instances):
+        arr[i].mesh = sc._h.value
+        arr[i].yaw = float(yaw)
+        arr[i].location[:] = [float(x) for x in loc]
+    out = torch.empty((h * w, 4), dtype=torch.int32, device="cuda")
+    idx = torch.empty(h * w, dtype=torch.int32, device="cuda")
+    call("re_trace_instances", arr, len(instances), ctypes.byref(cam), w, h, flags, _dptr(out),
+         _dptr(idx), _stream_ptr(stream))
+    return out, idx

@@ -181,6 +181,46 @@ __global__ void __launch_bounds__(256) k_trace(GridDev g, uint32_t quality, Marc
   out[2 * (size_t)pix + 1] = r1;
 }
 
+// Brush edit of every voxel (insert_sphere_to_texture, renderer.cu:31-92):
+// q = voxel position - centre; SPHERE_ADD smooth union (sdf_smin, k),
+// SPHERE_SUBTRACT max(v, -sphere), CUBE_ADD component-wise min of the
+// {distance, material} pairs (as the reference's fminf on float2),
+// CUBE_SUBTRACT max(v, -box); sphere = |q| - r, box as aabb_distance
+// (sdf_functions.cuh:424-436).
+__device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+
+__global__ void k_brush(GridDev g, uint32_t type, float cx, float cy, float cz, float ex, float ey,
+                        float ez, float mat, float k, float2* __restrict__ v) {
+  size_t n = (size_t)g.dim[0] * g.dim[1] * g.dim[2];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t x = (uint32_t)(i % g.dim[0]), y = (uint32_t)((i / g.dim[0]) % g.dim[1]),
+             z = (uint32_t)(i / ((size_t)g.dim[0] * g.dim[1]));
+    float qx = __fmaf_rn((float)x, g.spacing[0], g.origin[0]) - cx;
+    float qy = __fmaf_rn((float)y, g.spacing[1], g.origin[1]) - cy;
+    float qz = __fmaf_rn((float)z, g.spacing[2], g.origin[2]) - cz;
+    float2 a = v[i], r = a;
+    if (type == RE_BRUSH_SPHERE_ADD || type == RE_BRUSH_SPHERE_SUBTRACT) {
+      float sd = len3(qx, qy, qz) - ex;
+      if (type == RE_BRUSH_SPHERE_ADD) {
+        float h = fmaxf(k - fabsf(a.x - sd), 0.0f) / k;
+        float2 m = a.x < sd ? a : make_float2(sd, mat);
+        float c = h * h * k * 0.25f;
+        r = make_float2(m.x - c, m.y);
+      } else {
+        r = a.x > -sd ? a : make_float2(-sd, mat);
+      }
+    } else {
+      float dx = fabsf(qx) - ex, dy = fabsf(qy) - ey, dz = fabsf(qz) - ez;
+      float bd = len3(fmaxf(dx, 0.0f), fmaxf(dy, 0.0f), fmaxf(dz, 0.0f)) +
+                 fminf(fmaxf(dx, fmaxf(dy, dz)), 0.0f);
+      if (type == RE_BRUSH_CUBE_ADD) r = make_float2(fminf(a.x, bd), fminf(a.y, mat));
+      else r = a.x > -bd ? a : make_float2(-bd, mat);
+    }
+    v[i] = r;
+  }
+}
+
 }  // namespace voxel
 }  // namespace re
 
@@ -273,6 +313,20 @@ RE_API re_status re_voxel_trace(const float* d_grid, const re_voxel_grid* g, uin
       re::grid_dev(g, d_grid), quality, m, re::cam_of_voxel(*cam), w, h,
       reinterpret_cast<float4*>(d_out));
   RE_CHECK_LAUNCH("re_voxel_trace: launch");
+  return RE_OK;
+}
+
+RE_API re_status re_voxel_brush(float* d_grid, const re_voxel_grid* g, const re_voxel_brush_params* b,
+                                void* stream) {
+  re_status st = re::check_grid(g, "re_voxel_brush");
+  if (st != RE_OK) return st;
+  if (!d_grid || !b || b->type > RE_BRUSH_CUBE_SUBTRACT ||
+      (b->type == RE_BRUSH_SPHERE_ADD && !(b->smooth > 0.f)))
+    return re::fail(RE_ERR_INVALID_ARG, "re_voxel_brush: bad arguments");
+  re::voxel::k_brush<<<4 * re::sm_count(), 256, 0, (cudaStream_t)stream>>>(
+      re::grid_dev(g, d_grid), b->type, b->center[0], b->center[1], b->center[2], b->extent[0],
+      b->extent[1], b->extent[2], b->material, b->smooth, reinterpret_cast<float2*>(d_grid));
+  RE_CHECK_LAUNCH("re_voxel_brush: launch");
   return RE_OK;
 }
 

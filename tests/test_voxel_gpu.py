@@ -57,3 +57,19 @@ def test_voxel_trace_matches_oracle_and_file_round_trip(cuda, tmp_path):
     a = g.trace(rb.VOXEL_MEDIUM, march, cam, w, h).cpu().numpy()
     b = g2.trace(rb.VOXEL_MEDIUM, march, cam, w, h).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def test_brush_edits_match_oracle(cuda):
+    tc, g = _grid()
+    grid = g.data.cpu().numpy()
+    edits = [(rb.BRUSH_SPHERE_ADD, (0.0, 1.0, 4.0), 2.0, 3.0),
+             (rb.BRUSH_SPHERE_SUBTRACT, (2.0, -0.5, 6.0), 1.5, 4.0),
+             (rb.BRUSH_CUBE_ADD, (-4.0, 0.5, 8.0), (1.0, 2.0, 1.5), 5.0),
+             (rb.BRUSH_CUBE_SUBTRACT, (3.0, 0.0, 2.0), (2.0, 1.0, 1.0), 6.0)]
+    for kind, c, e, mat in edits:
+        g.brush(kind, c, e, material=mat, smooth=0.1)
+        grid = po.voxel_brush(grid, DIM, SP, ORG, kind, c, e, mat, 0.1)
+        assert np.array_equal(g.data.cpu().numpy(), grid), kind
+    # the edits changed the field
+    assert not np.array_equal(grid, po.voxel_bake(po.perm(tc.seed), tc.octaves, tc.scale,
+                                                  tc.amplitude, DIM, SP, ORG))

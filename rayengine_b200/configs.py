@@ -187,10 +187,27 @@ class BatchConfig:
                                 albedo=albedo))
         return out
 
-    def build(self):
-        """(Batch, [KDScene]) on the current device."""
+    @staticmethod
+    def shard(specs, rank: int, world: int):
+        """This rank's scenes when a batch is split across `world` GPUs:
+        largest scenes first, each to the rank with the fewest pixels so
+        far (ties to the lower rank); deterministic on every rank."""
+        load = [0] * world
+        owner = {}
+        order = sorted(range(len(specs)),
+                       key=lambda i: (-specs[i]["width"] * specs[i]["height"], i))
+        for i in order:
+            r = min(range(world), key=lambda k: (load[k], k))
+            owner[i] = r
+            load[r] += specs[i]["width"] * specs[i]["height"]
+        return [specs[i] for i in range(len(specs)) if owner[i] == rank]
+
+    def build(self, rank: int = 0, world: int = 1):
+        """(Batch, [KDScene]) on the current device: all scenes, or this
+        rank's shard when world > 1."""
         scenes, meshes = [], []
-        for s in self.specs():
+        specs = self.specs() if world <= 1 else self.shard(self.specs(), rank, world)
+        for s in specs:
             w, h = s["width"], s["height"]
             if s["kind"] == "soup":
                 sc = SoupConfig(num_tris=s["num_tris"], seed=s["seed"], width=w, height=h)

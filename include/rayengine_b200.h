@@ -539,7 +539,8 @@ typedef struct re_batch_tuning {
   uint32_t block_threads; /* 32..512, multiple of 32 (256)                  */
   uint32_t refill_min;    /* idle lanes a warp waits for before claiming    */
   uint32_t stage_nodes;   /* top nodes per mesh scene in shared memory      */
-  uint32_t reserved;
+  uint32_t steps_per_trip;/* leaves / field evaluations a lane advances     */
+                          /* between the warp's refills (0 = 1; 8)          */
 } re_batch_tuning;
 
 RE_API re_status re_batch_create(const re_batch_scene* scenes, uint32_t num_scenes,
@@ -569,7 +570,7 @@ RE_API re_status re_batch_counts(re_batch* b, float* d_radiance, void* stream,
 RE_API re_status re_batch_get_tuning(const re_batch* b, re_batch_tuning* out);
 RE_API re_status re_batch_set_tuning(re_batch* b, const re_batch_tuning* t);
 /* Times one frame per candidate (block size x refill threshold x staged
- * nodes) and keeps the fastest. */
+ * nodes x steps per trip) and keeps the fastest. */
 RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
                                    re_batch_tuning* out, float* best_ms);
 

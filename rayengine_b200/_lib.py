@@ -190,7 +190,7 @@ class re_path_params(ctypes.Structure):
 
 class re_batch_tuning(ctypes.Structure):
     _fields_ = [("block_threads", ctypes.c_uint32), ("refill_min", ctypes.c_uint32),
-                ("stage_nodes", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("stage_nodes", ctypes.c_uint32), ("steps_per_trip", ctypes.c_uint32)]
 
 
 BATCH_MESH, BATCH_TERRAIN = 0, 1

@@ -600,10 +600,10 @@ class Batch:
         t = _lib.re_batch_tuning()
         call("re_batch_get_tuning", self._h, ctypes.byref(t))
         return {"block_threads": t.block_threads, "refill_min": t.refill_min,
-                "stage_nodes": t.stage_nodes}
+                "stage_nodes": t.stage_nodes, "steps_per_trip": t.steps_per_trip}
 
-    def set_tuning(self, block_threads, refill_min, stage_nodes):
-        t = _lib.re_batch_tuning(block_threads, refill_min, stage_nodes, 0)
+    def set_tuning(self, block_threads, refill_min, stage_nodes, steps_per_trip=8):
+        t = _lib.re_batch_tuning(block_threads, refill_min, stage_nodes, steps_per_trip)
         call("re_batch_set_tuning", self._h, ctypes.byref(t))
 
     def autotune(self, out=None, stream=None) -> dict:
@@ -616,7 +616,8 @@ class Batch:
         call("re_batch_autotune", self._h, _dptr(out), _stream_ptr(stream), ctypes.byref(t),
              ctypes.byref(ms))
         return {"block_threads": t.block_threads, "refill_min": t.refill_min,
-                "stage_nodes": t.stage_nodes, "frame_ms": round(ms.value, 4)}
+                "stage_nodes": t.stage_nodes, "steps_per_trip": t.steps_per_trip,
+                "frame_ms": round(ms.value, 4)}
 
 
 # ------------------------------------------------------------ shaded frame

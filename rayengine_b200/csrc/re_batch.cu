@@ -56,25 +56,30 @@ constexpr uint32_t kMaxDepth = 8;
 constexpr uint32_t kMaxQueues = 2 * (kMaxDepth - 1);
 constexpr uint32_t kMesh = RE_BATCH_MESH, kTerrain = RE_BATCH_TERRAIN;
 
-// counters (uint32): cursor, created, finished, epoch, blocks done, error,
-// then reserved[q] at kReserved + q and claimed[q] at kClaimed + q; the last
-// frame's per-queue ray counts are copied to kStats + q before the reset.
+// Counters (uint32), each contended one on its own 128-byte line so that
+// atomics on different counters do not queue behind each other in one L2
+// slice: the pixel cursor, finished rays per bounce, the frame epoch,
+// blocks done and the error flag, reserved[q] / claimed[q] per queue; then
+// (cold) the last frame's statistics.  Rays created of bounce 0 = pixels,
+// of bounce b = the reserved counts of bounce b's two queues.
+constexpr uint32_t kLine = 32;
 enum : uint32_t {
-  kCursor = 0,
-  kCreated = 1,
-  kFinished = 2,
-  kEpoch = 3,
-  kDone = 4,
-  kError = 5,
-  kPrimaryRays = 6,
-  kReserved = 8,
-  kClaimed = kReserved + kMaxQueues,
-  kStats = kClaimed + kMaxQueues,
+  kCursor = 0 * kLine,
+  kFin = 1 * kLine,  // + bounce * kLine: finished rays of that bounce
+  kEpoch = (1 + kMaxDepth) * kLine,
+  kDone = (2 + kMaxDepth) * kLine,
+  kError = (2 + kMaxDepth) * kLine + 1,
+  kReserved = (3 + kMaxDepth) * kLine,  // + q * kLine
+  kClaimed = kReserved + kMaxQueues * kLine,
+  kStats = kClaimed + kMaxQueues * kLine,  // + q
   kStatsPrimary = kStats + kMaxQueues,
   kStatsError = kStatsPrimary + 1,
-  kNumCounters = 64
+  kNumCounters = kStats + kLine
 };
 static_assert(kStatsError < kNumCounters, "counter layout");
+__host__ __device__ constexpr uint32_t fin_at(uint32_t b) { return kFin + b * kLine; }
+__host__ __device__ constexpr uint32_t reserved_at(uint32_t q) { return kReserved + q * kLine; }
+__host__ __device__ constexpr uint32_t claimed_at(uint32_t q) { return kClaimed + q * kLine; }
 
 struct __align__(16) SceneDev {
   const uint2* nodes;
@@ -84,6 +89,7 @@ struct __align__(16) SceneDev {
   uint32_t max_visits, stage, stage_off;
   uint32_t perm_slot, octaves, max_steps;
   float scale, amp, step_factor, eps, tmax;
+  float ceiling;  // terrain: no surface above this height (|fBm| bound)
   CamDev cam;
   uint32_t w, h, kind, pix_off;
   float albedo;
@@ -93,11 +99,12 @@ struct BatchDev {
   const SceneDev* scenes;
   const uint8_t* perms;  // perm_count tables of 512 bytes
   uint32_t num_scenes, perm_count, stage_total, total_pixels;
-  uint32_t depth, seed, refill_min;
+  uint32_t depth, seed, refill_min, steps_per_trip;
   float mesh_bias;
   float4* queue;        // records: 2 float4 per slot
   uint32_t* flags;      // one per slot
   uint64_t qoff[kMaxQueues];  // first slot of queue q
+  uint32_t qcap[kMaxQueues];  // slots of queue q (pixels of its kind)
   uint32_t* ctr;
   float* radiance;
   int4* primary;        // optional re_hit per pixel
@@ -116,22 +123,6 @@ __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
-}
-
-// Claim up to `want` reserved slots of queue q; returns the count (base in
-// `base`).  Never claims past the reserved count.
-__device__ __forceinline__ uint32_t claim(uint32_t* ctr, uint32_t q, uint32_t want, uint32_t& base) {
-  for (int tries = 0; tries < 4; ++tries) {
-    uint32_t c = ld_relaxed(&ctr[kClaimed + q]);
-    uint32_t r = ld_relaxed(&ctr[kReserved + q]);
-    if (c >= r) return 0u;
-    uint32_t k = min(want, r - c);
-    if (atomicCAS(&ctr[kClaimed + q], c, c + k) == c) {
-      base = c;
-      return k;
-    }
-  }
-  return 0u;
 }
 
 __device__ __forceinline__ uint32_t scene_of(const SceneDev* sc, uint32_t n, uint32_t gpix) {
@@ -188,7 +179,24 @@ __device__ __forceinline__ float miss_radiance(float albedo, uint32_t bounce, V3
 enum : uint32_t { kIdle = 0, kPending = 1, kLive = 2 };
 enum : uint32_t { kMarch = 0, kNormal = 1 };
 constexpr uint32_t kPendingBound = 1u << 22;  // polls of one slot flag
-constexpr uint32_t kLoopBound = 1u << 24;     // trips of the persistent loop
+constexpr uint32_t kLoopBound = 1u << 22;     // trips of the persistent loop
+
+// Bounce b's queues are closed (no ray of bounce b can still be created)
+// once the pixel cursor is exhausted and every ray of bounce b - 1 has
+// finished.  Bit b of the result, b = 1 .. depth; bit depth = the frame is
+// done.  Each bounce's created count is read only after its predecessor's
+// finished count compared equal (a control dependency orders the loads), so
+// it is final when read: its producers all finished first.
+__device__ __forceinline__ uint32_t closed_mask(const uint32_t* ctr, const BatchDev& B) {
+  uint32_t mask = 0, created = B.total_pixels;
+  for (uint32_t b = 1; b <= B.depth; ++b) {
+    if (ld_relaxed(&ctr[fin_at(b - 1)]) != created) break;
+    mask |= 1u << b;
+    if (b == B.depth) break;
+    created = ld_relaxed(&ctr[reserved_at(2 * (b - 1))]) + ld_relaxed(&ctr[reserved_at(2 * (b - 1) + 1)]);
+  }
+  return mask;
+}
 
 template <bool COUNT>
 __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
@@ -196,12 +204,14 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
   SceneDev* sc = reinterpret_cast<SceneDev*>(smem_u4);
   uint8_t* sperm = reinterpret_cast<uint8_t*>(sc + B.num_scenes);
   uint2* snodes = reinterpret_cast<uint2*>(sperm + 512u * B.perm_count);
+  uint32_t* sfin = reinterpret_cast<uint32_t*>(snodes + B.stage_total);  // [warp][bounce]
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(B.scenes);
     uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
     for (uint32_t i = threadIdx.x; i < B.num_scenes * (uint32_t)(sizeof(SceneDev) / 4); i += blockDim.x)
       dst[i] = src[i];
     for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) sperm[i] = B.perms[i];
+    for (uint32_t i = threadIdx.x; i < (blockDim.x / 32u) * kMaxDepth; i += blockDim.x) sfin[i] = 0u;
     __syncthreads();
     for (uint32_t s = 0; s < B.num_scenes; ++s)
       for (uint32_t i = threadIdx.x; i < sc[s].stage; i += blockDim.x)
@@ -213,6 +223,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t nq = 2u * (B.depth - 1u);
+  uint32_t* wfin = sfin + (threadIdx.x >> 5) * kMaxDepth;  // this warp's unpublished counts
 
   uint32_t state = kIdle, pq = 0, pslot = 0, polls = 0;
   uint32_t gpix = 0, scene = 0, bounce = 0, kind = kMesh;
@@ -224,12 +235,39 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
   V3 p = {0.f, 0.f, 0.f};
   Counters cnt = {0, 0, 0, 0};
   uint32_t errors = 0;
+  uint32_t fin_pending = 0;   // lane 0: finished rays in wfin
+  uint32_t backoff = 32;      // lane 0: idle sleep, ns
+  bool primary_done = false;  // lane 0: the pixel cursor has passed the end
+
+  // publishes this warp's finished counts (after its reservations, which
+  // completed when their atomics returned)
+  auto flush = [&]() {
+    __syncwarp();
+    if (lane == 0 && fin_pending) {
+      __threadfence();
+      for (uint32_t b = 0; b < B.depth; ++b) {
+        uint32_t v = wfin[b];
+        if (v) {
+          atomicAdd(&ctr[fin_at(b)], v);
+          wfin[b] = 0u;
+        }
+      }
+      fin_pending = 0;
+    }
+    __syncwarp();
+  };
 
   uint32_t trip = 0;
   for (; trip < kLoopBound; ++trip) {
     // ---- pending claims: the slot's record is published once its flag holds this epoch
     if (state == kPending) {
-      if (ld_acquire(&B.flags[B.qoff[pq] + pslot]) == epoch) {
+      // The flag is polled with a relaxed load (an acquire load would
+      // invalidate this SM's L1, which every other warp's traversal uses).
+      // The record is read only after the flag compared equal (a control
+      // dependency: GPUs do not issue loads past an unresolved branch) and
+      // from L2 (ld.global.cg), where the producer's release store made it
+      // visible before the flag.
+      if (ld_relaxed(&B.flags[B.qoff[pq] + pslot]) == epoch) {
         const float4* rec = B.queue + 2 * (B.qoff[pq] + pslot);
         float4 A = __ldcg(rec), Bv = __ldcg(rec + 1);
         uint32_t tag = __float_as_uint(Bv.w);
@@ -248,35 +286,60 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
           mode = kMarch;
         }
         state = kLive;
-      } else if (++polls >= kPendingBound) {
+      } else {
+        ++polls;
+      }
+    }
+    // a warp with no live ray publishes its finished counts: its pending
+    // claims may wait on exactly those counts to see their queue close
+    if (__ballot_sync(0xFFFFFFFFu, state == kLive) == 0u && __shfl_sync(0xFFFFFFFFu, fin_pending, 0) != 0u)
+      flush();
+    // claims ahead of the producers: retire those whose queue closed short
+    // of their slot (checked every 64 unsuccessful polls)
+    if (__ballot_sync(0xFFFFFFFFu, state == kPending && polls != 0u && (polls & 63u) == 0u)) {
+      uint32_t mask = 0;
+      if (lane == 0) mask = closed_mask(ctr, B);
+      mask = __shfl_sync(0xFFFFFFFFu, mask, 0);
+      if (state == kPending && ((mask >> (pq / 2u + 1u)) & 1u)) {
+        if (pslot >= ld_relaxed(&ctr[reserved_at(pq)])) state = kIdle;  // never filled
+      }
+      if (state == kPending && polls >= kPendingBound) {
         errors = 1;
-        state = kIdle;  // dropped: counted as finished below
+        state = kIdle;
       }
     }
     // ---- refill idle lanes
     uint32_t idle = __ballot_sync(0xFFFFFFFFu, state == kIdle);
-    uint32_t live_mesh = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kMesh);
-    uint32_t live_terr = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kTerrain);
     uint32_t nidle = __popc(idle);
     if (nidle != 0u && (nidle >= B.refill_min || nidle == 32u)) {
+      uint32_t live_mesh = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kMesh);
+      uint32_t live_terr = __ballot_sync(0xFFFFFFFFu, state != kIdle && kind == kTerrain);
+      // lane q reads queue q's counters: one round trip for all queues
+      uint32_t avail = 0;
+      if (lane < nq) {
+        uint32_t r = ld_relaxed(&ctr[reserved_at(lane)]), c = ld_relaxed(&ctr[claimed_at(lane)]);
+        avail = r > c ? r - c : 0u;
+      }
       uint32_t src = 0xFFFFFFFFu, base = 0, k = 0;
-      if (lane == 0) {
-        uint32_t first = live_terr > live_mesh ? kTerrain : kMesh;
-        for (int b = (int)B.depth - 1; b >= 1 && k == 0; --b) {
-          for (uint32_t j = 0; j < 2 && k == 0; ++j) {
-            uint32_t q = 2u * (uint32_t)(b - 1) + (j == 0 ? first : 1u - first);
-            k = claim(ctr, q, nidle, base);
-            if (k) src = q;
-          }
+      const uint32_t first = live_terr > live_mesh ? kTerrain : kMesh;
+      for (int b = (int)B.depth - 1; b >= 1 && k == 0; --b) {
+        for (uint32_t j = 0; j < 2 && k == 0; ++j) {
+          uint32_t q = 2u * (uint32_t)(b - 1) + (j == 0 ? first : 1u - first);
+          uint32_t av = __shfl_sync(0xFFFFFFFFu, avail, q);
+          if (av == 0u) continue;
+          // atomicAdd claims pipeline in L2 (a compare-and-swap loop
+          // serialises thousands of warps); a claim that races past the
+          // reserved count waits for its slot or retires when the queue closes
+          k = min(nidle, av);
+          if (lane == 0) base = atomicAdd(&ctr[claimed_at(q)], k);
+          src = q;
         }
-        if (k == 0 && ld_relaxed(&ctr[kCursor]) < B.total_pixels) {
-          base = atomicAdd(&ctr[kCursor], nidle);
-          k = base < B.total_pixels ? min(nidle, B.total_pixels - base) : 0u;
-          if (k) {
-            atomicAdd(&ctr[kCreated], k);
-            src = 0xFFFFFFFEu;
-          }
-        }
+      }
+      if (k == 0 && lane == 0 && !primary_done) {
+        base = atomicAdd(&ctr[kCursor], nidle);
+        k = base < B.total_pixels ? min(nidle, B.total_pixels - base) : 0u;
+        if (k) src = 0xFFFFFFFEu;
+        if (base + nidle >= B.total_pixels) primary_done = true;
       }
       src = __shfl_sync(0xFFFFFFFFu, src, 0);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
@@ -302,7 +365,10 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
             mode = kMarch;
           }
           state = kLive;
-        } else {
+        } else if (base + rank < B.qcap[src]) {
+          // a claim at or past the queue's capacity can never be filled
+          // (each pixel adds at most one ray per bounce): it is dropped
+          // here and its flag is never read
           pq = src;
           pslot = base + rank;
           polls = 0;
@@ -312,19 +378,22 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
       }
     }
     if (__ballot_sync(0xFFFFFFFFu, state != kIdle) == 0u) {
-      // nothing in this warp: leave once nothing can be created any more
+      // nothing in this warp: publish its finished counts, then leave once
+      // every bounce is closed (all created rays have finished)
+      flush();
       uint32_t leave = 0;
       if (lane == 0) {
-        if (ld_relaxed(&ctr[kCursor]) >= B.total_pixels) {
-          uint32_t f = ld_acquire(&ctr[kFinished]);
-          uint32_t c = ld_acquire(&ctr[kCreated]);
-          leave = f == c ? 1u : 0u;
+        if (!primary_done) primary_done = ld_relaxed(&ctr[kCursor]) >= B.total_pixels;
+        if (primary_done) leave = (closed_mask(ctr, B) >> B.depth) & 1u;
+        if (!leave) {
+          __nanosleep(backoff);
+          backoff = min(2u * backoff, 4096u);
         }
-        if (!leave) __nanosleep(64);
       }
       if (__shfl_sync(0xFFFFFFFFu, leave, 0)) break;
       continue;
     }
+    backoff = 32;
     // ---- one step of every live ray
     bool done = false, hit = false;
     V3 n = {0.f, 0.f, 1.f}, hp = {0.f, 0.f, 0.f};
@@ -335,7 +404,9 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
       const SceneDev& S = sc[scene];
       if (kind == kMesh) {
         KdDev kd = kd_of(S);
-        trav_step<0, false, COUNT>(tr, kd, snodes + S.stage_off, cnt);
+        // up to steps_per_trip leaves before the warp's bookkeeping runs again
+        for (uint32_t it = 0; it < B.steps_per_trip && tr.live; ++it)
+          trav_step<0, false, COUNT>(tr, kd, snodes + S.stage_off, cnt);
         if (!tr.live) {
           done = true;
           hit = tr.best_id >= 0;
@@ -357,6 +428,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
         }
       } else {
         PermBytes P{sperm + 512u * S.perm_slot};
+        for (uint32_t it = 0; it < B.steps_per_trip && !done; ++it) {
         V3 qp;
         if (mode == kMarch) {
           qp = v3(__fmaf_rn(t, tr.d.x, tr.o.x), __fmaf_rn(t, tr.d.y, tr.o.y),
@@ -380,7 +452,10 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
             tap = 0;
           } else {
             t = __fmaf_rn(S.step_factor, v, t);
-            if (t > S.tmax || steps >= S.max_steps) done = true;
+            // going up above the ceiling it can only miss: stop early (the
+            // result, a miss with this direction, is what the march reaches)
+            if (t > S.tmax || steps >= S.max_steps || (tr.d.y >= 0.0f && qp.y > S.ceiling))
+              done = true;
           }
         } else {
           if ((tap & 1u) == 0u) {
@@ -405,6 +480,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
             ++tap;
           }
         }
+        }
       }
     }
     // ---- finished rays: write or continue the path
@@ -427,9 +503,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
       }
       state = kIdle;
     }
-    // dropped pending claims also finish (error path)
-    bool finished = done || (errors && state == kIdle && polls >= kPendingBound);
-    if (finished && !done) polls = 0;
     // ---- append continuations, one atomic per distinct queue
     uint32_t pushers = __ballot_sync(0xFFFFFFFFu, push);
     if (pushers) {
@@ -438,23 +511,26 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
         uint32_t peers = __match_any_sync(pushers, qn);
         uint32_t leader = __ffs(peers) - 1u;
         uint32_t b0 = 0;
-        if (lane == leader) b0 = atomicAdd(&ctr[kReserved + qn], (uint32_t)__popc(peers));
+        if (lane == leader) b0 = atomicAdd(&ctr[reserved_at(qn)], (uint32_t)__popc(peers));
         b0 = __shfl_sync(peers, b0, leader);
         slot = b0 + __popc(peers & lt_mask);
         float4* rec = B.queue + 2 * (B.qoff[qn] + slot);
         __stcg(rec, R0);
         __stcg(rec + 1, R1);
+        // the release store orders this lane's record before its flag
+        st_release(&B.flags[B.qoff[qn] + slot], epoch);
       }
-      if (lane == 0) atomicAdd(&ctr[kCreated], (uint32_t)__popc(pushers));
-      __threadfence();
-      if (push) st_release(&B.flags[B.qoff[qn] + slot], epoch);
     }
-    uint32_t fin = __ballot_sync(0xFFFFFFFFu, finished);
-    if (fin) {
-      __threadfence();
-      if (lane == 0) atomicAdd(&ctr[kFinished], (uint32_t)__popc(fin));
-    }
+    // finished rays are counted per warp and bounce in shared memory and
+    // published when the warp runs dry (or every 1024): their children were
+    // reserved first, so a published count never runs ahead of the created
+    // count
+    uint32_t fin = __ballot_sync(0xFFFFFFFFu, done);
+    if (done) atomicAdd(&wfin[bounce], 1u);
+    if (lane == 0) fin_pending += (uint32_t)__popc(fin);
+    if (__shfl_sync(0xFFFFFFFFu, fin_pending, 0) >= 1024u) flush();
   }
+  flush();
   if (trip >= kLoopBound) errors = 1;
   if (COUNT) {
     uint32_t v4[4] = {cnt.inner, cnt.leaf, cnt.tests, cnt.status};
@@ -469,19 +545,18 @@ __global__ void __launch_bounds__(512) k_batch(BatchDev B) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    uint32_t d = atomicAdd(&ctr[kDone], 1u);
-    if (d == gridDim.x - 1u) {
+    uint32_t dn = atomicAdd(&ctr[kDone], 1u);
+    if (dn == gridDim.x - 1u) {
       __threadfence();
       for (uint32_t q = 0; q < nq; ++q) {
-        ctr[kStats + q] = ctr[kReserved + q];
-        ctr[kReserved + q] = 0u;
-        ctr[kClaimed + q] = 0u;
+        ctr[kStats + q] = ctr[reserved_at(q)];
+        ctr[reserved_at(q)] = 0u;
+        ctr[claimed_at(q)] = 0u;
       }
+      for (uint32_t b = 0; b < kMaxDepth; ++b) ctr[fin_at(b)] = 0u;
       ctr[kStatsPrimary] = min(ctr[kCursor], B.total_pixels);
       ctr[kStatsError] = ctr[kError];
       ctr[kCursor] = 0u;
-      ctr[kCreated] = 0u;
-      ctr[kFinished] = 0u;
       ctr[kError] = 0u;
       ctr[kDone] = 0u;
       __threadfence();
@@ -510,7 +585,7 @@ struct re_batch {
   uint32_t* d_flags = nullptr;
   uint32_t* d_ctr = nullptr;
   uint64_t qoff[re::batch::kMaxQueues] = {};
-  re_batch_tuning tune = {256, 8, 0, 0};
+  re_batch_tuning tune = {256, 8, 0, 8};
   // captured frame
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -563,9 +638,9 @@ uint32_t layout_stage(re_batch* b, uint32_t stage_nodes) {
   return off;
 }
 
-size_t smem_bytes(const re_batch* b, uint32_t stage_total) {
+size_t smem_bytes(const re_batch* b, uint32_t stage_total, uint32_t block_threads) {
   return b->num_scenes * sizeof(SceneDev) + 512u * (b->perms.size() / 512) +
-         (size_t)stage_total * sizeof(uint2);
+         (size_t)stage_total * sizeof(uint2) + (size_t)(block_threads / 32) * kMaxDepth * 4;
 }
 
 // Scene table (with this tuning's staging offsets) to the device and the
@@ -576,9 +651,9 @@ re_status prepare(re_batch* b, const re_batch_tuning& tn, cudaStream_t st) {
                           cudaMemcpyHostToDevice, st));
   RE_CUDA(cudaStreamSynchronize(st));
   RE_CUDA(cudaFuncSetAttribute(k_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes(b, stage_total)));
+                               (int)smem_bytes(b, stage_total, 512)));
   RE_CUDA(cudaFuncSetAttribute(k_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes(b, stage_total)));
+                               (int)smem_bytes(b, stage_total, 512)));
   return RE_OK;
 }
 
@@ -586,7 +661,7 @@ re_status prepare(re_batch* b, const re_batch_tuning& tn, cudaStream_t st) {
 re_status launch(re_batch* b, float* d_radiance, re_hit* d_primary, cudaStream_t st,
                  const re_batch_tuning& tn, unsigned long long* totals = nullptr) {
   uint32_t stage_total = layout_stage(b, tn.stage_nodes);
-  size_t smem = smem_bytes(b, stage_total);
+  size_t smem = smem_bytes(b, stage_total, tn.block_threads);
   int per_sm = 0;
   auto kern = totals ? k_batch<true> : k_batch<false>;
   RE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)tn.block_threads,
@@ -602,10 +677,14 @@ re_status launch(re_batch* b, float* d_radiance, re_hit* d_primary, cudaStream_t
   B.depth = b->depth;
   B.seed = b->seed;
   B.refill_min = tn.refill_min;
+  B.steps_per_trip = tn.steps_per_trip ? tn.steps_per_trip : 1u;
   B.mesh_bias = b->mesh_bias;
   B.queue = b->d_queue;
   B.flags = b->d_flags;
-  for (uint32_t q = 0; q < kMaxQueues; ++q) B.qoff[q] = b->qoff[q];
+  for (uint32_t q = 0; q < kMaxQueues; ++q) {
+    B.qoff[q] = b->qoff[q];
+    B.qcap[q] = q < 2 * (b->depth - 1) ? (uint32_t)b->cap[q & 1u] : 0u;
+  }
   B.ctr = b->d_ctr;
   B.radiance = d_radiance;
   B.primary = reinterpret_cast<int4*>(d_primary);
@@ -621,6 +700,7 @@ re_status check_tuning(const re_batch_tuning& t) {
   if (t.refill_min == 0 || t.refill_min > 32)
     return fail(RE_ERR_INVALID_ARG, "re_batch: refill_min must be in [1, 32]");
   if (t.stage_nodes > 4096) return fail(RE_ERR_INVALID_ARG, "re_batch: stage_nodes > 4096");
+  if (t.steps_per_trip > 256) return fail(RE_ERR_INVALID_ARG, "re_batch: steps_per_trip > 256");
   return RE_OK;
 }
 
@@ -702,6 +782,9 @@ RE_API re_status re_batch_create(const re_batch_scene* scenes, uint32_t n, const
       d.step_factor = f.step_factor;
       d.eps = f.eps;
       d.tmax = f.tmax;
+      // |Perlin| <= 2 (corner terms |g . r| <= 2, convex blend), so
+      // |fBm| <= 2 (2 - 2^(1 - octaves)) and the density is positive above
+      d.ceiling = 2.0f * std::fabs(f.amplitude) * (2.0f - std::ldexp(1.0f, 1 - (int)f.octaves)) + 1e-3f;
       b->cap[1] += (uint64_t)s.width * s.height;
     } else {
       delete b;
@@ -853,14 +936,16 @@ RE_API re_status re_batch_set_tuning(re_batch* b, const re_batch_tuning* t) {
 }
 
 // Times one frame per candidate (after a warm-up frame) and keeps the
-// fastest: block size x refill threshold x staged nodes per mesh scene.
+// fastest: block size x refill threshold x staged nodes per mesh scene x
+// leaves / field evaluations per trip.
 RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
                                    re_batch_tuning* out, float* best_ms) {
   if (!b || !d_radiance) return re::fail(RE_ERR_INVALID_ARG, "re_batch_autotune: bad arguments");
   cudaStream_t st = (cudaStream_t)stream;
   const uint32_t blocks[] = {128, 256, 512};
-  const uint32_t refills[] = {4, 8, 16, 32};
-  const uint32_t stages[] = {0, 64, 512};
+  const uint32_t refills[] = {8, 32};
+  const uint32_t stages[] = {0, 512};
+  const uint32_t trips[] = {1, 8, 64};
   cudaEvent_t e0, e1;
   RE_CUDA(cudaEventCreate(&e0));
   RE_CUDA(cudaEventCreate(&e1));
@@ -869,9 +954,10 @@ RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
   re_status s = RE_OK;
   for (uint32_t bt : blocks)
     for (uint32_t rf : refills)
-      for (uint32_t sg : stages) {
-        re_batch_tuning t = {bt, rf, sg, 0};
-        size_t smem = re::smem_bytes(b, re::layout_stage(b, sg));
+      for (uint32_t sg : stages)
+        for (uint32_t tp : trips) {
+        re_batch_tuning t = {bt, rf, sg, tp};
+        size_t smem = re::smem_bytes(b, re::layout_stage(b, sg), bt);
         if (smem > 200 * 1024) continue;
         s = re::prepare(b, t, st);
         if (s != RE_OK) break;

@@ -115,8 +115,8 @@ def test_graph_replay_and_tunings_give_identical_frames(cuda):
             b.render(out=out, graph=True)
             assert np.array_equal(out.cpu().numpy(), ref)
             assert b.stats()["error"] == 0
-        for bt, rf, sg in ((128, 1, 0), (512, 32, 64), (256, 8, 512)):
-            b.set_tuning(bt, rf, sg)
+        for bt, rf, sg, sp in ((128, 1, 0, 1), (512, 32, 64, 64), (256, 8, 512, 8)):
+            b.set_tuning(bt, rf, sg, sp)
             assert np.array_equal(b.render().cpu().numpy(), ref)
         t = b.autotune()
         assert t["block_threads"] in (128, 256, 512) and t["frame_ms"] > 0

@@ -536,7 +536,7 @@ typedef struct re_path_params {
 } re_path_params;
 
 typedef struct re_batch_tuning {
-  uint32_t block_threads; /* 32..512, multiple of 32 (256)                  */
+  uint32_t block_threads; /* 32..256, multiple of 32 (256)                  */
   uint32_t refill_min;    /* idle lanes a warp waits for before claiming    */
   uint32_t stage_nodes;   /* top nodes per mesh scene in shared memory      */
   uint32_t steps_per_trip;/* leaves / field evaluations a lane advances     */

@@ -160,22 +160,13 @@ NSDF_FLOPS_PER_EVAL = 41088
 
 
 def measure_l2_gbs(torch) -> float:
-    """L2 bandwidth measured in this run: device copies between two 32 MB
-    buffers (64 MB resident in the 126 MB L2), bytes read + written per
-    second over 50 copies.  A reference figure for the traversal kernels,
-    whose reads mostly hit L2 (no measured L2 figure is provided)."""
-    n = 8 << 20
-    x = torch.ones(n, dtype=torch.float32, device="cuda")
-    y = torch.empty_like(x)
-    for _ in range(5):
-        y.copy_(x)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(50):
-        y.copy_(x)
-    b.record()
-    torch.cuda.synchronize()
-    return round(2 * 4 * n * 50 / (a.elapsed_time(b) / 1e3) / 1e9, 1)
+    """L2 read bandwidth measured in this run by the library's probe
+    (re_measure_l2_read: 16-byte L2-only loads over a 32 MB L2-resident
+    buffer, 100 passes in one launch).  The traversal kernels' reads mostly
+    hit L2; no measured L2 figure comes with the hardware peaks."""
+    import rayengine_b200 as rb
+
+    return round(rb.measure_l2_read_gbs(32 << 20, 100), 1)
 
 
 def hbm_roofline(wl, phase_ms, peaks):
@@ -188,7 +179,7 @@ def hbm_roofline(wl, phase_ms, peaks):
            "traffic": ncu_traffic(f"{wl.name}:{dom}")}
     if peaks.get("l2_gbs"):
         out["l2"] = {"peak": peaks["l2_gbs"], "frac": round(achieved / peaks["l2_gbs"], 4),
-                     "peak_source": "measured in this run (L2-resident device copy)"}
+                     "peak_source": "measured in this run (re_measure_l2_read)"}
     return out
 
 

@@ -574,6 +574,13 @@ RE_API re_status re_batch_set_tuning(re_batch* b, const re_batch_tuning* t);
 RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
                                    re_batch_tuning* out, float* best_ms);
 
+/* ---- measurement ---------------------------------------------------------
+ * L2 read bandwidth (16-byte L2-only loads over an L2-resident buffer of
+ * `bytes`, 1-64 MB, read `passes` times in one launch), in GB/s: the
+ * denominator of the traversal kernels' L2 roofline.  No reference
+ * counterpart. */
+RE_API re_status re_measure_l2_read(size_t bytes, uint32_t passes, float* gbs, void* stream);
+
 #ifdef __cplusplus
 }
 /* The reference's render call, same C++ signature (renderer.cu:701):

@@ -766,3 +766,10 @@ def trace_instances(instances, cam, w, h, flags=TRACE_TWO_SIDED, stream=None):
     call("re_trace_instances", arr, len(instances), ctypes.byref(cam), w, h, flags, _dptr(out),
          _dptr(idx), _stream_ptr(stream))
     return out, idx
+
+
+def measure_l2_read_gbs(nbytes: int = 32 << 20, passes: int = 100, stream=None) -> float:
+    """L2 read bandwidth of this GPU in GB/s (re_measure_l2_read)."""
+    v = ctypes.c_float()
+    call("re_measure_l2_read", nbytes, passes, ctypes.byref(v), _stream_ptr(stream))
+    return float(v.value)

@@ -317,6 +317,8 @@ class SoupPrimary:
         self.cam = cfg.camera()
         W, H = cfg.width, cfg.height
         self.out = torch.empty((H * W, 4), dtype=torch.int32, device="cuda")
+        # set-up: the autotuner picks staging depth and ray refill threshold
+        self.tuning = self.scene.autotune_primary(self.cam, W, H)
         c = self.scene.count_primary(self.cam, W, H).cpu().numpy().astype(np.int64)
         self.tot = {"inner": int(c[:, 0].sum()), "leaf": int(c[:, 1].sum()),
                     "tests": int(c[:, 2].sum()), "rays": W * H}
@@ -329,7 +331,8 @@ class SoupPrimary:
                             f"{self.cfg.width}x{self.cfg.height} primary rays",
                 "triangles": st["num_tris"], "kd_nodes": st["num_nodes"],
                 "kd_refs": st["num_refs"], "kd_build_s": round(self.build_s, 3),
-                "rays_per_step": self.rays_per_step, "l2": "flushed between steps (256 MB write)"}
+                "rays_per_step": self.rays_per_step, "tuning": self.tuning,
+                "l2": "flushed between steps (256 MB write)"}
 
     def phases(self, stream):
         W, H = self.cfg.width, self.cfg.height

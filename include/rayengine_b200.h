@@ -93,12 +93,14 @@ typedef struct re_kd_params {
 
 typedef struct re_scene re_scene;
 
-/* Launch tuning of a scene (see re_autotune_ao). */
+/* Launch tuning of a scene (see re_autotune_ao, re_autotune_primary). */
 typedef struct re_tuning {
   uint32_t stage_nodes;      /* top nodes staged in shared memory per block (<= 8192) */
   uint32_t queue_kind_major; /* secondary-ray queue: 0 pixel-major, 1 kind-major    */
   uint32_t refill_min;       /* idle lanes before a warp claims new secondary rays, 1..32 */
-  uint32_t reserved;
+  uint32_t ray_refill_min;   /* the same for primary and caller rays (re_trace_primary,
+                                re_count_primary, re_trace_rays), 1..32; 32 (default):
+                                each lane runs its ray to the end, no refill */
 } re_tuning;
 
 typedef struct re_scene_stats {
@@ -222,6 +224,12 @@ RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam,
 RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w,
                                 uint32_t h, const re_ao_params* p,
                                 re_tuning* best, float* best_ms, void* stream);
+/* Autotuner of the primary pass: times re_trace_primary(flags) for each
+ * combination of staging depth and ray_refill_min the same way and keeps
+ * the fastest (other fields unchanged).  Set-up time only. */
+RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w,
+                                     uint32_t h, uint32_t flags, re_tuning* best,
+                                     float* best_ms, void* stream);
 RE_API re_status re_scene_get_tuning(const re_scene* s, re_tuning* out);
 RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t);
 /* Work counters of the same frame (device array of 8 uint64): primary

@@ -83,7 +83,7 @@ class re_tuning(ctypes.Structure):
         ("stage_nodes", ctypes.c_uint32),
         ("queue_kind_major", ctypes.c_uint32),
         ("refill_min", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("ray_refill_min", ctypes.c_uint32),
     ]
 
 
@@ -218,6 +218,7 @@ _SIGS = {
     "re_render_ao_secondary": (ctypes.c_int, [_P, _P, _P, _P]),
     "re_render_ao_noalloc": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
     "re_autotune_ao": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), ctypes.POINTER(re_tuning), ctypes.POINTER(ctypes.c_float), _P]),
+    "re_autotune_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, ctypes.POINTER(re_tuning), ctypes.POINTER(ctypes.c_float), _P]),
     "re_scene_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_tuning)]),
     "re_scene_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_tuning)]),
     "re_render_ao_counts": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P]),

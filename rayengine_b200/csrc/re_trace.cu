@@ -39,12 +39,63 @@
 namespace re {
 
 // --------------------------------------------------------------- kernels
-// Primary rays, persistent warps over 8x4 pixel tiles.
+// Lane-refill driver shared by the ray kernels: each lane runs its ray one
+// leaf at a time (trav_step) and, as soon as at least refill_min lanes of the
+// warp are idle, the warp claims that many consecutive work indices with one
+// atomic, so lanes need not wait for the slowest ray of the warp and the
+// frame has no warp-sized tail.  gen(i, o, d, tmax) -> false for an index
+// without a ray; done(i, s, c) gets the finished walk (c: the ray's own
+// counters when COUNT).
+template <int MODE, bool ANYHIT, bool COUNT, class Gen, class Done>
+__device__ __forceinline__ void refill_walk(const KdDev& kd, const uint2* snodes, uint32_t n,
+                                            uint32_t refill_min, uint32_t* counter, Gen gen,
+                                            Done done) {
+  uint32_t lane = threadIdx.x & 31u;
+  Trav s;
+  s.live = false;
+  Counters c = {0, 0, 0, 0};
+  uint32_t cur = 0;
+  bool exhausted = false;
+  for (;;) {
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !s.live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && (nidle >= refill_min || nidle == 32u)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= n) exhausted = true;
+      if (!s.live) {
+        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+        V3 o, d;
+        float tmax;
+        if (i < n && gen(i, o, d, tmax)) {
+          cur = i;
+          if (COUNT) c = {0, 0, 0, 0};
+          trav_init(s, kd, o, d, tmax, 0u);
+          if (!s.live) done(cur, s, c);
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, s.live) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (s.live) {
+      trav_step<MODE, ANYHIT, COUNT>(s, kd, snodes, c);
+      if (!s.live) done(cur, s, c);
+    }
+  }
+}
+
+// Primary rays, persistent warps over 8x4 pixel tiles, each lane running its
+// ray to the end (ray_refill_min 32: no per-leaf bookkeeping; fastest when
+// rays of a tile take similar work).
 template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(256) k_primary(KdDev kd, CamDev cam, uint32_t w, uint32_t h,
-                                                 re_hit* __restrict__ out,
-                                                 uint4* __restrict__ counts,
-                                                 uint32_t* __restrict__ tile_counter) {
+__global__ void __launch_bounds__(256) k_primary_tiles(KdDev kd, CamDev cam, uint32_t w,
+                                                       uint32_t h, re_hit* __restrict__ out,
+                                                       uint4* __restrict__ counts,
+                                                       uint32_t* __restrict__ tile_counter,
+                                                       uint32_t) {
   extern __shared__ uint2 snodes[];
   stage_nodes(kd, snodes);
   uint32_t lane = threadIdx.x & 31u;
@@ -68,11 +119,49 @@ __global__ void __launch_bounds__(256) k_primary(KdDev kd, CamDev cam, uint32_t 
   }
 }
 
-// Caller rays (re_ray), persistent warps over 32-ray chunks.
+// Primary rays with lane refill (ray_refill_min < 32).  Work index i is lane
+// i % 32 of 8x4 pixel tile i / 32, so a warp's claims stay in one screen
+// region.
+template <int MODE, bool COUNT>
+__global__ void __launch_bounds__(256) k_primary(KdDev kd, CamDev cam, uint32_t w, uint32_t h,
+                                                 re_hit* __restrict__ out,
+                                                 uint4* __restrict__ counts,
+                                                 uint32_t* __restrict__ tile_counter,
+                                                 uint32_t refill_min) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
+  auto gen = [&](uint32_t i, V3& o, V3& d, float& tmax) {
+    uint32_t tile = i >> 5, l = i & 31u;
+    uint32_t x = (tile % tiles_x) * 8 + (l & 7u);
+    uint32_t y = (tile / tiles_x) * 4 + (l >> 3);
+    if (x >= w || y >= h) return false;
+    generate_ray(cam, w, h, x, y, o, d);
+    tmax = __int_as_float(0x7f800000);
+    return true;
+  };
+  auto done = [&](uint32_t i, const Trav& s, const Counters& c) {
+    uint32_t tile = i >> 5, l = i & 31u;
+    uint32_t x = (tile % tiles_x) * 8 + (l & 7u);
+    uint32_t y = (tile / tiles_x) * 4 + (l >> 3);
+    size_t pix = (size_t)y * w + x;
+    if (COUNT) {
+      counts[pix] = make_uint4(c.inner, c.leaf, c.tests, c.status);
+    } else {
+      HitState hs;
+      trav_result(s, hs);
+      store_hit(out, pix, hs);
+    }
+  };
+  refill_walk<MODE, false, COUNT>(kd, snodes, tiles * 32u, refill_min, tile_counter, gen, done);
+}
+
+// Caller rays (re_ray), persistent warps over 32-ray chunks, each lane
+// running its ray to the end (ray_refill_min 32).
 template <int MODE, bool ANYHIT>
-__global__ void __launch_bounds__(256) k_rays(KdDev kd, const float4* __restrict__ rays,
-                                              uint32_t n, re_hit* __restrict__ out,
-                                              uint32_t* __restrict__ counter) {
+__global__ void __launch_bounds__(256) k_rays_chunks(KdDev kd, const float4* __restrict__ rays,
+                                                     uint32_t n, re_hit* __restrict__ out,
+                                                     uint32_t* __restrict__ counter, uint32_t) {
   extern __shared__ uint2 snodes[];
   stage_nodes(kd, snodes);
   uint32_t lane = threadIdx.x & 31u;
@@ -88,6 +177,29 @@ __global__ void __launch_bounds__(256) k_rays(KdDev kd, const float4* __restrict
     traverse<MODE, ANYHIT, false>(kd, snodes, o, d, R0.w, 0u, hs, c);
     store_hit(out, i, hs);
   }
+}
+
+// Caller rays (re_ray), lane refill over ray indices (ray_refill_min < 32).
+template <int MODE, bool ANYHIT>
+__global__ void __launch_bounds__(256) k_rays(KdDev kd, const float4* __restrict__ rays,
+                                              uint32_t n, re_hit* __restrict__ out,
+                                              uint32_t* __restrict__ counter,
+                                              uint32_t refill_min) {
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  auto gen = [&](uint32_t i, V3& o, V3& d, float& tmax) {
+    float4 R0 = __ldg(&rays[2 * (size_t)i]), R1 = __ldg(&rays[2 * (size_t)i + 1]);
+    o = {R0.x, R0.y, R0.z};
+    d = {R1.x, R1.y, R1.z};
+    tmax = R0.w;
+    return true;
+  };
+  auto done = [&](uint32_t i, const Trav& s, const Counters&) {
+    HitState hs;
+    trav_result(s, hs);
+    store_hit(out, i, hs);
+  };
+  refill_walk<MODE, ANYHIT, false>(kd, snodes, n, refill_min, counter, gen, done);
 }
 
 // Primary + secondary-ray generation for the AO frame.
@@ -414,6 +526,42 @@ re_status create_from_packed(const float* tris, uint32_t n, const re_kd_params* 
 }  // namespace
 }  // namespace re
 
+namespace re {
+namespace {
+
+// One primary pass: whole-warp tiles when ray_refill_min is 32, else lane
+// refill.  Both kernels take the same arguments.
+template <int MODE, bool COUNT>
+re_status launch_primary(re_scene* s, const re_camera& cam, uint32_t w, uint32_t h, re_hit* out,
+                         uint4* counts, cudaStream_t st) {
+  KdDev kd = kd_view(s);
+  CamDev cd = cam_view(cam);
+  size_t smem = kd.stage * sizeof(uint2);
+  uint32_t refill = s->tune.ray_refill_min;
+  auto k = refill >= 32u ? k_primary_tiles<MODE, COUNT> : k_primary<MODE, COUNT>;
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st));
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, w, h, out, counts, s->d_counters, refill);
+  RE_CHECK_LAUNCH(COUNT ? "re_count_primary: launch" : "re_trace_primary: launch");
+  return RE_OK;
+}
+
+template <int MODE, bool ANYHIT>
+re_status launch_rays(re_scene* s, const float4* rays, uint32_t n, re_hit* out, cudaStream_t st) {
+  KdDev kd = kd_view(s);
+  size_t smem = kd.stage * sizeof(uint2);
+  uint32_t refill = s->tune.ray_refill_min;
+  auto k = refill >= 32u ? k_rays_chunks<MODE, ANYHIT> : k_rays<MODE, ANYHIT>;
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st));
+  RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<grid_for(k, smem), 256, smem, st>>>(kd, rays, n, out, s->d_counters, refill);
+  RE_CHECK_LAUNCH("re_trace_rays: launch");
+  return RE_OK;
+}
+
+}  // namespace
+}  // namespace re
+
 extern "C" {
 
 RE_API void re_kd_params_default(re_kd_params* p) {
@@ -516,22 +664,9 @@ RE_API re_status re_trace_primary(re_scene* s, const re_camera* cam, uint32_t w,
     return re::fail(RE_ERR_INVALID_ARG, "re_trace_primary: bad arguments");
   if ((uint64_t)w * h > (1ull << 31)) return re::fail(RE_ERR_LIMIT, "re_trace_primary: image too large");
   if (flags & ~1u) return re::fail(RE_ERR_INVALID_ARG, "re_trace_primary: unknown flags");
-  cudaStream_t st_ = (cudaStream_t)stream;
-  re::KdDev kd = re::kd_view(s);
-  re::CamDev cd = re::cam_view(*cam);
-  size_t smem = kd.stage * sizeof(uint2);
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
-  if (flags & RE_TRACE_ONE_SIDED) {
-    auto k = re::k_primary<1, false>;
-    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, d_out, nullptr, s->d_counters);
-  } else {
-    auto k = re::k_primary<0, false>;
-    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, d_out, nullptr, s->d_counters);
-  }
-  RE_CHECK_LAUNCH("re_trace_primary: launch");
-  return RE_OK;
+  if (flags & RE_TRACE_ONE_SIDED)
+    return re::launch_primary<1, false>(s, *cam, w, h, d_out, nullptr, (cudaStream_t)stream);
+  return re::launch_primary<0, false>(s, *cam, w, h, d_out, nullptr, (cudaStream_t)stream);
 }
 
 RE_API re_status re_count_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
@@ -542,23 +677,10 @@ RE_API re_status re_count_primary(re_scene* s, const re_camera* cam, uint32_t w,
     return re::fail(RE_ERR_INVALID_ARG, "re_count_primary: bad arguments");
   if ((uint64_t)w * h > (1ull << 31)) return re::fail(RE_ERR_LIMIT, "re_count_primary: image too large");
   if (flags & ~1u) return re::fail(RE_ERR_INVALID_ARG, "re_count_primary: unknown flags");
-  cudaStream_t st_ = (cudaStream_t)stream;
-  re::KdDev kd = re::kd_view(s);
-  re::CamDev cd = re::cam_view(*cam);
-  size_t smem = kd.stage * sizeof(uint2);
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
   uint4* c4 = reinterpret_cast<uint4*>(d_counts);
-  if (flags & RE_TRACE_ONE_SIDED) {
-    auto k = re::k_primary<1, true>;
-    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, nullptr, c4, s->d_counters);
-  } else {
-    auto k = re::k_primary<0, true>;
-    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, cd, w, h, nullptr, c4, s->d_counters);
-  }
-  RE_CHECK_LAUNCH("re_count_primary: launch");
-  return RE_OK;
+  if (flags & RE_TRACE_ONE_SIDED)
+    return re::launch_primary<1, true>(s, *cam, w, h, nullptr, c4, (cudaStream_t)stream);
+  return re::launch_primary<0, true>(s, *cam, w, h, nullptr, c4, (cudaStream_t)stream);
 }
 
 RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n, uint32_t flags,
@@ -569,26 +691,14 @@ RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n, ui
   if (n == 0) return RE_OK;
   if (n > (1u << 31)) return re::fail(RE_ERR_LIMIT, "re_trace_rays: n > 2^31");
   if (flags & ~3u) return re::fail(RE_ERR_INVALID_ARG, "re_trace_rays: unknown flags");
-  cudaStream_t st_ = (cudaStream_t)stream;
-  re::KdDev kd = re::kd_view(s);
-  size_t smem = kd.stage * sizeof(uint2);
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st_));
   const float4* r4 = reinterpret_cast<const float4*>(d_rays);
-#define RE_LAUNCH_RAYS(M, A)                                                                \
-  do {                                                                                      \
-    auto k = re::k_rays<M, A>;                                                              \
-    RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    k<<<re::grid_for(k, smem), 256, smem, st_>>>(kd, r4, n, d_out, s->d_counters);           \
-  } while (0)
+  cudaStream_t st_ = (cudaStream_t)stream;
   switch (flags & 3u) {
-    case 0: RE_LAUNCH_RAYS(0, false); break;
-    case 1: RE_LAUNCH_RAYS(1, false); break;
-    case 2: RE_LAUNCH_RAYS(0, true); break;
-    default: RE_LAUNCH_RAYS(1, true); break;
+    case 0: return re::launch_rays<0, false>(s, r4, n, d_out, st_);
+    case 1: return re::launch_rays<1, false>(s, r4, n, d_out, st_);
+    case 2: return re::launch_rays<0, true>(s, r4, n, d_out, st_);
+    default: return re::launch_rays<1, true>(s, r4, n, d_out, st_);
   }
-#undef RE_LAUNCH_RAYS
-  RE_CHECK_LAUNCH("re_trace_rays: launch");
-  return RE_OK;
 }
 
 }  // extern "C"
@@ -818,8 +928,9 @@ RE_API re_status re_scene_get_tuning(const re_scene* s, re_tuning* out) {
 
 RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t) {
   if (!s || !t) return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: null argument");
-  if (t->refill_min < 1 || t->refill_min > 32)
-    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: refill_min must be in [1, 32]");
+  if (t->refill_min < 1 || t->refill_min > 32 || t->ray_refill_min < 1 || t->ray_refill_min > 32)
+    return re::fail(RE_ERR_INVALID_ARG,
+                    "re_scene_set_tuning: refill_min and ray_refill_min must be in [1, 32]");
   if (t->queue_kind_major > 1)
     return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0 or 1");
   s->tune = *t;
@@ -856,7 +967,7 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
     if (si > 0 && stages[si] == stages[si - 1]) continue;
     for (uint32_t km = 0; km < 2 && rs == RE_OK; ++km) {
       for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
-        re_tuning t = {stages[si], km, refills[ri], 0};
+        re_tuning t = {stages[si], km, refills[ri], keep.ray_refill_min};
         rs = re_scene_set_tuning(s, &t);
         if (rs != RE_OK) break;
         rs = re_render_ao(s, cam, w, h, p, hits, mask, nullptr, stream);
@@ -888,6 +999,67 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
     s->tune = keep;
     s->stage = keep.stage_nodes;
     return rs;
+  }
+  re_scene_set_tuning(s, &best);
+  if (best_out) *best_out = best;
+  if (best_ms_out) *best_ms_out = best_ms / 3.0f;
+  return RE_OK;
+}
+
+// Times the primary pass (re_trace_primary with `flags`) for every
+// combination of staging depth and ray refill threshold (one warm-up and
+// three timed passes each, CUDA events on the caller's stream) and keeps the
+// fastest on the scene.  Set-up time only: it allocates its own output.
+RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
+                                     uint32_t flags, re_tuning* best_out, float* best_ms_out,
+                                     void* stream) {
+  re_status rs = re::check_scene(s, "re_autotune_primary");
+  if (rs != RE_OK) return rs;
+  if (!cam || w < 2 || h < 2 || (flags & ~1u))
+    return re::fail(RE_ERR_INVALID_ARG, "re_autotune_primary: bad arguments");
+  if ((uint64_t)w * h > (1ull << 28))
+    return re::fail(RE_ERR_LIMIT, "re_autotune_primary: image > 2^28 pixels");
+  cudaStream_t st = (cudaStream_t)stream;
+  re_hit* hits = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  RE_CUDA(cudaMalloc(&hits, (size_t)w * h * sizeof(re_hit)));
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  re_tuning keep = s->tune, best = s->tune;
+  float best_ms = 1e30f;
+  uint32_t bfs = std::min(s->host.bfs_nodes, re::kMaxStage);
+  const uint32_t stages[3] = {0u, std::min(1024u, bfs), std::min(4096u, bfs)};
+  const uint32_t refills[4] = {32u, 16u, 8u, 4u};
+  for (int si = 0; si < 3 && ce == cudaSuccess && rs == RE_OK; ++si) {
+    if (si > 0 && stages[si] == stages[si - 1]) continue;
+    for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
+      re_tuning t = keep;
+      t.stage_nodes = stages[si];
+      t.ray_refill_min = refills[ri];
+      rs = re_scene_set_tuning(s, &t);
+      if (rs != RE_OK) break;
+      rs = re_trace_primary(s, cam, w, h, flags, hits, stream);
+      if (rs != RE_OK) break;
+      ce = cudaEventRecord(e0, st);
+      for (int r = 0; r < 3 && rs == RE_OK; ++r) rs = re_trace_primary(s, cam, w, h, flags, hits, stream);
+      if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+      if (ce != cudaSuccess) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = s->tune;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(hits);
+  if (ce != cudaSuccess || rs != RE_OK) {
+    s->tune = keep;
+    s->stage = keep.stage_nodes;
+    return ce != cudaSuccess ? re::cuda_fail(ce, "re_autotune_primary") : rs;
   }
   re_scene_set_tuning(s, &best);
   if (best_out) *best_out = best;

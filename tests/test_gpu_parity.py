@@ -134,6 +134,40 @@ def test_caller_rays_closest_and_anyhit(cuda):
                 assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4))
 
 
+def test_ray_refill_threshold_changes_only_speed(cuda):
+    """Primary and caller-ray kernels refill idle lanes; every threshold gives
+    the oracle's hits (and per-pixel work counts)."""
+    cfg = rb.configs.SoupConfig(num_tris=8192, width=200, height=120)
+    packed = cfg.packed()
+    cam = cfg.camera()
+    rng = np.random.default_rng(9)
+    n = 20011  # not a multiple of 32
+    o = rng.uniform(-1.5, 1.5, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    rays = np.concatenate([o, np.full((n, 1), np.inf, np.float32), d, np.zeros((n, 1), np.float32)], 1)
+    with rb.KDScene.from_packed(packed) as sc:
+        st, kd = _kd(sc)
+        ref = po.primary_kd(kd, cam, 200, 120).view(np.int32).reshape(-1, 4)
+        _, rc = po.primary_kd(kd, cam, 200, 120, counts=True)
+        rref = po.rays_kd(kd, rays).view(np.int32).reshape(-1, 4)
+        dr = torch.from_numpy(rays).cuda()
+        t = sc.tuning()
+        assert t["ray_refill_min"] == 32
+        for refill in (1, 3, 8, 32):
+            sc.set_tuning(t["stage_nodes"], t["queue_kind_major"], t["refill_min"], refill)
+            assert np.array_equal(_hits(sc.trace_primary(cam, 200, 120)), ref), refill
+            cnt = sc.count_primary(cam, 200, 120).cpu().numpy()
+            assert np.array_equal(cnt, rc.view(np.uint32).reshape(-1, 4).astype(np.int32)), refill
+            assert np.array_equal(_hits(sc.trace_rays(dr, 0)), rref), refill
+        with pytest.raises(rb.RayEngineError):
+            sc.set_tuning(t["stage_nodes"], t["queue_kind_major"], t["refill_min"], 0)
+        best = sc.autotune_primary(cam, 200, 120)
+        assert best["ray_refill_min"] in (4, 8, 16, 32) and best["frame_ms"] > 0
+        assert sc.tuning()["ray_refill_min"] == best["ray_refill_min"]
+        assert np.array_equal(_hits(sc.trace_primary(cam, 200, 120)), ref)
+
+
 def test_heightfield_kernel_bitexact(cuda):
     cfg = rb.configs.HeightfieldConfig()
     P = po.perm(cfg.seed)

@@ -159,6 +159,20 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   float4 A = __ldg(L), B = __ldg(L + 1);
   if (COUNT) c.leaf++;
   uint32_t first = __float_as_uint(B.z), count = __float_as_uint(B.w);
+  // exit face of the leaf box and the rope behind it, taken before the
+  // triangle tests so that the rope load overlaps them
+  float texit = __int_as_float(0x7f800000);
+  int face = -1;
+  {
+    float tk;
+    if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
+    else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
+    if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
+    else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
+    if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
+    else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
+  }
+  int32_t rope = face >= 0 ? __ldg(reinterpret_cast<const int32_t*>(L + 2) + face) : -1;
   for (uint32_t i = first; i < first + count; ++i) {
     const float4* T = kd.tris + 3 * (size_t)i;
     float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
@@ -180,17 +194,6 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
       }
     }
   }
-  float texit = __int_as_float(0x7f800000);
-  int face = -1;
-  {
-    float tk;
-    if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
-    else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
-    if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
-    else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
-    if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
-    else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
-  }
   if (face < 0) {
     s.live = false;
     return;
@@ -200,7 +203,6 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
     s.live = false;
     return;
   }
-  int32_t rope = __ldg(reinterpret_cast<const int32_t*>(L + 2) + face);
   if (rope < 0) {
     s.live = false;
     return;

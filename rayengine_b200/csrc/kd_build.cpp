@@ -469,7 +469,9 @@ bool build_kdtree(const float* tris, uint32_t num_tris, const re_kd_params& para
       N[1] = (uint32_t)n->axis | (n->child[0]->flat << 2);
       continue;
     }
-    N[0] = 0;
+    // first triangle reference, so traversal can fetch it with the leaf
+    // record; bit 31 marks an empty leaf (references stay below 2^31)
+    N[0] = n->tris.empty() ? (ref | 0x80000000u) : ref;
     N[1] = 3u | (n->leaf_index << 2);
     uint32_t* L = &out.leaves[16 * (size_t)n->leaf_index];
     std::memcpy(&L[0], n->box.lo, 12);

@@ -241,7 +241,7 @@ __device__ __forceinline__ void flush_counts(const Counters& c, uint32_t rays,
 // [2] secondary cursor, [3] secondary rays.  COUNT: also sum the traversal
 // work into totals[0..3].
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_ao_primary(KdDev kd, CamDev cam, AoDev ao, uint32_t w,
+__global__ void __launch_bounds__(256, 5) k_ao_primary(KdDev kd, CamDev cam, AoDev ao, uint32_t w,
                                                     uint32_t h, re_hit* __restrict__ out,
                                                     uint32_t* __restrict__ mask,
                                                     AoQueue aq, uint32_t* __restrict__ counters,

@@ -57,6 +57,8 @@ def test_tree_invariants(soup):
         L = nodes[i, 1] >> 2
         lo, hi = boxes[i]
         assert np.array_equal(lf[L, 0:3], lo) and np.array_equal(lf[L, 3:6], hi)
+        # a leaf node carries its first reference, bit 31 set for an empty leaf
+        assert nodes[i, 0] == leaves[L, 6] | (0x80000000 if leaves[L, 7] == 0 else 0)
         count = leaves[L, 7]
         assert count <= 8 or depth[i] == 24
         assert leaves[L, 14] == depth[i]

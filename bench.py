@@ -308,7 +308,7 @@ class SoupPrimary:
         self.cfg = cfg = rb.configs.SoupConfig(num_tris=num_tris)
         self.packed = cfg.packed()
         t0 = time.time()
-        self.scene = rb.KDScene.from_packed(self.packed)
+        self.scene = rb.KDScene.from_packed(self.packed, cfg.kd_params())
         self.build_s = time.time() - t0
         self.cam = cfg.camera()
         W, H = cfg.width, cfg.height

@@ -81,11 +81,11 @@ typedef struct re_ray {
 
 /* kd-tree build parameters (defaults from re_kd_params_default). */
 typedef struct re_kd_params {
-  uint32_t max_depth;      /* 24                                  */
-  uint32_t leaf_size;      /* 8: nodes above this size are split */
-  float cost_traversal;    /* SAH cost of one inner-node step     */
-  float cost_intersect;    /* SAH cost of one triangle test       */
-  float empty_bonus;       /* SAH discount for an empty child     */
+  uint32_t max_depth;      /* 40 (<= 64)                          */
+  uint32_t leaf_size;      /* 4: nodes above this size are split  */
+  float cost_traversal;    /* SAH cost of one inner-node step (1) */
+  float cost_intersect;    /* SAH cost of one triangle test (2)   */
+  float empty_bonus;       /* SAH discount for an empty child (0.1) */
   uint32_t bfs_levels;     /* top levels laid out breadth-first   */
   uint32_t threads;        /* host build threads, 0 = all         */
   uint32_t max_leaf_visits;/* per-ray traversal bound             */

@@ -40,6 +40,12 @@ class SoupConfig:
     def camera(self):
         return api.build_camera(self.campos, self.lookat, self.fov)
 
+    def kd_params(self):
+        """Tree parameters for random soups: leaves of up to 8 references
+        (their large overlapping triangles duplicate heavily when split
+        finer; measured on B200)."""
+        return api.kd_params(leaf_size=8)
+
     def packed(self) -> np.ndarray:
         v = api.triangle_soup(self.num_tris, self.seed)
         p = np.zeros((self.num_tris, 12), np.float32)
@@ -211,7 +217,7 @@ class BatchConfig:
             w, h = s["width"], s["height"]
             if s["kind"] == "soup":
                 sc = SoupConfig(num_tris=s["num_tris"], seed=s["seed"], width=w, height=h)
-                m = api.KDScene.from_packed(sc.packed())
+                m = api.KDScene.from_packed(sc.packed(), sc.kd_params())
                 meshes.append(m)
                 cam = api.build_camera(sc.campos, sc.lookat,
                                        (60.0, api.vertical_fov(60.0, w, h)))

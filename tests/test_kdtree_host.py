@@ -42,7 +42,7 @@ def region_boxes(st, nodes, leaves):
 @pytest.fixture(scope="module")
 def soup():
     packed = rb.configs.SoupConfig(num_tris=20000, seed=5).packed()
-    return packed, build(packed)
+    return packed, build(packed, leaf_size=8, max_depth=24)
 
 
 def test_tree_invariants(soup):

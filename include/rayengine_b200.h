@@ -82,7 +82,7 @@ typedef struct re_ray {
 /* kd-tree build parameters (defaults from re_kd_params_default). */
 typedef struct re_kd_params {
   uint32_t max_depth;      /* 40 (<= 64)                          */
-  uint32_t leaf_size;      /* 4: nodes above this size are split  */
+  uint32_t leaf_size;      /* 2: nodes above this size are split  */
   float cost_traversal;    /* SAH cost of one inner-node step (1) */
   float cost_intersect;    /* SAH cost of one triangle test (2)   */
   float empty_bonus;       /* SAH discount for an empty child (0.1) */

@@ -144,13 +144,10 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
     uint32_t k = nd.y & 3u;
     float split = __uint_as_float(nd.x);
     float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
-    bool left;
-    if (dk > 0.0f)
-      left = t_entry < (split - ok) * ik;
-    else if (dk < 0.0f)
-      left = t_entry >= (split - ok) * ik;
-    else
-      left = ok < split;
+    // branch-free form of: dk > 0: t_entry < ts; dk < 0: t_entry >= ts;
+    // dk == 0: ok < split (ts is computed but unused when dk == 0)
+    float ts = (split - ok) * ik;
+    bool left = dk > 0.0f ? (t_entry < ts) : (dk < 0.0f ? (t_entry >= ts) : (ok < split));
     node = (nd.y >> 2) + (left ? 0u : 1u);
     nd = load_node(kd, snodes, node);
     if (COUNT) c.inner++;
@@ -174,16 +171,20 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   uint32_t count = __float_as_uint(B.w);
   // exit face of the leaf box and the rope behind it, taken before the
   // triangle tests so that the rope load overlaps them
-  float texit = __int_as_float(0x7f800000);
+  // per axis the face the ray leaves through (+k when d.k > 0, -k when
+  // d.k < 0, none when d.k == 0: its distance is taken as +inf, which the
+  // strict comparisons below never accept), written with selects so that
+  // lanes of different direction signs do not diverge
+  const float kInf = __int_as_float(0x7f800000);
+  float texit = kInf;
   int face = -1;
   {
-    float tk;
-    if (d.x > 0.0f) { tk = (A.w - o.x) * inv.x; if (tk < texit) { texit = tk; face = 1; } }
-    else if (d.x < 0.0f) { tk = (A.x - o.x) * inv.x; if (tk < texit) { texit = tk; face = 0; } }
-    if (d.y > 0.0f) { tk = (B.x - o.y) * inv.y; if (tk < texit) { texit = tk; face = 3; } }
-    else if (d.y < 0.0f) { tk = (A.y - o.y) * inv.y; if (tk < texit) { texit = tk; face = 2; } }
-    if (d.z > 0.0f) { tk = (B.y - o.z) * inv.z; if (tk < texit) { texit = tk; face = 5; } }
-    else if (d.z < 0.0f) { tk = (A.z - o.z) * inv.z; if (tk < texit) { texit = tk; face = 4; } }
+    float tx = d.x != 0.0f ? ((d.x > 0.0f ? A.w : A.x) - o.x) * inv.x : kInf;
+    float ty = d.y != 0.0f ? ((d.y > 0.0f ? B.x : A.y) - o.y) * inv.y : kInf;
+    float tz = d.z != 0.0f ? ((d.z > 0.0f ? B.y : A.z) - o.z) * inv.z : kInf;
+    if (tx < texit) { texit = tx; face = d.x > 0.0f ? 1 : 0; }
+    if (ty < texit) { texit = ty; face = d.y > 0.0f ? 3 : 2; }
+    if (tz < texit) { texit = tz; face = d.z > 0.0f ? 5 : 4; }
   }
   int32_t rope = face >= 0 ? __ldg(reinterpret_cast<const int32_t*>(L + 2) + face) : -1;
   for (uint32_t i = first, end = first + count; i < end; ++i) {

@@ -49,27 +49,27 @@ __device__ __forceinline__ bool ray_box(V3 lo, V3 hi, V3 o, V3 inv, float& tn, f
 template <int MODE>
 __device__ __forceinline__ bool ray_tri(V3 o, V3 d, float4 T0, float4 T1, float4 T2,
                                         float& t, float& u, float& v) {
+  // The reference's early-out tests, evaluated as one predicate so that the
+  // lanes of a warp do not diverge on them; every value is computed exactly
+  // as in the early-out form (a division by a rejected determinant is
+  // computed and discarded).
   V3 v0 = {T0.x, T0.y, T0.z}, e1 = {T1.x, T1.y, T1.z}, e2 = {T2.x, T2.y, T2.z};
   V3 h = cross(d, e2);
   float a = dot(e1, h);
-  if (MODE == 0) {
-    if (a > -0.00001f && a < 0.00001f) return false;
-  } else {
-    if (a < 1e-4f) return false;
-  }
+  bool ok = MODE == 0 ? !(a > -0.00001f && a < 0.00001f) : !(a < 1e-4f);
   float f = 1.0f / a;
   V3 s = sub(o, v0);
   float uu = f * dot(s, h);
-  if (uu < 0.0f || uu > 1.0f) return false;
+  ok = ok & !(uu < 0.0f || uu > 1.0f);
   V3 q = cross(s, e1);
   float vv = f * dot(d, q);
-  if (vv < 0.0f || uu + vv > 1.0f) return false;
+  ok = ok & !(vv < 0.0f || uu + vv > 1.0f);
   float tt = f * dot(e2, q);
-  if (!(tt > (MODE == 0 ? 0.00001f : 1e-4f))) return false;
+  ok = ok & (tt > (MODE == 0 ? 0.00001f : 1e-4f));
   t = tt;
   u = uu;
   v = vv;
-  return true;
+  return ok;
 }
 
 struct HitState {

@@ -21,18 +21,28 @@ struct PermTable {
 
 // The table lives in shared memory once per lane: entry j of lane c is the
 // word 32*j + c, so a warp's 32 lookups (divergent lattice indices) always
-// fall in 32 different banks.  512 entries x 32 lanes x 4 B = 64 KB.
+// fall in 32 different banks.  512 entries x 32 lanes x 4 B = 64 KB.  Each
+// word holds P[j] in bits 0-7 and the gradient case of P[j] as the bit
+// 1 << (16 + (P[j] & 15)), so a corner's gradient lookup needs no decoding.
 constexpr uint32_t kPermSmemBytes = 512 * 32 * 4;
 
+__host__ __device__ __forceinline__ uint32_t perm_word(uint32_t p) {
+  return p | (1u << (16u + (p & 15u)));
+}
+
 __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
-  for (uint32_t i = threadIdx.x; i < 512 * 32; i += blockDim.x) s[i] = t.p[i >> 5];
+  for (uint32_t i = threadIdx.x; i < 512 * 32; i += blockDim.x) s[i] = perm_word(t.p[i >> 5]);
   __syncthreads();
 }
 
+// Permutation-table views: idx(j) = P[j] (a lattice index), grad(j) = the
+// gradient case bit of P[j] (1 << (16 + (P[j] & 15))).
 struct Perm {
   const uint32_t* __restrict__ s;
   uint32_t lane;
-  __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return s[(j << 5) + lane]; }
+  __device__ __forceinline__ uint32_t word(uint32_t j) const { return s[(j << 5) + lane]; }
+  __device__ __forceinline__ uint32_t idx(uint32_t j) const { return word(j) & 255u; }
+  __device__ __forceinline__ uint32_t grad(uint32_t j) const { return word(j); }
 };
 
 __device__ __forceinline__ Perm perm_view(const uint32_t* s) { return Perm{s, threadIdx.x & 31u}; }
@@ -41,7 +51,8 @@ __device__ __forceinline__ Perm perm_view(const uint32_t* s) { return Perm{s, th
 // may share banks).
 struct PermBytes {
   const uint8_t* __restrict__ s;
-  __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return s[j]; }
+  __device__ __forceinline__ uint32_t idx(uint32_t j) const { return s[j]; }
+  __device__ __forceinline__ uint32_t grad(uint32_t j) const { return perm_word(s[j]); }
 };
 
 // gradientDotV (sdf_functions.cuh:26-47) without branches: each case is a
@@ -51,12 +62,12 @@ struct PermBytes {
 //   first operand is y for cases 8-12, 14, 15 (x otherwise), negated for
 //   1, 3, 5, 7, 9, 11, 13, 14, 15; second operand is y for 0-3 and 13, x for
 //   12 (z otherwise), negated for 2, 3, 6, 7, 10, 11, 15.
-__device__ __forceinline__ float grad_dot(uint32_t h, float x, float y, float z) {
-  uint32_t b = 1u << (h & 15u);
-  float u = (b & 0xDF00u) ? y : x;
-  u = (b & 0xEAAAu) ? -u : u;
-  float v = (b & 0x200Fu) ? y : ((b & 0x1000u) ? x : z);
-  v = (b & 0x8CCCu) ? -v : v;
+// g: the case bit 1 << (16 + h) (a grad() lookup).
+__device__ __forceinline__ float grad_dot(uint32_t g, float x, float y, float z) {
+  float u = (g & (0xDF00u << 16)) ? y : x;
+  u = (g & (0xEAAAu << 16)) ? -u : u;
+  float v = (g & (0x200Fu << 16)) ? y : ((g & (0x1000u << 16)) ? x : z);
+  v = (g & (0x8CCCu << 16)) ? -v : v;
   return u + v;
 }
 
@@ -66,27 +77,30 @@ __device__ __forceinline__ float quintic(float t) {
   return ((t * t) * t) * in;
 }
 
-// PT: a permutation-table view with operator[] (Perm: per-lane shared
-// copies; PermBytes: one byte table).
+// PT: a permutation-table view with idx() and grad() (Perm: per-lane shared
+// copies; PermBytes: one byte table).  The table's second half repeats the
+// first (P[256 + i] = P[i], RPerlinNoise), so the upper lattice corners
+// index it with xi0 + 1 etc. unmasked, which reads the same entries as the
+// reference's (xi0 + 1) & 255.
 template <class PT>
 __device__ __forceinline__ float perlin(const PT& P, float x, float y, float z) {
   float fx = floorf(x), fy = floorf(y), fz = floorf(z);
   uint32_t xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
-  uint32_t xi1 = (xi0 + 1) & 255, yi1 = (yi0 + 1) & 255, zi1 = (zi0 + 1) & 255;
+  uint32_t xi1 = xi0 + 1, yi1 = yi0 + 1, zi1 = zi0 + 1;
   float tx = x - fx, ty = y - fy, tz = z - fz;
   float u = quintic(tx), v = quintic(ty), w = quintic(tz);
   float x1 = tx - 1.0f, y1 = ty - 1.0f, z1 = tz - 1.0f;
-  uint32_t px0 = P[xi0], px1 = P[xi1];
-  uint32_t p00 = P[px0 + yi0], p10 = P[px1 + yi0];
-  uint32_t p01 = P[px0 + yi1], p11 = P[px1 + yi1];
-  float a = grad_dot(P[p00 + zi0], tx, ty, tz);
-  float b = grad_dot(P[p10 + zi0], x1, ty, tz);
-  float c = grad_dot(P[p01 + zi0], tx, y1, tz);
-  float d = grad_dot(P[p11 + zi0], x1, y1, tz);
-  float e = grad_dot(P[p00 + zi1], tx, ty, z1);
-  float f = grad_dot(P[p10 + zi1], x1, ty, z1);
-  float g = grad_dot(P[p01 + zi1], tx, y1, z1);
-  float h = grad_dot(P[p11 + zi1], x1, y1, z1);
+  uint32_t px0 = P.idx(xi0), px1 = P.idx(xi1);
+  uint32_t p00 = P.idx(px0 + yi0), p10 = P.idx(px1 + yi0);
+  uint32_t p01 = P.idx(px0 + yi1), p11 = P.idx(px1 + yi1);
+  float a = grad_dot(P.grad(p00 + zi0), tx, ty, tz);
+  float b = grad_dot(P.grad(p10 + zi0), x1, ty, tz);
+  float c = grad_dot(P.grad(p01 + zi0), tx, y1, tz);
+  float d = grad_dot(P.grad(p11 + zi0), x1, y1, tz);
+  float e = grad_dot(P.grad(p00 + zi1), tx, ty, z1);
+  float f = grad_dot(P.grad(p10 + zi1), x1, ty, z1);
+  float g = grad_dot(P.grad(p01 + zi1), tx, y1, z1);
+  float h = grad_dot(P.grad(p11 + zi1), x1, y1, z1);
   float k1 = b - a;
   float k2 = c - a;
   float k3 = e - a;

@@ -193,6 +193,27 @@ def test_fbm_kernel_bitexact(cuda):
     assert np.array_equal(got, po.fbm_batch(po.perm(7), big, 8, scale=0.25, amp=3.0))
 
 
+def test_fbm_lattice_edges_bitexact(cuda):
+    """Points on and next to lattice planes (fractional parts 0 and just
+    below 1), at the 255/256 wrap of the table, negative, and with
+    coordinates of large magnitude: every corner case of the lattice
+    indexing and of the gradient selection, bit-exact against the oracle."""
+    rng = np.random.default_rng(11)
+    ints = rng.integers(-600, 600, (40000, 3)).astype(np.float32)
+    wrap = np.array([255.0, 256.0, -1.0, -256.0, 511.0, 512.0], np.float32)
+    ints[:6000] = rng.choice(wrap, (6000, 3))
+    below = np.nextafter(ints, np.float32(-np.inf))
+    above = np.nextafter(ints, np.float32(np.inf))
+    half = ints + np.float32(0.5)
+    large = rng.uniform(-1e6, 1e6, (20000, 3)).astype(np.float32)
+    pts = np.concatenate([ints, below, above, half, large, -ints]).astype(np.float32)
+    for seed, octaves in ((2016, 1), (3, 8)):
+        params = rb.fbm_params(seed=seed, octaves=octaves)
+        got = rb.generate_noise(params, torch.from_numpy(pts).cuda()).cpu().numpy()
+        assert np.array_equal(got.view(np.uint32),
+                              po.fbm_batch(po.perm(seed), pts, octaves).view(np.uint32)), seed
+
+
 def test_render_ao_small_bitexact(cuda):
     cfg = rb.configs.HeightfieldConfig(cells=128, width=320, height=180)
     P = po.perm(cfg.seed)

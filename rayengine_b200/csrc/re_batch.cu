@@ -239,10 +239,21 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
   uint32_t gpix = 0, scene = 0, bounce = 0, kind = kMesh;
   Trav tr;
   tr.live = false;
-  // terrain march state
-  float t = 0.f, v_hit = 0.f, delta = 0.f, plus = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
-  uint32_t steps = 0, mode = kMarch, tap = 0;
-  V3 p = {0.f, 0.f, 0.f};
+  // Terrain march state, kept in the Trav fields that a terrain ray leaves
+  // unused (its ray is tr.o / tr.d) so that it takes no registers of its
+  // own in this register-bound kernel: nx, ny, nz as float bits, the mode
+  // (bit 3) and the normal tap (bits 0-2) in one word.  Every field is set
+  // by a ray's start (trav_init or the terrain start below) before use.
+  float& t = tr.t_entry;
+  float& v_hit = tr.best_t;
+  float& delta = tr.best_u;
+  float& plus = tr.best_v;
+  V3& p = tr.inv;
+  uint32_t& steps = tr.visits;
+  uint32_t& mode_tap = tr.node;
+  uint32_t& nx_bits = tr.best_ref;
+  uint32_t& ny_bits = tr.best_leaf;
+  int32_t& nz_bits = tr.best_id;
   Counters cnt = {0, 0, 0, 0};
   uint32_t errors = 0;
   uint32_t fin_pending = 0;   // lane 0: finished rays in wfin
@@ -293,7 +304,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
           tr.d = d;
           t = 0.f;
           steps = 0;
-          mode = kMarch;
+          mode_tap = kMarch << 3;
         }
         state = kLive;
       } else {
@@ -372,7 +383,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
             tr.d = d;
             t = 0.f;
             steps = 0;
-            mode = kMarch;
+            mode_tap = kMarch << 3;
           }
           state = kLive;
         } else if (base + rank < B.qcap[src]) {
@@ -440,10 +451,11 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
         PermBytes P{sperm + 512u * S.perm_slot};
         for (uint32_t it = 0; it < B.steps_per_trip && !done; ++it) {
         V3 qp;
-        if (mode == kMarch) {
+        if ((mode_tap >> 3) == kMarch) {
           qp = v3(__fmaf_rn(t, tr.d.x, tr.o.x), __fmaf_rn(t, tr.d.y, tr.o.y),
                   __fmaf_rn(t, tr.d.z, tr.o.z));
         } else {
+          uint32_t tap = mode_tap & 7u;
           float sd = (tap & 1u) ? -delta : delta;
           qp = p;
           if (tap < 2) qp.x = p.x + sd;
@@ -452,14 +464,13 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
         }
         float v = terrain_density(P, qp, S.octaves, S.scale, S.amp);
         if (COUNT) ++cnt.status;  // field evaluations
-        if (mode == kMarch) {
+        if ((mode_tap >> 3) == kMarch) {
           ++steps;
           if (v < S.eps) {
             p = qp;
             v_hit = v;
             delta = fmaxf(0.002f * t, 1e-3f);
-            mode = kNormal;
-            tap = 0;
+            mode_tap = kNormal << 3;  // tap 0
           } else {
             t = __fmaf_rn(S.step_factor, v, t);
             // going up above the ceiling it can only miss: stop early (the
@@ -468,15 +479,18 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
               done = true;
           }
         } else {
+          uint32_t tap = mode_tap & 7u;
           if ((tap & 1u) == 0u) {
             plus = v;
           } else {
             float diff = plus - v;
-            if (tap == 1) nx = diff;
-            else if (tap == 3) ny = diff;
-            else nz = diff;
+            if (tap == 1) nx_bits = __float_as_uint(diff);
+            else if (tap == 3) ny_bits = __float_as_uint(diff);
+            else nz_bits = __float_as_int(diff);
           }
           if (tap == 5) {
+            float nx = __uint_as_float(nx_bits), ny = __uint_as_float(ny_bits),
+                  nz = __int_as_float(nz_bits);
             done = true;
             hit = true;
             hit_t = t;
@@ -487,7 +501,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
             float off = fmaxf(-v_hit, 0.0f) / (gl / (2.0f * delta)) + 2e-3f;
             hp = v3(__fmaf_rn(n.x, off, p.x), __fmaf_rn(n.y, off, p.y), __fmaf_rn(n.z, off, p.z));
           } else {
-            ++tap;
+            ++mode_tap;
           }
         }
         }

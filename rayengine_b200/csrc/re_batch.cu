@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
   const uint32_t nq = 2u * (B.depth - 1u);
   uint32_t* wfin = sfin + (threadIdx.x >> 5) * kMaxDepth;  // this warp's unpublished counts
 
-  uint32_t state = kIdle, pq = 0, pslot = 0, polls = 0;
+  uint32_t state = kIdle;
   uint32_t gpix = 0, scene = 0, bounce = 0, kind = kMesh;
   Trav tr;
   tr.live = false;
@@ -254,6 +254,12 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
   uint32_t& nx_bits = tr.best_ref;
   uint32_t& ny_bits = tr.best_leaf;
   int32_t& nz_bits = tr.best_id;
+  // A pending claim (queue, slot, polls so far) likewise: a lane waiting
+  // for its record has no ray yet, and the ray's start overwrites these
+  // fields only after the record has been read.
+  uint32_t& pq = tr.best_ref;
+  uint32_t& pslot = tr.best_leaf;
+  uint32_t& polls = tr.visits;
   Counters cnt = {0, 0, 0, 0};
   uint32_t errors = 0;
   uint32_t fin_pending = 0;   // lane 0: finished rays in wfin

@@ -97,7 +97,7 @@ struct __align__(16) SceneDev {
 
 struct BatchDev {
   const SceneDev* scenes;
-  const uint8_t* perms;  // perm_count tables of 512 bytes
+  const uint8_t* perms;  // perm_count tables of 512 bytes (words in shared memory)
   uint32_t num_scenes, perm_count, stage_total, total_pixels;
   uint32_t depth, seed, refill_min, steps_per_trip;
   float mesh_bias;
@@ -212,7 +212,7 @@ template <bool COUNT>
 __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_batch(BatchDev B) {
   extern __shared__ uint4 smem_u4[];
   SceneDev* sc = reinterpret_cast<SceneDev*>(smem_u4);
-  uint8_t* sperm = reinterpret_cast<uint8_t*>(sc + B.num_scenes);
+  uint32_t* sperm = reinterpret_cast<uint32_t*>(sc + B.num_scenes);
   uint2* snodes = reinterpret_cast<uint2*>(sperm + 512u * B.perm_count);
   uint32_t* sfin = reinterpret_cast<uint32_t*>(snodes + B.stage_total);  // [warp][bounce]
   {
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
     uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
     for (uint32_t i = threadIdx.x; i < B.num_scenes * (uint32_t)(sizeof(SceneDev) / 4); i += blockDim.x)
       dst[i] = src[i];
-    for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) sperm[i] = B.perms[i];
+    for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) sperm[i] = perm_word(B.perms[i]);
     for (uint32_t i = threadIdx.x; i < (blockDim.x / 32u) * kMaxDepth; i += blockDim.x) sfin[i] = 0u;
     __syncthreads();
     for (uint32_t s = 0; s < B.num_scenes; ++s)
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
           }
         }
       } else {
-        PermBytes P{sperm + 512u * S.perm_slot};
+        PermWords P{sperm + 512u * S.perm_slot};
         for (uint32_t it = 0; it < B.steps_per_trip && !done; ++it) {
         V3 qp;
         if ((mode_tap >> 3) == kMarch) {
@@ -669,7 +669,7 @@ uint32_t layout_stage(re_batch* b, uint32_t stage_nodes) {
 }
 
 size_t smem_bytes(const re_batch* b, uint32_t stage_total, uint32_t block_threads) {
-  return b->num_scenes * sizeof(SceneDev) + 512u * (b->perms.size() / 512) +
+  return b->num_scenes * sizeof(SceneDev) + 4u * 512u * (b->perms.size() / 512) +
          (size_t)stage_total * sizeof(uint2) + (size_t)(block_threads / 32) * kMaxDepth * 4;
 }
 

@@ -634,7 +634,7 @@ void o_secondary_rays(const float hitp[3], const float n[3], uint32_t seed,
   }
 }
 
-/* ------------------------------------------------------- FP64 judge */
+/* ------------------------------------------------------- FP64 arbiter */
 /* The same lattice noise in double precision (exact quintic and trilinear
  * polynomial), for the error of float hit positions. */
 static double quintic_d(double t) { return t * t * t * (t * (t * 6.0 - 15.0) + 10.0); }

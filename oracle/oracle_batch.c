@@ -210,9 +210,9 @@ int o_sdf_root_d(const uint32_t P[512], const float o[3], const float d[3], int 
                  double scale, double amp, double factor, double tmax, int max_steps,
                  int refine, double pos[3], double* t_out);
 
-/* FP64 judge over pixels: out[i] = {x, y, z, hit} of the surface point
+/* FP64 arbiter over pixels: out[i] = {x, y, z, hit} of the surface point
  * (refine != 0: bisected root of the first crossing the march reaches). */
-void o_batch_sdf_judge(const uint32_t perm[512], const o_camera* cam, uint32_t w, uint32_t h,
+void o_batch_sdf_arbiter(const uint32_t perm[512], const o_camera* cam, uint32_t w, uint32_t h,
                        int octaves, double scale, double amp, double factor, double tmax,
                        int max_steps, int refine, const uint32_t* pixels, int64_t npix,
                        double* out, int threads) {

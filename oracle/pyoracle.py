@@ -201,7 +201,7 @@ def hash_u32(a, b, c) -> int:
     return lib().o_hash_u32(a, b, c)
 
 
-# ---------------------------------------------------------- FP64 judge
+# ---------------------------------------------------------- FP64 arbiter
 def edge_margin(packed, ids, o, d):
     """Barycentric margin min(u, v, 1-u-v) of the ray against triangle ids,
     in float64 (the relative edge distance used to exempt grazing rays)."""
@@ -221,7 +221,7 @@ def edge_margin(packed, ids, o, d):
 
 
 def camera_rays(cam, w, h, pixels):
-    """Float64 ray origins/directions of the given pixels (judge only)."""
+    """Float64 ray origins/directions of the given pixels (arbiter only)."""
     campos = np.array(cam.campos, np.float64)
     view = np.array(cam.view, np.float64)
     view /= np.linalg.norm(view)
@@ -323,7 +323,7 @@ def frame_ao_bruteforce(packed, bmin, bmax, cam, w, h, light_dir, ao_length, bia
     return n + nsec.value
 
 
-def sdf_judge(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6, tmax=200.0,
+def sdf_arbiter(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6, tmax=200.0,
               max_steps=4096, refine=True, nthreads=0):
     """FP64 surface points of the given pixels' rays: (n, 3) positions and a hit mask.
 
@@ -332,26 +332,26 @@ def sdf_judge(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6, 
     pix = np.ascontiguousarray(pixels, np.uint32)
     out = np.zeros((pix.shape[0], 4), np.float64)
     oc = camera(cam)
-    lib().o_batch_sdf_judge(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+    lib().o_batch_sdf_arbiter(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
                             ctypes.c_int(octaves), ctypes.c_double(scale), ctypes.c_double(amp),
                             ctypes.c_double(factor), ctypes.c_double(tmax), ctypes.c_int(max_steps),
                             ctypes.c_int(1 if refine else 0), _p(pix), ctypes.c_int64(pix.shape[0]), _p(out), ctypes.c_int(nthreads))
     return out[:, :3], out[:, 3] > 0.5
 
 
-def hit_errors(sdf_out, judge_pos, judge_hit, pixels):
+def hit_errors(sdf_out, arbiter_pos, arbiter_hit, pixels):
     """Per-pixel |p_gpu - p_fp64| where both hit, plus hit/miss disagreements."""
     o = np.asarray(sdf_out)
     f = o.view(np.float32).reshape(-1, 8)[pixels]
     status = o.view(np.uint32).reshape(-1, 8)[pixels, 7]
     gpu_hit = status == 1
-    both = gpu_hit & judge_hit
-    err = np.linalg.norm(f[both, 0:3].astype(np.float64) - judge_pos[both], axis=1)
-    return err, int((gpu_hit != judge_hit).sum()), int(both.sum())
+    both = gpu_hit & arbiter_hit
+    err = np.linalg.norm(f[both, 0:3].astype(np.float64) - arbiter_pos[both], axis=1)
+    return err, int((gpu_hit != arbiter_hit).sum()), int(both.sum())
 
 
 def density_d(p, pts, octaves=8, scale=0.25, amp=3.0, nthreads=0):
-    """FP64 terrain density p.y - amp * fbm(scale * p) (the judge's field)."""
+    """FP64 terrain density p.y - amp * fbm(scale * p) (the arbiter's field)."""
     pts = np.ascontiguousarray(pts, np.float64)
     out = np.zeros(pts.shape[0], np.float64)
     lib().o_batch_density_d(_p(p), _p(pts), ctypes.c_int64(pts.shape[0]), ctypes.c_int(octaves),

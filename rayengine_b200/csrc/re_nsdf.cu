@@ -2,7 +2,7 @@
 //
 // The reference has no learned component.  The network stands in for the
 // fBm terrain density (sdf_functions.cuh:147-206, d(p) = p.y - 3 fBm(p/4) in
-// the configs) during sphere tracing; the exact field stays the judge and
+// the configs) during sphere tracing; the exact field stays the arbiter and
 // finishes every hit (sphere_tracing.cuh:183-216 restated in re_noise.cu).
 //
 //   data      k_nsdf_data: 50% points uniform in the view box, 50% near the

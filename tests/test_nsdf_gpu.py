@@ -106,7 +106,7 @@ def test_training_reduces_loss_and_checkpoints(cuda):
 
 def _sdf_errors(out, tc, pix):
     P = po.perm(tc.seed)
-    jpos, jhit = po.sdf_judge(P, tc.camera(), tc.width, tc.height, pix)
+    jpos, jhit = po.sdf_arbiter(P, tc.camera(), tc.width, tc.height, pix)
     return po.hit_errors(out, jpos, jhit, pix)
 
 

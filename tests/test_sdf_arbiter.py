@@ -1,6 +1,6 @@
-"""The FP64 judge of SDF hit positions (oracle) on the exact-SDF terrain.
+"""The FP64 arbiter of SDF hit positions (oracle) on the exact-SDF terrain.
 
-The judge marches the same rule as the float tracer (t += 0.6 d) in double
+The arbiter marches the same rule as the float tracer (t += 0.6 d) in double
 precision and bisects the first crossing it reaches to the density's root.
 Without the bisection it reproduces the float march to rounding; with it,
 it measures how far the 0.6-step march ends inside the terrain.
@@ -23,13 +23,13 @@ def _setup(n=3000):
     return tc, P, cam, pix, arr.view(np.int32)
 
 
-def test_judge_reproduces_the_float_march_and_finds_roots():
+def test_arbiter_reproduces_the_float_march_and_finds_roots():
     tc, P, cam, pix, out = _setup()
-    pos, hit = po.sdf_judge(P, cam, tc.width, tc.height, pix, refine=False)
+    pos, hit = po.sdf_arbiter(P, cam, tc.width, tc.height, pix, refine=False)
     err, mism, both = po.hit_errors(out, pos, hit, pix)
     assert mism == 0 and both > 0.8 * len(pix)
     assert np.median(err) < 1e-5
-    rpos, rhit = po.sdf_judge(P, cam, tc.width, tc.height, pix, refine=True)
+    rpos, rhit = po.sdf_arbiter(P, cam, tc.width, tc.height, pix, refine=True)
     assert np.array_equal(rhit, hit)
     # the bisected points are on the surface
     d = po.density_d(P, rpos[rhit])
@@ -41,7 +41,7 @@ def test_exact_march_overshoots_the_surface():
     # the float tracer stops inside the terrain: its median error against
     # the root is well above 1e-3 scene units
     tc, P, cam, pix, out = _setup()
-    rpos, rhit = po.sdf_judge(P, cam, tc.width, tc.height, pix, refine=True)
+    rpos, rhit = po.sdf_arbiter(P, cam, tc.width, tc.height, pix, refine=True)
     err, mism, both = po.hit_errors(out, rpos, rhit, pix)
     assert mism == 0
     assert np.median(err) > 2e-3

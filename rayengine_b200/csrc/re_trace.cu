@@ -573,7 +573,8 @@ RE_API void re_kd_params_default(re_kd_params* p) {
   // Measured on B200 (AO frame of the 2.1M-triangle heightfield, primary
   // pass of 2^16- and 2^20-triangle soups): depth 24 cut the heightfield
   // tree short (+18 % frame time against depth >= 28); splitting down to
-  // leaves of <= 2 references (SAH permitting) with an empty-side bonus of
+  // leaves of <= 2 references (splits stop early only when a side does not
+  // shrink or the reference budget is spent) with an empty-side bonus of
   // 0.1 gave the fastest heightfield frame (3.14 ms; leaves of 4: 3.24 ms;
   // depth 24, leaf 8, bonus 0.2: 3.91 ms).  Random soups of large
   // overlapping triangles prefer leaves of 8 (finer splits duplicate

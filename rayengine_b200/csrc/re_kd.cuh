@@ -169,12 +169,12 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   float4 A = __ldg(L), B = __ldg(L + 1);
   if (COUNT) c.leaf++;
   uint32_t count = __float_as_uint(B.w);
-  // exit face of the leaf box and the rope behind it, taken before the
-  // triangle tests so that the rope load overlaps them
-  // per axis the face the ray leaves through (+k when d.k > 0, -k when
-  // d.k < 0, none when d.k == 0: its distance is taken as +inf, which the
-  // strict comparisons below never accept), written with selects so that
-  // lanes of different direction signs do not diverge
+  // The exit face of the leaf box and the rope behind it are taken before
+  // the triangle tests, so that the rope load overlaps them.  Per axis the
+  // ray leaves through +k when d.k > 0 and -k when d.k < 0; an axis with
+  // d.k == 0 gets the distance +inf, which the strict comparisons below
+  // never accept.  Written with selects so that lanes of different
+  // direction signs do not diverge.
   const float kInf = __int_as_float(0x7f800000);
   float texit = kInf;
   int face = -1;

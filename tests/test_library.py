@@ -69,3 +69,25 @@ def test_host_only_scene_refuses_to_trace():
                   8, 8, 0, ctypes.c_void_p(16), None)
     assert e.value.status == 5
     sc.close()
+
+
+def test_plain_c_caller(tmp_path):
+    """The header compiles as C11 and a C program drives the host-only
+    entry points through the shared library (the ABI a C or FFI caller
+    binds)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(root, "rayengine_b200")
+    exe = str(tmp_path / "host_only")
+    subprocess.run([gcc, "-std=c11", "-Wall", "-Werror", "-O1",
+                    "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "c_abi", "host_only.c"),
+                    "-L", lib_dir, "-lrayengine_b200", "-Wl,-rpath," + lib_dir, "-o", exe],
+                   check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr

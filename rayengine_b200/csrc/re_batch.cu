@@ -208,19 +208,28 @@ __device__ __forceinline__ uint32_t closed_mask(const uint32_t* ctr, const Batch
 #define RE_BATCH_MAX_THREADS 256
 #endif
 
-template <bool COUNT>
+// WORDS: the terrain permutation tables in shared memory as perm_word()
+// entries (2 KB per seed), else as bytes (512 B per seed; batches with
+// more than kWordTablesMax seeds, where word tables would cost blocks per SM).
+template <bool COUNT, bool WORDS>
 __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_batch(BatchDev B) {
   extern __shared__ uint4 smem_u4[];
   SceneDev* sc = reinterpret_cast<SceneDev*>(smem_u4);
-  uint32_t* sperm = reinterpret_cast<uint32_t*>(sc + B.num_scenes);
-  uint2* snodes = reinterpret_cast<uint2*>(sperm + 512u * B.perm_count);
+  uint8_t* sperm = reinterpret_cast<uint8_t*>(sc + B.num_scenes);
+  uint32_t* sperm_w = reinterpret_cast<uint32_t*>(sperm);
+  uint2* snodes = reinterpret_cast<uint2*>(sperm + (WORDS ? 4u : 1u) * 512u * B.perm_count);
   uint32_t* sfin = reinterpret_cast<uint32_t*>(snodes + B.stage_total);  // [warp][bounce]
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(B.scenes);
     uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
     for (uint32_t i = threadIdx.x; i < B.num_scenes * (uint32_t)(sizeof(SceneDev) / 4); i += blockDim.x)
       dst[i] = src[i];
-    for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) sperm[i] = perm_word(B.perms[i]);
+    for (uint32_t i = threadIdx.x; i < 512u * B.perm_count; i += blockDim.x) {
+      if (WORDS)
+        sperm_w[i] = perm_word(B.perms[i]);
+      else
+        sperm[i] = B.perms[i];
+    }
     for (uint32_t i = threadIdx.x; i < (blockDim.x / 32u) * kMaxDepth; i += blockDim.x) sfin[i] = 0u;
     __syncthreads();
     for (uint32_t s = 0; s < B.num_scenes; ++s)
@@ -454,7 +463,12 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
           }
         }
       } else {
-        PermWords P{sperm + 512u * S.perm_slot};
+        const auto P = [&] {
+          if constexpr (WORDS)
+            return PermWords{sperm_w + 512u * S.perm_slot};
+          else
+            return PermBytes{sperm + 512u * S.perm_slot};
+        }();
         for (uint32_t it = 0; it < B.steps_per_trip && !done; ++it) {
         V3 qp;
         if ((mode_tap >> 3) == kMarch) {
@@ -668,8 +682,13 @@ uint32_t layout_stage(re_batch* b, uint32_t stage_nodes) {
   return off;
 }
 
+// Word tables while the batch has at most this many terrain seeds (32 KB).
+constexpr uint32_t kWordTablesMax = 16;
+
+bool word_tables(const re_batch* b) { return b->perms.size() / 512 <= kWordTablesMax; }
+
 size_t smem_bytes(const re_batch* b, uint32_t stage_total, uint32_t block_threads) {
-  return b->num_scenes * sizeof(SceneDev) + 4u * 512u * (b->perms.size() / 512) +
+  return b->num_scenes * sizeof(SceneDev) + (word_tables(b) ? 4u : 1u) * b->perms.size() +
          (size_t)stage_total * sizeof(uint2) + (size_t)(block_threads / 32) * kMaxDepth * 4;
 }
 
@@ -680,10 +699,11 @@ re_status prepare(re_batch* b, const re_batch_tuning& tn, cudaStream_t st) {
   RE_CUDA(cudaMemcpyAsync(b->d_scenes, b->host_scenes.data(), b->num_scenes * sizeof(SceneDev),
                           cudaMemcpyHostToDevice, st));
   RE_CUDA(cudaStreamSynchronize(st));
-  RE_CUDA(cudaFuncSetAttribute(k_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes(b, stage_total, 512)));
-  RE_CUDA(cudaFuncSetAttribute(k_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes(b, stage_total, 512)));
+  int bytes = (int)smem_bytes(b, stage_total, 512);
+  RE_CUDA(cudaFuncSetAttribute(k_batch<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RE_CUDA(cudaFuncSetAttribute(k_batch<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RE_CUDA(cudaFuncSetAttribute(k_batch<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RE_CUDA(cudaFuncSetAttribute(k_batch<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   return RE_OK;
 }
 
@@ -693,7 +713,8 @@ re_status launch(re_batch* b, float* d_radiance, re_hit* d_primary, cudaStream_t
   uint32_t stage_total = layout_stage(b, tn.stage_nodes);
   size_t smem = smem_bytes(b, stage_total, tn.block_threads);
   int per_sm = 0;
-  auto kern = totals ? k_batch<true> : k_batch<false>;
+  auto kern = word_tables(b) ? (totals ? k_batch<true, true> : k_batch<false, true>)
+                             : (totals ? k_batch<true, false> : k_batch<false, false>);
   RE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)tn.block_threads,
                                                         smem));
   if (per_sm < 1) return fail(RE_ERR_LIMIT, "re_batch: tuning does not fit on an SM");

@@ -50,13 +50,20 @@ struct Perm {
 
 __device__ __forceinline__ Perm perm_view(const uint32_t* s) { return Perm{s, threadIdx.x & 15u}; }
 
-// One shared table of perm_word() entries for several tables side by side
-// (the batched renderer: 2 KB per terrain seed, no per-lane copies; lookups
-// may share banks).  Measured 4 % faster on the batch than byte tables.
+// Single shared tables for several seeds side by side (the batched
+// renderer; no per-lane copies, lookups may share banks): perm_word()
+// entries, 2 KB per seed (measured 4 % faster on the batch), or plain bytes,
+// 512 B per seed, for batches with many seeds.
 struct PermWords {
   const uint32_t* __restrict__ s;
   __device__ __forceinline__ uint32_t idx(uint32_t j) const { return s[j] & 255u; }
   __device__ __forceinline__ uint32_t grad(uint32_t j) const { return s[j]; }
+};
+
+struct PermBytes {
+  const uint8_t* __restrict__ s;
+  __device__ __forceinline__ uint32_t idx(uint32_t j) const { return s[j]; }
+  __device__ __forceinline__ uint32_t grad(uint32_t j) const { return perm_word(s[j]); }
 };
 
 // gradientDotV (sdf_functions.cuh:26-47) without branches: each case is a

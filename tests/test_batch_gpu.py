@@ -125,3 +125,28 @@ def test_graph_replay_and_tunings_give_identical_frames(cuda):
             b.set_tuning(512, 8, 0)
     for m in meshes:
         m.close()
+
+
+def test_batch_with_many_terrain_seeds_bit_exact(cuda):
+    """More distinct terrain seeds than the word-table limit (16): the
+    kernel keeps its noise tables as bytes; the frame must still match the
+    oracle bit for bit."""
+    specs, meshes = [], []
+    packed = _soup(3000, 9)
+    sc = rb.KDScene.from_packed(packed)
+    meshes.append(sc)
+    w, h = 24, 16
+    cam = rb.build_camera((0, 0, 3), (0, 0, 0), (60.0, rb.vertical_fov(60.0, w, h)))
+    specs.append(dict(mesh=sc, packed=packed, camera=cam, width=w, height=h, albedo=0.7))
+    for i in range(18):
+        tc = rb.configs.TerrainConfig(seed=100 + i, amplitude=1.5 + 0.1 * i, width=16, height=10)
+        specs.append(dict(terrain=tc.params(), tc=tc, camera=tc.camera(), width=16, height=10,
+                          albedo=0.6))
+    with rb.Batch(specs, max_depth=DEPTH, seed=SEED, mesh_bias=BIAS) as b:
+        rad = b.render().cpu().numpy()
+        assert b.stats()["error"] == 0
+        orad, _, _ = _oracle(specs, b)
+        assert np.array_equal(rad.view(np.uint32), orad.view(np.uint32))
+        assert np.array_equal(b.render(graph=True).cpu().numpy(), rad)
+    for m in meshes:
+        m.close()

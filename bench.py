@@ -8,15 +8,25 @@ cosine-weighted AO rays (length 1) per primary hit.  Metric: Mrays/s over all
 rays traced in the frame.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config heightfield_ao|soup|soup1m|terrain_sdf]
+                    [--config heightfield_ao|soup|soup1m|terrain_sdf|nsdf_terrain|batch32]
+                    [--tree tuned|configured]
+
+The mesh workloads run over the library's B200-tuned kd-tree; the same
+frame over the tree the configuration names (SAH, depth <= 24, leaf <= 8)
+is timed after the headline and reported under "configured_tree" (hits do
+not depend on the tree).  On one GPU the line also carries the CPU baseline
+(the oracle's traversal of the same tree on all host cores) and "parity",
+the checker's comparison of the last frame with the oracle and with the
+reference as shipped.
 
 Under torchrun (N > 1) every rank holds a replica of the scene and renders
 its own frame (rays are independent, nothing is exchanged): weak scaling,
 value = rays of all ranks / the slowest rank's time.  Rank 0 prints one JSON
-line.  `--impl reference` times the reference's own CPU path (its compiled
-kd-tree builder, which ships as a single leaf, plus its traversal restated on
-the host: brute-force Moller-Trumbore) on all host cores over a bounded pixel
-sample of the same frame.
+line.  `--impl reference` times the reference's own CPU path on all host
+cores over a bounded pixel sample of the same frame: for meshes its
+RKDTreeCPU and CPU ray query compiled from its sources (the tree ships as a
+single leaf, so every query is brute-force Moller-Trumbore); for the SDF
+and batch workloads the oracle's restatement of its march.
 """
 from __future__ import annotations
 
@@ -171,15 +181,95 @@ def measure_l2_gbs(torch) -> float:
 
 def hbm_roofline(wl, phase_ms, peaks):
     ab = wl.alg_bytes()
+    lb = wl.layout_bytes() if hasattr(wl, "layout_bytes") else {}
     dom = max(phase_ms, key=phase_ms.get)
     achieved = ab[dom] / (phase_ms[dom] / 1e3) / 1e9
     out = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
            "peak_source": peaks["source"], "alg_bytes_per_launch": ab[dom],
+           "alg_bytes_model": "per ray 16 (hit) + 16/inner node + 48/leaf + 4/reference + "
+                              "48/triangle test (+32 per stored ray)",
            "traffic": ncu_traffic(f"{wl.name}:{dom}")}
+    if dom in lb:
+        out["layout_bytes_per_launch"] = lb[dom]
     if peaks.get("l2_gbs"):
         out["l2"] = {"peak": peaks["l2_gbs"], "frac": round(achieved / peaks["l2_gbs"], 4),
                      "peak_source": "measured in this run (re_measure_l2_read)"}
+    return out
+
+
+def survey_bytes(rays, inner, leaf, tests, stored=0):
+    """Algorithmic bytes of a traversal launch: 16 (hit out) per ray, 16 per
+    inner-node visit, 48 per leaf visit (24-byte box + 24-byte ropes), 4 per
+    triangle reference read and 48 per triangle test, plus 32 per stored ray
+    read or written.  The visit and test counts are the traversal's own
+    (equal to the oracle's walk of the same tree on the same rays)."""
+    return 16 * rays + 16 * inner + 48 * leaf + 52 * tests + 32 * stored
+
+
+def layout_bytes(rays, inner, leaf, tests, stored=0, hit_bytes=16):
+    """Bytes the kernels' own records move: 8 per inner node, 36 per leaf
+    (32-byte box and range, 4-byte rope), 48 per triangle reference (with
+    its vertex data), plus the hit records and stored rays."""
+    return hit_bytes * rays + 8 * inner + 36 * leaf + 48 * tests + 32 * stored
+
+
+def kd_description(params, choice):
+    return {"max_depth": params.max_depth, "leaf_size": params.leaf_size,
+            "empty_bonus": round(params.empty_bonus, 4),
+            "cost_traversal": params.cost_traversal, "cost_intersect": params.cost_intersect,
+            "choice": choice}
+
+
+CONFIGURED_TREE = dict(max_depth=24, leaf_size=8)  # configs 0/1: SAH, depth <= 24, leaf <= 8
+
+
+def hit_parity(got, packed, st, kd, cam, W, H, pix_kd, pix_ref, ref_mesh=None):
+    """Checker (oracle) comparison of a primary pass's hits `got` (W*H, 4 int32):
+    bit-exact against the oracle's walk of the same tree on pix_kd; against the
+    reference as shipped (brute force in index order, strict <) on pix_ref with
+    the FP64 edge-margin rule; and, when ref_mesh = (verts, faces) is given,
+    hit/miss and t against the reference's own compiled CPU query."""
+    from oracle import pyoracle as po
+
+    out = {}
+    ref = po.primary_kd(kd, cam, W, H, pixels=pix_kd)
+    g = got[pix_kd]
+    out["vs_oracle_same_tree"] = {"rays": int(pix_kd.size),
+                                  "bitexact": int((g == ref.view(np.int32).reshape(-1, 4)).all(1).sum())}
+    bf = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, W, H, pixels=pix_ref)
+    g = got[pix_ref]
+    gid, bid = g[:, 0], bf["id"]
+    diff = np.nonzero(gid != bid)[0]
+    exempt = 0
+    if diff.size:
+        o, d = po.camera_rays(cam, W, H, pix_ref[diff])
+        m = np.full(diff.size, np.inf)
+        for ids in (gid[diff], bid[diff]):
+            ok = ids >= 0
+            m[ok] = np.minimum(m[ok], po.edge_margin(packed, ids[ok], o[ok], d[ok]))
+        exempt = int((m < 1e-6).sum())
+    same = (gid == bid) & (bid >= 0)
+    gf = g[same, 1:].view(np.float32)
+    bv = np.stack([bf["t"], bf["u"], bf["v"]], 1)[same]
+    rel = np.abs(gf - bv) / np.maximum(np.abs(bv), 1e-3)
+    out["vs_reference_as_shipped"] = {
+        "rays": int(pix_ref.size), "hits": int((bid >= 0).sum()), "id_mismatch": int(diff.size),
+        "id_mismatch_edge_exempt": exempt, "max_rel_tuv": float(rel.max(initial=0.0)),
+        "rule": "ids equal except rays whose FP64 edge margin < 1e-6; t, u, v within 1e-5 relative"}
+    if ref_mesh is not None and po.ref_lib() is not None:
+        tree = po.RefTree(*ref_mesh)
+        o, d = po.camera_rays(cam, W, H, pix_ref)
+        t, _, _ = tree.trace(o, d)
+        tree.close()
+        rh = t < 1e19
+        gh = g[:, 0] >= 0
+        both = rh & gh
+        gt = g[both, 1].view(np.float32)
+        out["vs_reference_compiled_query"] = {
+            "rays": int(pix_ref.size), "hit_miss_disagree": int((rh != gh).sum()),
+            "max_rel_t": float((np.abs(gt - t[both]) / np.abs(t[both])).max(initial=0.0)),
+            "what": "RKDTreeCPU::singleRayStacklessIntersect compiled from the reference's sources"}
     return out
 
 
@@ -198,14 +288,23 @@ class HeightfieldAO:
 
     name = "heightfield_ao"
 
-    def __init__(self, torch):
+    def __init__(self, torch, tree="tuned", mesh=None):
         import rayengine_b200 as rb
 
         self.rb = rb
+        self.tree = tree
         self.cfg = cfg = rb.configs.HeightfieldConfig()
-        self.verts, self.faces = cfg.mesh_on_device()
+        self.verts, self.faces = mesh if mesh is not None else cfg.mesh_on_device()
+        if tree == "configured":
+            self.kd = rb.kd_params(**CONFIGURED_TREE)
+            choice = "as configured: SAH, depth <= 24, leaf <= 8 (library defaults for the rest)"
+        else:
+            self.kd = rb.kd_params()
+            choice = ("tuned on B200 (library default); hits do not depend on the tree, "
+                      "see configured_tree for the configured one")
+        self.kd_desc = kd_description(self.kd, choice)
         t0 = time.time()
-        self.scene = rb.KDScene.from_mesh(self.verts, self.faces)
+        self.scene = rb.KDScene.from_mesh(self.verts, self.faces, self.kd)
         self.build_s = time.time() - t0
         self.cam = cfg.camera()
         self.params = rb.ao_params(cfg.light_dir, cfg.ao_length, cfg.bias, cfg.ao_seed)
@@ -226,7 +325,8 @@ class HeightfieldAO:
                             "primary + 1 shadow + 4 AO rays per hit",
                 "triangles": st["num_tris"], "kd_nodes": st["num_nodes"],
                 "kd_leaves": st["num_leaves"], "kd_refs": st["num_refs"],
-                "kd_build_s": round(self.build_s, 3), "image": [c.width, c.height],
+                "kd_build_s": round(self.build_s, 3), "kd_tree": self.kd_desc,
+                "image": [c.width, c.height],
                 "rays_per_step": self.rays_per_step,
                 "secondary_rays_per_step": self.counts["secondary"]["rays"],
                 "work_per_ray": {
@@ -244,14 +344,48 @@ class HeightfieldAO:
         ]
 
     def alg_bytes(self):
-        """Algorithmic bytes per launch of each kernel: 8 B per inner-node step, 36 B per leaf visit (32 B box+range, 4 B
-        rope), 48 B per triangle test, 16 B hit + 4 B mask per primary ray,
-        32 B per queued secondary ray (written by the primary pass, read by
-        the secondary pass)."""
+        """Algorithmic bytes per launch (survey_bytes): the primary pass also
+        stores the five secondary rays of every hit, the secondary pass reads
+        them."""
         p, s = self.counts["primary"], self.counts["secondary"]
-        prim = 20 * p["rays"] + 8 * p["inner"] + 36 * p["leaf"] + 48 * p["tests"] + 32 * s["rays"]
-        sec = 32 * s["rays"] + 8 * s["inner"] + 36 * s["leaf"] + 48 * s["tests"]
-        return {"ao_primary": prim, "ao_secondary": sec}
+        return {"ao_primary": survey_bytes(p["rays"], p["inner"], p["leaf"], p["tests"], s["rays"]),
+                "ao_secondary": survey_bytes(s["rays"], s["inner"], s["leaf"], s["tests"], s["rays"])}
+
+    def layout_bytes(self):
+        p, s = self.counts["primary"], self.counts["secondary"]
+        return {"ao_primary": layout_bytes(p["rays"], p["inner"], p["leaf"], p["tests"], s["rays"], 20),
+                "ao_secondary": layout_bytes(0, s["inner"], s["leaf"], s["tests"], s["rays"])}
+
+    def configured_variant(self, torch):
+        """The same frame over the configured tree (depth 24, leaf 8)."""
+        if self.tree == "configured":
+            return None
+        return HeightfieldAO(torch, tree="configured", mesh=(self.verts, self.faces))
+
+    def parity(self):
+        """Checker comparison of the bench's last frame (see hit_parity)."""
+        from oracle import pyoracle as po
+
+        st = self.scene.stats()
+        nodes, leaves, tris = self.scene.export()
+        kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+        packed = self.rb.pack_triangles(self.verts, self.faces)
+        W, H = self.cfg.width, self.cfg.height
+        got = self.primary.cpu().numpy().reshape(-1, 4)
+        mask = self.mask.cpu().numpy().view(np.uint32)
+        rng = np.random.default_rng(12)
+        pix = rng.choice(W * H, 4000, replace=False).astype(np.uint32)
+        light = self.rb.unit(self.cfg.light_dir)
+        rh, rm, _ = po.frame_ao(kd, packed, self.cam, W, H, light, self.cfg.ao_length,
+                                self.cfg.bias, self.cfg.ao_seed, pixels=pix)
+        out = {"ao_frame_vs_oracle_same_tree": {
+            "pixels": int(pix.size),
+            "hits_bitexact": int((got[pix] == rh.view(np.int32).reshape(-1, 4)).all(1).sum()),
+            "masks_equal": int((mask[pix] == rm).sum()),
+            "truncated_pixels": int(((mask >> 6) & 1).sum())}}
+        out.update(hit_parity(got, packed, st, kd, self.cam, W, H, pix[:2000], pix[:150],
+                              (self.verts, self.faces)))
+        return out
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height
@@ -301,14 +435,28 @@ class HeightfieldAO:
 class SoupPrimary:
     name = "soup"
 
-    def __init__(self, torch, num_tris=65536):
+    def __init__(self, torch, num_tris=65536, tree="tuned", packed=None):
         import rayengine_b200 as rb
 
         self.rb = rb
+        self.tree = tree
+        self.num_tris = num_tris
+        if num_tris == 1 << 20:
+            self.name = "soup1m"
         self.cfg = cfg = rb.configs.SoupConfig(num_tris=num_tris)
-        self.packed = cfg.packed()
+        self.packed = cfg.packed() if packed is None else packed
+        if tree == "configured":
+            self.kd = cfg.kd_params()
+            for k, v in CONFIGURED_TREE.items():
+                setattr(self.kd, k, v)
+            choice = "as configured: SAH, depth <= 24, leaf <= 8 (soup empty bonus 0.15)"
+        else:
+            self.kd = cfg.kd_params()
+            choice = ("tuned on B200 for random soups (depth <= 40, leaf <= 8, empty bonus "
+                      "0.15); hits do not depend on the tree, see configured_tree")
+        self.kd_desc = kd_description(self.kd, choice)
         t0 = time.time()
-        self.scene = rb.KDScene.from_packed(self.packed, cfg.kd_params())
+        self.scene = rb.KDScene.from_packed(self.packed, self.kd)
         self.build_s = time.time() - t0
         self.cam = cfg.camera()
         W, H = cfg.width, cfg.height
@@ -327,6 +475,9 @@ class SoupPrimary:
                             f"{self.cfg.width}x{self.cfg.height} primary rays",
                 "triangles": st["num_tris"], "kd_nodes": st["num_nodes"],
                 "kd_refs": st["num_refs"], "kd_build_s": round(self.build_s, 3),
+                "kd_tree": self.kd_desc,
+                "work_per_ray": {f: round(self.tot[f] / self.tot["rays"], 2)
+                                 for f in ("inner", "leaf", "tests")},
                 "rays_per_step": self.rays_per_step, "tuning": self.tuning,
                 "l2": "flushed between steps (256 MB write)"}
 
@@ -336,7 +487,31 @@ class SoupPrimary:
 
     def alg_bytes(self):
         t = self.tot
-        return {"primary": 16 * t["rays"] + 8 * t["inner"] + 36 * t["leaf"] + 48 * t["tests"]}
+        return {"primary": survey_bytes(t["rays"], t["inner"], t["leaf"], t["tests"])}
+
+    def layout_bytes(self):
+        t = self.tot
+        return {"primary": layout_bytes(t["rays"], t["inner"], t["leaf"], t["tests"])}
+
+    def configured_variant(self, torch):
+        if self.tree == "configured":
+            return None
+        return SoupPrimary(torch, self.num_tris, tree="configured", packed=self.packed)
+
+    def parity(self):
+        from oracle import pyoracle as po
+
+        st = self.scene.stats()
+        nodes, leaves, tris = self.scene.export()
+        kd = po.KdTree(nodes, leaves, tris, st["bmin"], st["bmax"])
+        W, H = self.cfg.width, self.cfg.height
+        got = self.out.cpu().numpy().reshape(-1, 4)
+        full = np.arange(W * H, dtype=np.uint32)
+        pix = np.random.default_rng(12).choice(W * H, 600, replace=False).astype(np.uint32)
+        v = self.packed[:, 0:3]
+        verts = np.stack([v, v + self.packed[:, 4:7], v + self.packed[:, 8:11]], 1).reshape(-1, 3)
+        faces = np.arange(verts.shape[0], dtype=np.uint32).reshape(-1, 3)
+        return hit_parity(got, self.packed, st, kd, self.cam, W, H, full, pix, (verts, faces))
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height
@@ -410,6 +585,29 @@ class TerrainSDF:
                 "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1965 MHz",
                 "alg_ops_per_launch": evals * SDF_OPS_PER_EVAL,
                 "traffic": ncu_traffic(f"{self.name}:sdf")}
+
+    def parity(self):
+        """Bit-exact agreement with the oracle's march on a pixel sample, and
+        the hit error against the FP64 arbiter (the float march's rule in
+        double precision, its first crossing bisected to the root)."""
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        out = self.out.cpu().numpy()
+        pix = np.random.default_rng(12).choice(W * H, 3000, replace=False).astype(np.uint32)
+        P = po.perm(self.cfg.seed)
+        ref = po.sdf_image(P, self.cam, W, H, pixels=pix)
+        f = out.view(np.float32)[pix]
+        u = out.view(np.uint32)[pix]
+        same = ((u[:, 7] == ref["status"]) & (u[:, 6] == ref["steps"]) &
+                (f[:, 0:3].view(np.uint32) == ref["pos"].view(np.uint32)).all(1) &
+                (f[:, 3:6].view(np.uint32) == ref["normal"].view(np.uint32)).all(1))
+        jp, jh = po.sdf_arbiter(P, self.cam, W, H, pix[:1000])
+        err, disagree, both = po.hit_errors(out, jp, jh, pix[:1000])
+        return {"vs_oracle": {"pixels": int(pix.size), "bitexact": int(same.sum())},
+                "vs_fp64_arbiter": {"pixels": 1000, "hit_miss_disagree": disagree,
+                                    "median_hit_error": float(np.median(err)) if both else None,
+                                    "p95_hit_error": float(np.quantile(err, 0.95)) if both else None}}
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height
@@ -546,6 +744,22 @@ class NeuralTerrainSDF:
         # the reference's method for this field on the host: the exact march
         return TerrainSDF.cpu_baseline(self, budget_s)
 
+    def parity(self):
+        """Hit error of the neural tracer's frame against the FP64 arbiter
+        (target: median <= 1e-3 scene units), beside the exact tracer's."""
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        out = self.out.cpu().numpy()
+        pix = np.random.default_rng(12).choice(W * H, 1500, replace=False).astype(np.uint32)
+        P = po.perm(self.cfg.seed)
+        jp, jh = po.sdf_arbiter(P, self.cam, W, H, pix)
+        err, disagree, both = po.hit_errors(out, jp, jh, pix)
+        return {"vs_fp64_arbiter": {"pixels": int(pix.size), "hit_miss_disagree": disagree,
+                                    "median_hit_error": float(np.median(err)) if both else None,
+                                    "p95_hit_error": float(np.quantile(err, 0.95)) if both else None,
+                                    "target": "median <= 1e-3 scene units"}}
+
 
 class BatchWavefront:
     """32 seeded scenes (soups of 10k-2M triangles and volumetric terrains)
@@ -599,8 +813,26 @@ class BatchWavefront:
     def alg_bytes(self):
         w = self.work
         cont = int(self.rays[1:].sum())
+        return {"batch": survey_bytes(int(self.rays.sum()), w["inner"], w["leaf"], w["tests"], cont)}
+
+    def layout_bytes(self):
+        w = self.work
+        cont = int(self.rays[1:].sum())
         return {"batch": 16 * w["inner"] + 48 * w["leaf"] + 52 * w["tests"] + 64 * cont +
                 4 * self.batch.total_pixels}
+
+    def parity(self):
+        from oracle import pyoracle as po
+
+        scenes, offsets, _ = reference_batch_scenes(self.cfg)
+        rad = self.out.cpu().numpy()
+        g = np.sort(np.random.default_rng(12).choice(self.batch.total_pixels, 400,
+                                                      replace=False)).astype(np.uint32)
+        orad, _, _ = po.batch_path(scenes, offsets, g, self.cfg.max_depth, self.cfg.path_seed,
+                                   self.cfg.mesh_bias)
+        return {"vs_oracle_path_tracer": {
+            "pixels": int(g.size),
+            "radiance_bitexact": int((rad[g].view(np.uint32) == orad.view(np.uint32)).sum())}}
 
     def e2e_compute(self, torch, stream):
         self.batch.render(self.out, stream=stream, graph=True)
@@ -666,11 +898,33 @@ def reference_batch_scenes(cfg):
 
 
 # ---------------------------------------------------- the reference's path
+def _cosine_dirs(n, rng, k):
+    """k cosine-weighted directions around each unit normal n (m, 3) -> (m, k, 3)."""
+    m = n.shape[0]
+    t = np.where(np.abs(n[:, :1]) > np.abs(n[:, 1:2]),
+                 np.stack([n[:, 2], np.zeros(m), -n[:, 0]], 1),
+                 np.stack([np.zeros(m), -n[:, 2], n[:, 1]], 1))
+    t /= np.maximum(np.linalg.norm(t, axis=1, keepdims=True), 1e-30)
+    b = np.cross(n, t)
+    u1, u2 = rng.random((m, k)), rng.random((m, k))
+    r, phi = np.sqrt(u1), 2.0 * np.pi * u2
+    x, y, z = r * np.cos(phi), np.sqrt(1.0 - u1), r * np.sin(phi)
+    return x[..., None] * b[:, None] + y[..., None] * n[:, None] + z[..., None] * t[:, None]
+
+
 def reference_workload(name):
-    """(workload description, built-by note, step(npix) -> rays traced) for the
-    reference's own CPU path.  Scene inputs come from the CPU oracle's
-    generators (the same seeded values the kernels produce); nothing of this
-    repository's engine runs on this path."""
+    """(workload description, built-by note, kind, step(npix) -> rays traced)
+    for the reference's own CPU path.
+
+    Meshes: the reference's RKDTreeCPU and its CPU ray query
+    singleRayStacklessIntersect, compiled from its sources (oracle/_ref),
+    over the same seeded scene (generated by the CPU oracle's generators);
+    as shipped the tree is one leaf, so every query tests every triangle.
+    SDF and batch workloads: the reference's device march cannot be compiled
+    for the host (texture hash, CUDA 10 texture references), so the arm
+    times the oracle's restatement of it.  Nothing of this repository's
+    engine runs on this path: the package is imported for its pure-Python
+    workload descriptions only and its library is never loaded."""
     from oracle import pyoracle as po
     import rayengine_b200.configs as C
     from rayengine_b200 import api
@@ -686,8 +940,8 @@ def reference_workload(name):
                                      cfg.mesh_bias)
             return int(nr.sum())
         return ("batched path tracing of the 32-scene batch (depth 4, 1 spp), seeded-random "
-                "pixels", "restated single-leaf build (brute-force Moller-Trumbore) and the "
-                "restated exact SDF march", step)
+                "pixels", "oracle restatement: single-leaf build (brute-force Moller-Trumbore) "
+                "and the exact SDF march", "port", step)
     if name in ("terrain_sdf", "nsdf_terrain"):
         cfg = C.TerrainConfig()
         W, H = cfg.width, cfg.height
@@ -698,51 +952,64 @@ def reference_workload(name):
             po.sdf_image(P, cam, W, H, pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32))
             return npix
         return ("exact-SDF sphere tracing of d(p)=p.y-3fBm(0.25p), 8 octaves, 1920x1080",
-                "restated exact-SDF march (sphere_tracing.cuh:183-216)", step)
-    if name == "heightfield_ao":
+                "oracle restatement of the exact-SDF march (sphere_tracing.cuh:183-216; the "
+                "reference's device code does not compile for the host)", "port", step)
+    if name.startswith("heightfield_ao"):
         cfg = C.HeightfieldConfig()
         verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
                                       cfg.amplitude)
         desc = ("heightfield 1024x1024 cells (2,097,152 tris); 1920x1080 primary + 1 shadow + 4 AO "
                 "rays per hit")
     else:
-        cfg = C.SoupConfig(num_tris=65536 if name == "soup" else 1 << 20)
+        cfg = C.SoupConfig(num_tris=(1 << 20) if name.startswith("soup1m") else 65536)
         tri = po.soup(cfg.seed, cfg.num_tris)
         verts = tri.reshape(-1, 3)
         faces = np.arange(verts.shape[0], dtype=np.uint32).reshape(-1, 3)
         desc = f"triangle soup {cfg.num_tris} tris; {cfg.width}x{cfg.height} primary rays"
-    packed = api.pack_triangles(verts, faces)
-    v = verts[faces.reshape(-1)]
-    bmin, bmax = v.min(0), v.max(0)
-    built_by = "restated single-leaf build (RKDTreeCPU with MAX_DEPTH=1)"
-    if po.ref_lib() is not None:
-        nodes, idx, root, _, _ = po.ref_build(verts, faces)
-        rn = po.ref_node_fields(nodes[root])
-        assert rn["is_leaf"] and np.array_equal(idx, np.arange(len(idx)))
-        bmin, bmax = rn["min"], rn["max"]
-        built_by = "reference RKDTreeCPU/RKDThreeGPU compiled from its sources (one leaf)"
+    if po.ref_lib() is None:
+        raise FileNotFoundError("oracle/_ref/libre_ref.so (the reference's compiled host code)")
+    tree = po.RefTree(verts, faces)
     cam = cfg.camera()
     W, H = cfg.width, cfg.height
-    if name == "heightfield_ao":
-        light = api.unit(cfg.light_dir)
+    built_by = ("the reference's RKDTreeCPU (one leaf as shipped, KDTree.cpp:12,347) and its CPU "
+                "query RKDTreeCPU::singleRayStacklessIntersect (KDTree.cpp:993-1066), compiled "
+                "from its sources, OpenMP schedule(dynamic) over rays (RayTracer.cpp:154)")
+
+    def primary(npix):
+        o, d = po.camera_rays(cam, W, H, rng.choice(W * H, npix, replace=False))
+        t, nrm, _ = tree.trace(o, d)
+        return o, d, t, nrm
+
+    if name.startswith("heightfield_ao"):
+        light = np.array(api.unit(cfg.light_dir), np.float64)
 
         def step(npix):
-            return po.frame_ao_bruteforce(packed, bmin, bmax, cam, W, H, light, cfg.ao_length,
-                                          cfg.bias, cfg.ao_seed,
-                                          rng.choice(W * H, npix, replace=False).astype(np.uint32))
+            o, d, t, nrm = primary(npix)
+            hit = t < 1e19
+            if not hit.any():
+                return npix
+            n = nrm[hit].astype(np.float64)
+            n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+            flip = np.einsum("ij,ij->i", n, d[hit]) > 0.0
+            n[flip] = -n[flip]
+            p = o[hit] + t[hit, None].astype(np.float64) * d[hit] + cfg.bias * n
+            dirs = np.concatenate([np.broadcast_to(light, (n.shape[0], 1, 3)),
+                                   _cosine_dirs(n, rng, 4)], 1).reshape(-1, 3)
+            tree.trace(np.repeat(p, 5, axis=0), dirs)
+            return npix + 5 * n.shape[0]
     else:
         def step(npix):
-            po.primary_bruteforce(packed, bmin, bmax, cam, W, H,
-                                  pixels=rng.choice(W * H, npix, replace=False).astype(np.uint32))
+            primary(npix)
             return npix
-    return desc, built_by + "; traversal restated from ray_functions.cuh:231-360, i.e. " \
-        "Moller-Trumbore over every triangle per ray", step
+    return desc, built_by, "reference", step
 
+
+TREE_WORKLOADS = ("heightfield_ao", "soup", "soup1m")
 
 WORKLOADS = {
     "heightfield_ao": HeightfieldAO,
     "soup": SoupPrimary,
-    "soup1m": lambda torch: SoupPrimary(torch, num_tris=1 << 20),
+    "soup1m": lambda torch, **kw: SoupPrimary(torch, num_tris=1 << 20, **kw),
     "terrain_sdf": TerrainSDF,
     "nsdf_terrain": NeuralTerrainSDF,
     "batch32": BatchWavefront,
@@ -759,13 +1026,16 @@ def run_reference(args):
         return 0
     from oracle import pyoracle as po
 
-    desc, built_by, step = reference_workload(args.config)
-    # size one step to roughly one second of work on all host cores
+    desc, built_by, kind, step = reference_workload(args.config)
+    # size one step to about a second of work on all host cores, less when
+    # many steps are asked for, so that the whole run stays within minutes
+    target_s = min(1.0, 90.0 / max(1, args.steps + args.warmup))
     npix = 4
-    t0 = time.perf_counter()
-    step(npix)
-    dt = time.perf_counter() - t0
-    npix = max(4, min(200000, int(npix * 1.0 / max(dt, 1e-4))))
+    for _ in range(2):  # the first call also pays one-time set-up
+        t0 = time.perf_counter()
+        step(npix)
+        dt = time.perf_counter() - t0
+        npix = max(4, min(200000, int(npix * target_s / max(dt, 1e-4))))
     for _ in range(args.warmup):
         step(npix)
     rays = 0
@@ -781,14 +1051,60 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": desc, "pixels_per_step": npix},
         "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": po.threads(),
-                         "kind": "port",
+                         "kind": kind,
                          "sample": f"{npix} seeded-random pixels per step ({rays // args.steps} "
-                                   f"rays per step); tree: {built_by}"},
+                                   f"rays per step); {built_by}"},
         "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def timed_steps(torch, phases, stream, flush, steps, world):
+    """K steps bracketed by a barrier and a device synchronize on both sides,
+    L2 flushed before each; CUDA events on the launching stream around every
+    phase.  Returns (mean step ms, {phase: mean ms})."""
+    n_ph = len(phases)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(n_ph + 1)] for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(stream)
+        for j, (_, fn) in enumerate(phases):
+            fn()
+            ev[k][j + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [ev[k][0].elapsed_time(ev[k][n_ph]) for k in range(steps)]
+    phase_ms = {name: statistics.mean(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(steps))
+                for j, (name, _) in enumerate(phases)}
+    return statistics.mean(step_ms), phase_ms
+
+
+def configured_tree_line(torch, wl, stream, flush, args, world, dev):
+    """The same workload over the tree the configuration names (depth 24,
+    leaf 8), timed like the headline (same steps, warm-up and L2 flush)."""
+    alt = wl.configured_variant(torch)
+    if alt is None:
+        return None
+    phases = alt.phases(stream)
+    for i in range(args.warmup):
+        flush.fill_(i & 0xFF)
+        for _, fn in phases:
+            fn()
+    ms, phase_ms = timed_steps(torch, phases, stream, flush, args.steps, world)
+    ms_max = max_over_ranks(ms, world, dev)
+    total = sum_over_ranks(alt.rays_per_step, world, dev)
+    st = alt.scene.stats()
+    out = {"value": round(total / (ms_max / 1e3) / 1e6, 3), "unit": "Mrays/s",
+           "ms_per_step": round(ms_max, 4), "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+           "kd_tree": alt.kd_desc, "kd_nodes": st["num_nodes"], "kd_refs": st["num_refs"],
+           "kd_build_s": round(alt.build_s, 3), "rays_per_step": alt.rays_per_step,
+           "note": "same rays and same hits as the headline; only the tree differs"}
+    alt.scene.close()
+    return out
 
 
 def e2e_times(torch, wl, stream, flush, steps, world):
@@ -872,6 +1188,8 @@ def run_ours(args):
         opts["num_scenes"] = args.scenes
     if args.config == "batch32" and world > 1:
         opts["rank"], opts["world"] = rank, world  # scenes split across ranks
+    if args.config in TREE_WORKLOADS:
+        opts["tree"] = args.tree
     wl = WORKLOADS[args.config](torch, **opts)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -899,27 +1217,12 @@ def run_ours(args):
         step()
     torch.cuda.synchronize()
 
-    n_ph = len(phases)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(n_ph + 1)] for _ in range(args.steps)]
     cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     clocks = ClockSampler(cvd.split(",")[local] if cvd else str(local))
     clocks.start()
     time.sleep(0.5)  # let nvidia-smi take its first samples before the timed region
-    barrier(world)
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        flush.fill_(k & 0xFF)
-        ev[k][0].record(stream)
-        for j, (_, fn) in enumerate(phases):
-            fn()
-            ev[k][j + 1].record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
+    ms, phase_ms = timed_steps(torch, phases, stream, flush, args.steps, world)
     clk = clocks.stop()
-    step_ms = [ev[k][0].elapsed_time(ev[k][n_ph]) for k in range(args.steps)]
-    phase_ms = {name: statistics.mean(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(args.steps))
-                for j, (name, _) in enumerate(phases)}
-    ms = statistics.mean(step_ms)
     ms_max = max_over_ranks(ms, world, dev)
     total_rays = sum_over_ranks(wl.rays_per_step, world, dev)
     value = total_rays / (ms_max / 1e3) / 1e6
@@ -953,8 +1256,14 @@ def run_ours(args):
         "gpu_launches": wl.kernels_per_step * args.steps,
         "clocks": clk,
     }
+    if not args.no_configured_tree and hasattr(wl, "configured_variant"):
+        ct = configured_tree_line(torch, wl, stream, flush, args, world, dev)
+        if ct is not None:
+            line["configured_tree"] = ct
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = wl.cpu_baseline()
+        if hasattr(wl, "parity"):
+            line["parity"] = wl.parity()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -971,7 +1280,13 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS), default="heightfield_ao")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline and the checker's parity summary")
+    ap.add_argument("--tree", choices=["tuned", "configured"], default="tuned",
+                    help="kd-tree of the mesh workloads: the B200-tuned library default, or "
+                         "the configured SAH tree (depth <= 24, leaf <= 8)")
+    ap.add_argument("--no-configured-tree", action="store_true",
+                    help="do not also time the configured tree after the headline")
     ap.add_argument("--train-steps", type=int, default=0,
                     help="nsdf_terrain: training steps at set-up (default: the config's 20000)")
     ap.add_argument("--scenes", type=int, default=0,

@@ -88,7 +88,11 @@ typedef struct re_kd_params {
   float empty_bonus;       /* SAH discount for an empty child (0.1) */
   uint32_t bfs_levels;     /* top levels laid out breadth-first   */
   uint32_t threads;        /* host build threads, 0 = all         */
-  uint32_t max_leaf_visits;/* per-ray traversal bound             */
+  uint32_t max_leaf_visits;/* per-ray traversal bound (16384); a ray that
+                              reaches it stops and is reported: see
+                              re_scene_truncated and the AO mask bit 6
+                              (the reference stops at 50 leaves without
+                              a report, ray_functions.cuh:284)           */
 } re_kd_params;
 
 typedef struct re_scene re_scene;
@@ -154,6 +158,16 @@ RE_API re_status re_trace_primary(re_scene* s, const re_camera* cam,
 RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n,
                                uint32_t flags, re_hit* d_out, void* stream);
 
+/* Rays of the last trace call on this scene that stopped at the leaf-visit
+ * cap (re_kd_params.max_leaf_visits), copied to *d_count (device memory) on
+ * `stream`.  Counted by re_trace_primary, re_count_primary, re_trace_rays,
+ * re_render_ao (both passes: the count covers the frame), re_render_frame;
+ * each of those calls clears it first.  Per ray: re_count_primary's status
+ * word (1 = stopped at the cap) and the AO mask bit 6.  Replaces the
+ * reference's silent cut-off (stackless_kdtree_traversal's
+ * `limit < 50`, ray_functions.cuh:284). */
+RE_API re_status re_scene_truncated(const re_scene* s, uint32_t* d_count, void* stream);
+
 /* Per-pixel work counters of a primary-ray pass (device array of w*h
  * uint4: inner-node steps, leaf visits, triangle tests, status).  Used to
  * compute the algorithmic bytes of a pass. */
@@ -164,7 +178,9 @@ RE_API re_status re_count_primary(re_scene* s, const re_camera* cam,
 /* Primary + shadow + ambient-occlusion frame.
  *   d_primary: w*h re_hit (closest hit, two-sided)
  *   d_mask:    w*h uint32, bit0 primary hit, bit1 shadow ray unoccluded,
- *              bits 2..5 AO ray j unoccluded.
+ *              bits 2..5 AO ray j unoccluded, bit6 one of the pixel's rays
+ *              stopped at the leaf-visit cap (its result covers only the
+ *              leaves it reached).
  * Secondary rays start at hit + n * bias (n = geometric normal facing the
  * ray); the shadow ray goes along light_dir without bound, the four
  * cosine-weighted AO rays are ao_length long.  The secondary-ray queue is
@@ -204,8 +220,11 @@ RE_API re_status re_render_ao_secondary(re_scene* s, uint32_t* d_mask,
  * identical.
  *   - w * h must not exceed RE_NOALLOC_MAX_PIXELS (5 secondary rays of 32
  *     bytes per pixel); larger images return RE_ERR_LIMIT without launching.
- *   - The first call on a device looks up the array's device address (with
- *     that device current); make that first call before any stream capture.
+ *   - Every call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress, which allocates nothing), so the entry point
+ *     stays valid after a device reset; the first call on a device may also
+ *     load the library's device code, so make that first call before any
+ *     stream capture.
  *   - Every call on a device shares the one array: calls that overlap on the
  *     GPU (other streams, other threads) race and must be serialised by the
  *     caller. */
@@ -571,6 +590,14 @@ RE_API re_status re_batch_render_graph(re_batch* b, float* d_radiance,
  * primary rays under kind 0), 2 * max_depth values; error = 1 if a wait
  * bound was reached (rays dropped). */
 RE_API re_status re_batch_stats_get(re_batch* b, uint64_t* rays, int* error);
+/* Bounds of the persistent kernel's waits: polls of one queue slot's flag
+ * before a claim is dropped, and trips of the kernel's loop (0 = the
+ * defaults, 2^22 each).  Reaching either sets the frame's error flag
+ * (re_batch_stats_get) and the kernel returns instead of waiting on.  Lower
+ * them only to exercise that error path (tests); the next frame after the
+ * defaults are restored is complete again.  No reference counterpart. */
+RE_API re_status re_batch_set_wait_bounds(re_batch* b, uint32_t pending_polls,
+                                          uint32_t loop_trips);
 /* One frame with work counters: totals[0..3] = inner-node visits, leaf
  * visits, triangle tests, terrain field evaluations (host array). */
 RE_API re_status re_batch_counts(re_batch* b, float* d_radiance, void* stream,

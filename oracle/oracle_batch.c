@@ -56,9 +56,12 @@ void o_batch_rays_kd(const o_kdtree* kd, const float* rays, int64_t n, int mode,
   }
 }
 
-/* Primary + shadow + 4 AO rays per pixel; mask bits as re_render_ao.
- * packed: the scene's triangles in input order (12 floats each), used for
- * the hit triangle's geometric normal. */
+/* Primary + shadow + 4 AO rays per pixel; mask bits as re_render_ao (bit 6:
+ * a ray of the pixel stopped at the leaf-visit cap).  packed: the scene's
+ * triangles in input order (12 floats each), used for the hit triangle's
+ * geometric normal.  totals[0..7]: inner/leaf/tests/rays of the primary and
+ * of the secondary pass; totals[8], totals[9]: primary and secondary rays
+ * stopped at the cap. */
 static inline void cross3c(const float a[3], const float b[3], float r[3]) {
   r[0] = fmaf(a[1], b[2], -(a[2] * b[1]));
   r[1] = fmaf(a[2], b[0], -(a[0] * b[2]));
@@ -77,8 +80,8 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
   o_camera_setup(cam, &b);
   if (!pixels) npix = (int64_t)w * h;
   uint64_t total = 0;
-  uint64_t pi = 0, pl = 0, pt = 0, si = 0, sl = 0, stt = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total, pi, pl, pt, si, sl, stt) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  uint64_t pi = 0, pl = 0, pt = 0, si = 0, sl = 0, stt = 0, ptr = 0, str_ = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total, pi, pl, pt, si, sl, stt, ptr, str_) num_threads(threads > 0 ? threads : omp_get_max_threads())
   for (int64_t i = 0; i < npix; ++i) {
     uint32_t p = pixels ? pixels[i] : (uint32_t)i;
     float o[3], d[3];
@@ -92,8 +95,12 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
     pt += c.tri_tests;
     out[i] = hit;
     uint32_t m = 0;
+    if (c.status == 1) {
+      m |= 1u << 6;
+      ptr++;
+    }
     if (hit.id >= 0) {
-      m = 1;
+      m |= 1u;
       const float* T = packed + 12 * (size_t)hit.id;
       float n[3];
       cross3c(T + 4, T + 8, n);
@@ -119,6 +126,10 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
         sl += sc.leaf_visits;
         stt += sc.tri_tests;
         if (sh.id < 0) m |= 1u << (1 + j);
+        if (sc.status == 1) {
+          m |= 1u << 6;
+          str_++;
+        }
       }
       total += 5;
     }
@@ -128,6 +139,7 @@ void o_batch_frame_ao(const o_kdtree* kd, const float* packed, const o_camera* c
   if (totals) {
     totals[0] = pi; totals[1] = pl; totals[2] = pt; totals[3] = (uint64_t)npix;
     totals[4] = si; totals[5] = sl; totals[6] = stt; totals[7] = total;
+    totals[8] = ptr; totals[9] = str_;
   }
 }
 

@@ -163,7 +163,7 @@ def frame_ao(kd: KdTree, packed, cam, w, h, light_dir, ao_length, bias, seed, pi
     out = np.zeros(n, HIT_DTYPE)
     mask = np.zeros(n, np.uint32)
     nsec = ctypes.c_uint32(0)
-    tot = np.zeros(8, np.uint64)
+    tot = np.zeros(10, np.uint64)
     oc = camera(cam)
     ld = (ctypes.c_float * 3)(*light_dir)
     lib().o_batch_frame_ao(ctypes.byref(kd.s), _p(packed), ctypes.byref(oc), ctypes.c_uint32(w),
@@ -274,6 +274,55 @@ def ref_build(verts, faces):
     if nn < 0:
         raise RuntimeError("reference tree larger than the buffers")
     return nodes[:nn].copy(), idx[: nidx.value].copy(), root.value, levels.value, leaves.value
+
+
+class RefTree:
+    """The reference's own CPU kd-tree and ray query (RKDTreeCPU built by its
+    constructor, KDTree.cpp:117-173, queried with singleRayStacklessIntersect,
+    KDTree.cpp:993-1066), compiled from its sources into oracle/_ref.  As
+    shipped the tree is one leaf, so a query is Moller-Trumbore over every
+    triangle (two-sided, t > 1e-5) keeping the smallest t."""
+
+    def __init__(self, verts, faces):
+        L = ref_lib()
+        if L is None:
+            raise FileNotFoundError(REF_LIB_PATH)
+        L.ref_tree_create.restype = ctypes.c_void_p
+        L.ref_tree_destroy.argtypes = [ctypes.c_void_p]
+        L.ref_tree_trace.restype = ctypes.c_int64
+        L.ref_tree_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.ref_max_threads.restype = ctypes.c_int
+        self._L = L
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+        self._h = L.ref_tree_create(_p(v), ctypes.c_int(v.shape[0]), _p(f), ctypes.c_int(f.shape[0]))
+
+    def threads(self) -> int:
+        return int(self._L.ref_max_threads())
+
+    def trace(self, o, d, nthreads=0):
+        """Closest hits of rays (o, d): (t (inf-like 1e20 where none), normals, hit count)."""
+        o = np.asarray(o, np.float32).reshape(-1, 3)
+        d = np.asarray(d, np.float32).reshape(-1, 3)
+        rays = np.ascontiguousarray(np.concatenate([o, d], 1), np.float32)
+        n = rays.shape[0]
+        t = np.empty(n, np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        hits = self._L.ref_tree_trace(self._h, _p(rays), ctypes.c_int64(n), _p(t), _p(nrm),
+                                      ctypes.c_int(nthreads))
+        return t, nrm, int(hits)
+
+    def close(self):
+        if self._h:
+            self._L.ref_tree_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ref_perm(seed: int) -> np.ndarray:

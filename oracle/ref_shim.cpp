@@ -9,12 +9,23 @@
 //     flattened 128-byte RKDTreeNodeGPU records and obj_index_list.
 //   * RPerlinNoise (RayEngine/src/World/PerlinNoise.h:16-52): the 512-entry
 //     permutation table for a seed.
+//   * RKDTreeCPU::singleRayStacklessIntersect (KDTree.cpp:993-1066): the
+//     reference's own CPU ray query (closest hit: t and the interpolated
+//     vertex normal, two-sided triIntersect, KDTree.cpp:909-949) over its
+//     own tree, run over many rays with OpenMP `parallel for
+//     schedule(dynamic)` as RRayTracer::trace does
+//     (RayEngine/src/Engine/RayTracer.cpp:154).  The benchmark's reference
+//     arm times this.
 //
 // Nothing in the product links this file.
 #include "repch.h"
 #include "Primitives/KDThreeGPU.h"
+#include "Primitives/Ray.h"
 #include "World/PerlinNoise.h"
 
+#include <omp.h>
+
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 
@@ -61,6 +72,61 @@ int ref_build_kdtree(const float* verts, int num_verts, const uint32_t* faces,
   delete cpu;
   return rc;
 }
+
+// The reference's CPU tree (RKDTreeCPU) over an indexed mesh, kept for ray
+// queries.  Vertex normals: the normalised sum of the adjacent faces'
+// normals (the reference's mesh loaders supply per-vertex normals).
+void* ref_tree_create(const float* verts, int num_verts, const uint32_t* faces, int num_faces) {
+  std::vector<float3> v(num_verts), n(num_verts, make_float3(0.f, 0.f, 0.f));
+  for (int i = 0; i < num_verts; ++i)
+    v[i] = make_float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+  std::vector<uint3> f(num_faces);
+  for (int i = 0; i < num_faces; ++i) {
+    f[i] = make_uint3(faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]);
+    float3 a = v[f[i].x], b = v[f[i].y], c = v[f[i].z];
+    float3 e1 = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+    float3 e2 = make_float3(c.x - a.x, c.y - a.y, c.z - a.z);
+    float3 fn = make_float3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z,
+                            e1.x * e2.y - e1.y * e2.x);
+    for (uint32_t k : {f[i].x, f[i].y, f[i].z}) {
+      n[k].x += fn.x;
+      n[k].y += fn.y;
+      n[k].z += fn.z;
+    }
+  }
+  for (auto& x : n) {
+    float l = std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z);
+    x = l > 0.f ? make_float3(x.x / l, x.y / l, x.z / l) : make_float3(0.f, 1.f, 0.f);
+  }
+  return new RKDTreeCPU(v.data(), f.data(), n.data(), nullptr, num_verts, num_faces, num_verts, 0);
+}
+
+void ref_tree_destroy(void* tree) { delete static_cast<RKDTreeCPU*>(tree); }
+
+// rays: n x 6 floats {origin, direction}.  out_t: closest hit distance
+// (K_INFINITY where the query reports no hit), out_n: n x 3 normal.
+// Returns the number of rays that hit.
+int64_t ref_tree_trace(void* tree, const float* rays, int64_t n, float* out_t, float* out_n,
+                       int threads) {
+  RKDTreeCPU* t = static_cast<RKDTreeCPU*>(tree);
+  int64_t hits = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : hits) num_threads(threads > 0 ? threads : omp_get_max_threads())
+  for (int64_t i = 0; i < n; ++i) {
+    const float* r = rays + 6 * i;
+    RRay ray(make_float3(r[0], r[1], r[2]), make_float3(r[3], r[4], r[5]));
+    float th = K_INFINITY;
+    float3 nrm = make_float3(0.f, 0.f, 0.f);
+    bool hit = t->singleRayStacklessIntersect(ray, th, nrm);
+    out_t[i] = hit ? th : K_INFINITY;
+    out_n[3 * i] = nrm.x;
+    out_n[3 * i + 1] = nrm.y;
+    out_n[3 * i + 2] = nrm.z;
+    hits += hit ? 1 : 0;
+  }
+  return hits;
+}
+
+int ref_max_threads(void) { return omp_get_max_threads(); }
 
 // Writes RPerlinNoise(seed).permutationTable (512 entries) to out.
 void ref_perlin_permutation(uint32_t seed, uint32_t* out) {

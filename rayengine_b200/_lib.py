@@ -1,7 +1,10 @@
 """ctypes binding of librayengine_b200.so (declarations: include/rayengine_b200.h).
 
 The shared library is the product: there is no Python or CPU fallback.  If
-the library is missing this module raises at import time.
+the library file is missing this module raises at import time.  The library
+is mapped into the process on the first call through ``lib`` (not at
+import), so code that only uses the package's pure-Python helpers (camera
+construction, triangle packing, workload descriptions) never loads it.
 """
 from __future__ import annotations
 
@@ -25,8 +28,6 @@ if not os.path.exists(LIB_PATH):
         f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
         "or `make -f rayengine_b200/csrc/Makefile`"
     )
-
-lib = ctypes.CDLL(LIB_PATH)
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
 c_u32_p = ctypes.POINTER(ctypes.c_uint32)
@@ -213,6 +214,7 @@ _SIGS = {
     "re_trace_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P]),
     "re_trace_rays": (ctypes.c_int, [_P, _P, _U32, _U32, _P, _P]),
     "re_count_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P]),
+    "re_scene_truncated": (ctypes.c_int, [_P, _P, _P]),
     "re_render_ao": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P, _P]),
     "re_render_ao_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, ctypes.POINTER(re_ao_params), _P, _P, _P]),
     "re_render_ao_secondary": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -266,6 +268,7 @@ _SIGS = {
     "re_batch_render": (ctypes.c_int, [_P, _P, _P, _P]),
     "re_batch_render_graph": (ctypes.c_int, [_P, _P, _P, _P]),
     "re_batch_stats_get": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_int)]),
+    "re_batch_set_wait_bounds": (ctypes.c_int, [_P, _U32, _U32]),
     "re_batch_counts": (ctypes.c_int, [_P, _P, _P, _P]),
     "re_batch_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_batch_tuning)]),
     "re_batch_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(re_batch_tuning)]),
@@ -276,10 +279,34 @@ _SIGS = {
 
 EXPORTED = tuple(_SIGS)
 
-for _name, (_res, _args) in _SIGS.items():
-    _fn = getattr(lib, _name)
-    _fn.restype = _res
-    _fn.argtypes = _args
+
+class _Library:
+    """librayengine_b200.so, loaded (and its signatures declared) on first use."""
+
+    def __init__(self):
+        self._dll = None
+
+    def _load(self):
+        if self._dll is None:
+            dll = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(dll, name)
+                fn.restype = res
+                fn.argtypes = args
+            self._dll = dll
+        return self._dll
+
+    @property
+    def loaded(self) -> bool:
+        return self._dll is not None
+
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        return getattr(self._load(), name)
+
+
+lib = _Library()
 
 
 def check(status: int, fn: str) -> None:

@@ -250,6 +250,15 @@ class KDScene:
              _stream_ptr(stream))
         return out
 
+    def truncated(self, stream=None) -> int:
+        """Rays of the last trace call on this scene that stopped at the
+        leaf-visit cap (re_scene_truncated); synchronises the stream."""
+        import torch
+
+        t = torch.zeros(1, dtype=torch.int32, device="cuda")
+        call("re_scene_truncated", self._h, _dptr(t), _stream_ptr(stream))
+        return int(t.item())
+
     def trace_rays(self, rays, flags: int = TRACE_TWO_SIDED, out=None, stream=None):
         """rays: float32 CUDA tensor (n, 8) = re_ray {o, tmax, d, tag}."""
         import torch
@@ -595,6 +604,10 @@ class Batch:
         err = ctypes.c_int()
         call("re_batch_stats_get", self._h, rays.ctypes.data, ctypes.byref(err))
         return {"rays": rays.reshape(self.max_depth, 2).astype(np.int64), "error": int(err.value)}
+
+    def set_wait_bounds(self, pending_polls: int = 0, loop_trips: int = 0) -> None:
+        """Lower the kernel's wait bounds (0 = defaults); for error-path tests."""
+        call("re_batch_set_wait_bounds", self._h, pending_polls, loop_trips)
 
     def counts(self, out=None, stream=None) -> dict:
         """Traversal and field-evaluation work of one frame."""

@@ -94,12 +94,17 @@ struct __align__(16) SceneDev {
   uint32_t w, h, kind, pix_off;
   float albedo;
 };
+// Shared memory holds SceneDev[num_scenes], then the noise tables (multiples
+// of 512 bytes), then the staged nodes (uint2): the nodes stay 8-byte
+// aligned only while the scene records are a multiple of 16 bytes.
+static_assert(sizeof(SceneDev) % 16 == 0, "SceneDev must keep the staged nodes aligned");
 
 struct BatchDev {
   const SceneDev* scenes;
   const uint8_t* perms;  // perm_count tables of 512 bytes (words in shared memory)
   uint32_t num_scenes, perm_count, stage_total, total_pixels;
   uint32_t depth, seed, refill_min, steps_per_trip;
+  uint32_t pending_bound, loop_bound;  // polls of one slot flag, trips of the loop
   float mesh_bias;
   float4* queue;        // records: 2 float4 per slot
   uint32_t* flags;      // one per slot
@@ -144,6 +149,7 @@ __device__ __forceinline__ KdDev kd_of(const SceneDev& s) {
   kd.bmax = v3(s.bmax[0], s.bmax[1], s.bmax[2]);
   kd.max_visits = s.max_visits;
   kd.stage = s.stage;
+  kd.trunc = nullptr;
   return kd;
 }
 
@@ -178,6 +184,7 @@ __device__ __forceinline__ float miss_radiance(float albedo, uint32_t bounce, V3
 
 enum : uint32_t { kIdle = 0, kPending = 1, kLive = 2 };
 enum : uint32_t { kMarch = 0, kNormal = 1 };
+// Default wait bounds (re_batch_set_wait_bounds lowers them for tests).
 constexpr uint32_t kPendingBound = 1u << 22;  // polls of one slot flag
 constexpr uint32_t kLoopBound = 1u << 22;     // trips of the persistent loop
 
@@ -294,7 +301,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
   };
 
   uint32_t trip = 0;
-  for (; trip < kLoopBound; ++trip) {
+  for (; trip < B.loop_bound; ++trip) {
     // ---- pending claims: the slot's record is published once its flag holds this epoch
     if (state == kPending) {
       // The flag is polled with a relaxed load (an acquire load would
@@ -339,7 +346,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
       if (state == kPending && ((mask >> (pq / 2u + 1u)) & 1u)) {
         if (pslot >= ld_relaxed(&ctr[reserved_at(pq)])) state = kIdle;  // never filled
       }
-      if (state == kPending && polls >= kPendingBound) {
+      if (state == kPending && polls >= B.pending_bound) {
         errors = 1;
         state = kIdle;
       }
@@ -575,7 +582,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
     if (__shfl_sync(0xFFFFFFFFu, fin_pending, 0) >= 1024u) flush();
   }
   flush();
-  if (trip >= kLoopBound) errors = 1;
+  if (trip >= B.loop_bound) errors = 1;
   if (COUNT) {
     uint32_t v4[4] = {cnt.inner, cnt.leaf, cnt.tests, cnt.status};
 #pragma unroll
@@ -630,6 +637,7 @@ struct re_batch {
   uint32_t* d_ctr = nullptr;
   uint64_t qoff[re::batch::kMaxQueues] = {};
   re_batch_tuning tune = {256, 8, 0, 8};
+  uint32_t pending_bound = 0, loop_bound = 0;  // 0: the kernel's defaults
   // captured frame
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -729,6 +737,8 @@ re_status launch(re_batch* b, float* d_radiance, re_hit* d_primary, cudaStream_t
   B.seed = b->seed;
   B.refill_min = tn.refill_min;
   B.steps_per_trip = tn.steps_per_trip ? tn.steps_per_trip : 1u;
+  B.pending_bound = b->pending_bound ? b->pending_bound : kPendingBound;
+  B.loop_bound = b->loop_bound ? b->loop_bound : kLoopBound;
   B.mesh_bias = b->mesh_bias;
   B.queue = b->d_queue;
   B.flags = b->d_flags;
@@ -895,6 +905,15 @@ RE_API re_status re_batch_pixels(const re_batch* b, uint64_t* total, uint64_t* o
   if (!b || !total) return re::fail(RE_ERR_INVALID_ARG, "re_batch_pixels: bad arguments");
   *total = b->total_pixels;
   if (offsets) std::memcpy(offsets, b->offsets.data(), b->num_scenes * sizeof(uint64_t));
+  return RE_OK;
+}
+
+RE_API re_status re_batch_set_wait_bounds(re_batch* b, uint32_t pending_polls,
+                                          uint32_t loop_trips) {
+  if (!b) return re::fail(RE_ERR_INVALID_ARG, "re_batch_set_wait_bounds: null batch");
+  b->pending_bound = pending_polls;
+  b->loop_bound = loop_trips;
+  re::free_graph(b);  // a captured frame holds the old bounds
   return RE_OK;
 }
 

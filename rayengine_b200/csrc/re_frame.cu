@@ -147,6 +147,7 @@ KdDev kd_of_scene(const re_scene* s) {
   kd.bmax = {s->host.bmax[0], s->host.bmax[1], s->host.bmax[2]};
   kd.max_visits = s->max_visits;
   kd.stage = s->stage;
+  kd.trunc = s->d_counters + RE_SCENE_TRUNC_SLOT;
   return kd;
 }
 
@@ -207,7 +208,7 @@ RE_API re_status re_render_frame(re_scene* s, const re_camera* cam, const re_lig
     sh.light_int[i] = lights[i].intensity;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st));
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   re::KdDev kd = re::kd_of_scene(s);
   size_t smem = (size_t)kd.stage * sizeof(uint2);
   int grid = 0;

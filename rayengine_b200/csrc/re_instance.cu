@@ -113,6 +113,7 @@ RE_API re_status re_trace_instances(const re_instance* instances, uint32_t n, co
     I.kd.bmax = {s->host.bmax[0], s->host.bmax[1], s->host.bmax[2]};
     I.kd.max_visits = s->max_visits;
     I.kd.stage = 0;
+    I.kd.trunc = nullptr;
     re_instance_trig(instances[k].yaw, &I.c, &I.s);
     I.loc = {instances[k].location[0], instances[k].location[1], instances[k].location[2]};
   }

@@ -24,7 +24,13 @@ struct KdDev {
   V3 bmin, bmax;
   uint32_t max_visits;
   uint32_t stage;  // nodes [0, stage) are read from shared memory
+  // rays stopped by the leaf-visit cap are counted here (may be null); the
+  // reference stops at its cap silently (ray_functions.cuh:284)
+  uint32_t* trunc;
 };
+
+// Trav::visits of a walk that stopped at the leaf-visit cap.
+constexpr uint32_t kTruncated = 0xFFFFFFFFu;
 
 struct Counters {
   uint32_t inner, leaf, tests, status;
@@ -229,8 +235,14 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   if (++s.visits >= kd.max_visits) {
     c.status = 1;
     s.live = false;
+    s.visits = kTruncated;
+    if (kd.trunc) atomicAdd(kd.trunc, 1u);
   }
 }
+
+// The walk ended at the leaf-visit cap (its hit, if any, is the closest one
+// found among the leaves it reached).
+__device__ __forceinline__ bool trav_truncated(const Trav& s) { return s.visits == kTruncated; }
 
 __device__ __forceinline__ void trav_result(const Trav& s, HitState& hs) {
   if (s.best_id >= 0) {
@@ -250,13 +262,15 @@ __device__ __forceinline__ void trav_result(const Trav& s, HitState& hs) {
   }
 }
 
+// Runs one ray to the end; returns true when it stopped at the leaf-visit cap.
 template <int MODE, bool ANYHIT, bool COUNT>
-__device__ __forceinline__ void traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
+__device__ __forceinline__ bool traverse(const KdDev& kd, const uint2* snodes, V3 o, V3 d,
                                          float tmax, uint32_t start, HitState& hs, Counters& c) {
   Trav s;
   trav_init(s, kd, o, d, tmax, start);
   while (s.live) trav_step<MODE, ANYHIT, COUNT>(s, kd, snodes, c);
   trav_result(s, hs);
+  return trav_truncated(s);
 }
 
 __device__ __forceinline__ void stage_nodes(const KdDev& kd, uint2* snodes) {

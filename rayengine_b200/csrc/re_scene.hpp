@@ -7,13 +7,20 @@
 #include "kd_build.hpp"
 #include "../../include/rayengine_b200.h"
 
+// 16 32-bit counters per scene (64 bytes)
+#define RE_SCENE_TRUNC_SLOT 8
+#define RE_SCENE_RESET_BYTES (4 * (RE_SCENE_TRUNC_SLOT + 1))
+
 struct re_scene {
   int device = 0;
   re::FlatTree host;
   uint2* d_nodes = nullptr;
   float4* d_leaves = nullptr;
   float4* d_tris = nullptr;
-  uint32_t* d_counters = nullptr;  // [0] tiles, [1] queue size, [2] queue chunks
+  // [0] tile cursor, [1] queue size, [2] queue cursor, [3] secondary rays,
+  // [RE_SCENE_TRUNC_SLOT] rays of the last trace call stopped at the
+  // leaf-visit cap; every trace call clears the first RE_SCENE_RESET_BYTES
+  uint32_t* d_counters = nullptr;
   float4* d_queue = nullptr;
   size_t queue_cap = 0;  // rays
   uint32_t max_visits = 16384;

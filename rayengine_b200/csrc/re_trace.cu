@@ -27,7 +27,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <new>
 
 #include "kd_build.hpp"
@@ -206,6 +205,11 @@ __global__ void __launch_bounds__(256, 5) k_rays(KdDev kd, const float4* __restr
   refill_walk<MODE, ANYHIT, false>(kd, snodes, n, refill_min, counter, gen, done);
 }
 
+// Pixel mask bit of the AO frame: one of the pixel's rays (primary, shadow
+// or AO) stopped at the leaf-visit cap.  Bits 0..5: hit, light visible, AO
+// rays 1..4 unoccluded.
+constexpr uint32_t kMaskTruncated = 1u << 6;
+
 // Primary + secondary-ray generation for the AO frame.
 struct AoDev {
   V3 light;
@@ -267,12 +271,13 @@ __global__ void __launch_bounds__(256, 5) k_ao_primary(KdDev kd, CamDev cam, AoD
     V3 o = {0, 0, 0}, d = {0, 0, 1};
     if (valid) {
       generate_ray(cam, w, h, x, y, o, d);
-      traverse<0, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), 0u, hs, c);
+      bool cut = traverse<0, false, COUNT>(kd, snodes, o, d, __int_as_float(0x7f800000), 0u,
+                                           hs, c);
       ++rays;
       size_t pix = (size_t)y * w + x;
       if (!COUNT) {
         store_hit(out, pix, hs);
-        mask[pix] = hs.id >= 0 ? 1u : 0u;
+        mask[pix] = (hs.id >= 0 ? 1u : 0u) | (cut ? kMaskTruncated : 0u);
       }
     }
     bool hit = valid && hs.id >= 0;
@@ -389,7 +394,11 @@ __global__ void __launch_bounds__(256, 5) k_ao_secondary(KdDev kd, AoDev ao, AoQ
     }
     if (s.live) {
       trav_step<0, true, COUNT>(s, kd, snodes, c);
-      if (!s.live && !COUNT && s.best_id < 0) atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
+      if (!s.live && !COUNT) {
+        uint32_t bits = (s.best_id < 0 ? 1u << (tag & 7u) : 0u) |
+                        (trav_truncated(s) ? kMaskTruncated : 0u);
+        if (bits) atomicOr(&mask[tag >> 3], bits);
+      }
     }
   }
   if (COUNT) flush_counts(c, rays, totals + 4);
@@ -417,6 +426,7 @@ KdDev kd_view(const re_scene* s) {
   kd.bmax = {s->host.bmax[0], s->host.bmax[1], s->host.bmax[2]};
   kd.max_visits = s->max_visits;
   kd.stage = s->stage;
+  kd.trunc = s->d_counters + RE_SCENE_TRUNC_SLOT;
   return kd;
 }
 
@@ -543,7 +553,7 @@ re_status launch_primary(re_scene* s, const re_camera& cam, uint32_t w, uint32_t
   size_t smem = kd.stage * sizeof(uint2);
   uint32_t refill = s->tune.ray_refill_min;
   auto k = refill >= 32u ? k_primary_tiles<MODE, COUNT> : k_primary<MODE, COUNT>;
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st));
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, w, h, out, counts, s->d_counters, refill);
   RE_CHECK_LAUNCH(COUNT ? "re_count_primary: launch" : "re_trace_primary: launch");
@@ -556,7 +566,7 @@ re_status launch_rays(re_scene* s, const float4* rays, uint32_t n, re_hit* out, 
   size_t smem = kd.stage * sizeof(uint2);
   uint32_t refill = s->tune.ray_refill_min;
   auto k = refill >= 32u ? k_rays_chunks<MODE, ANYHIT> : k_rays<MODE, ANYHIT>;
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 4, st));
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<grid_for(k, smem), 256, smem, st>>>(kd, rays, n, out, s->d_counters, refill);
   RE_CHECK_LAUNCH("re_trace_rays: launch");
@@ -696,6 +706,15 @@ RE_API re_status re_count_primary(re_scene* s, const re_camera* cam, uint32_t w,
   return re::launch_primary<0, true>(s, *cam, w, h, nullptr, c4, (cudaStream_t)stream);
 }
 
+RE_API re_status re_scene_truncated(const re_scene* s, uint32_t* d_count, void* stream) {
+  re_status st = re::check_scene(s, "re_scene_truncated");
+  if (st != RE_OK) return st;
+  if (!d_count) return re::fail(RE_ERR_INVALID_ARG, "re_scene_truncated: null output");
+  RE_CUDA(cudaMemcpyAsync(d_count, s->d_counters + RE_SCENE_TRUNC_SLOT, 4,
+                          cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return RE_OK;
+}
+
 RE_API re_status re_trace_rays(re_scene* s, const re_ray* d_rays, uint32_t n, uint32_t flags,
                                re_hit* d_out, void* stream) {
   re_status st = re::check_scene(s, "re_trace_rays");
@@ -753,7 +772,7 @@ re_status ao_primary(re_scene* s, const CamDev& cd, const AoDev& ao, uint32_t w,
                      cudaStream_t st) {
   KdDev kd = kd_view(s);
   size_t smem = kd.stage * sizeof(uint2);
-  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, 16, st));
+  RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   auto k = k_ao_primary<COUNT>;
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, ao, w, h, d_primary, d_mask,
@@ -848,31 +867,20 @@ namespace {
 constexpr size_t kNoAllocCounterBytes = 256;
 constexpr size_t kNoAllocQueueBytes = (size_t)5 * 32 * RE_NOALLOC_MAX_PIXELS;
 constexpr size_t kNoAllocScratchBytes = kNoAllocCounterBytes + kNoAllocQueueBytes;
-constexpr int kNoAllocMaxDevices = 64;
 
 // counters (tile cursor, queue size, queue cursor) followed by the queue
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the symbol's name is only a host-side handle; the address comes from
-// cudaGetSymbolAddress, looked up once per device with that device current.
+// cudaGetSymbolAddress with the device current.  It is looked up on every
+// call (a lookup allocates nothing), so no address outlives the context it
+// belongs to: after a device reset the next call finds the new one.
 re_status noalloc_scratch(unsigned char** out) {
-  int dev = -1;
-  RE_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return fail(RE_ERR_LIMIT, "re_render_ao_noalloc: device ordinal %d >= %d", dev,
-                kNoAllocMaxDevices);
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+  *out = static_cast<unsigned char*>(p);
   return RE_OK;
 }
 
@@ -900,6 +908,7 @@ RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam, uint32_
   float4* queue = reinterpret_cast<float4*>(scratch + re::kNoAllocCounterBytes);
   cudaStream_t st = (cudaStream_t)stream;
   re::KdDev kd = re::kd_view(s);
+  kd.trunc = counters + RE_SCENE_TRUNC_SLOT;
   re::CamDev cd = re::cam_view(*cam);
   re::AoDev ao;
   ao.light = {p->light_dir[0], p->light_dir[1], p->light_dir[2]};
@@ -908,7 +917,7 @@ RE_API re_status re_render_ao_noalloc(re_scene* s, const re_camera* cam, uint32_
   ao.seed = p->seed;
   size_t smem = kd.stage * sizeof(uint2);
   // the array keeps the previous call's contents: the cursors must restart at zero
-  RE_CUDA(cudaMemsetAsync(counters, 0, 16, st));
+  RE_CUDA(cudaMemsetAsync(counters, 0, RE_SCENE_RESET_BYTES, st));
   {
     auto k = re::k_ao_primary<false>;
     RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -150,3 +150,30 @@ def test_batch_with_many_terrain_seeds_bit_exact(cuda):
         assert np.array_equal(b.render(graph=True).cpu().numpy(), rad)
     for m in meshes:
         m.close()
+
+
+def test_wait_bounds_run_out_and_the_next_frame_recovers(cuda):
+    """The persistent kernel bounds its loop and its polls of queue slots.
+    Lowered bounds must make a frame end early with the error flag set (no
+    wait runs on), and the next frame with the default bounds must be whole
+    again.  Two trips of the loop cannot finish a depth-4 path (each bounce
+    ray is claimed in a later trip than the ray that made it), so the
+    loop-bound case always trips; the second case also lowers the poll bound."""
+    specs, meshes = _build(cuda)
+    with rb.Batch(specs, max_depth=DEPTH, seed=SEED, mesh_bias=BIAS) as b:
+        ref = b.render().cpu().numpy()
+        assert b.stats()["error"] == 0
+        for pending, trips in ((0, 2), (64, 4096)):
+            b.set_wait_bounds(pending, trips)
+            for graph in (False, True):
+                b.render(graph=graph)
+                torch.cuda.synchronize()
+                st = b.stats()
+                assert st["error"] == 1, (pending, trips, graph)
+            b.set_wait_bounds(0, 0)
+            assert np.array_equal(b.render().cpu().numpy(), ref)
+            assert b.stats()["error"] == 0
+            assert np.array_equal(b.render(graph=True).cpu().numpy(), ref)
+            assert b.stats()["error"] == 0
+    for m in meshes:
+        m.close()

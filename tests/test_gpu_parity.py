@@ -30,8 +30,12 @@ def _hits(t):
     return t.cpu().numpy().reshape(-1, 4)
 
 
-def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels, mode=0):
-    """Reference-as-shipped comparison with the FP64 edge-margin exemption."""
+def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels, mode=0, label=None):
+    """Reference-as-shipped comparison with the FP64 edge-margin exemption.
+
+    Returns a report: rays compared, hits, id mismatches (every one of them
+    must be edge-margin exempt), and the largest t/u/v relative difference on
+    the rays whose ids agree (bound REL_TOL).  Printed when `label` is given."""
     bf = po.primary_bruteforce(packed, st["bmin"], st["bmax"], cam, w, h, mode=mode, pixels=pixels)
     g = got[pixels].view(np.int32).reshape(-1, 4)
     gid, bid = g[:, 0], bf["id"]
@@ -49,7 +53,12 @@ def _assert_vs_bruteforce(got, packed, st, cam, w, h, pixels, mode=0):
     gf = g[same, 1:].view(np.float32)
     bfv = np.stack([bf["t"], bf["u"], bf["v"]], 1)[same]
     rel = np.abs(gf - bfv) / np.maximum(np.abs(bfv), 1e-3)
-    assert rel.max(initial=0) <= REL_TOL
+    rel_max = float(rel.max(initial=0))
+    assert rel_max <= REL_TOL
+    report = {"rays": int(len(pixels)), "hits": int((bid >= 0).sum()),
+              "id_mismatch_edge_exempt": int(exempt), "max_rel_tuv": rel_max}
+    if label:
+        print(f"parity vs reference brute force [{label}]: {report}")
     return exempt, int((bid >= 0).sum())
 
 
@@ -328,3 +337,53 @@ def test_tunings_give_identical_frames(cuda):
                                                      cfg.ao_length, cfg.bias, cfg.ao_seed)]
         for a, b in zip(got, ref):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("cap", [1, 2])
+def test_visit_cap_is_reported(cuda, cap):
+    """The reference stops a walk after 50 leaves without saying so
+    (ray_functions.cuh:284).  Here a walk that reaches max_leaf_visits stops
+    too, with the closest hit among the leaves it reached, and is reported:
+    the per-ray status of re_count_primary, the scene's truncated-ray count
+    and bit 6 of the AO mask, each equal to the oracle's."""
+    cfg = rb.configs.SoupConfig(num_tris=8192, width=160, height=120)
+    packed = cfg.packed()
+    cam = cfg.camera()
+    W, H = cfg.width, cfg.height
+    with rb.KDScene.from_packed(packed, rb.kd_params(leaf_size=8, max_leaf_visits=cap)) as sc:
+        st, kd = _kd(sc)
+        ref, rc = po.primary_kd(kd, cam, W, H, max_visits=cap, counts=True)
+        got = _hits(sc.trace_primary(cam, W, H))
+        assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4))
+        n_cut = int((rc["status"] == 1).sum())
+        assert n_cut > 100
+        assert sc.truncated() == n_cut
+        cnt = sc.count_primary(cam, W, H).cpu().numpy()
+        assert np.array_equal(cnt[:, 3], rc["status"].astype(np.int32))
+        assert sc.truncated() == n_cut
+    hcfg = rb.configs.HeightfieldConfig(cells=96, width=200, height=120)
+    verts, faces = po.heightfield(po.perm(hcfg.seed), hcfg.cells, hcfg.lo, hcfg.hi,
+                                  hcfg.octaves, hcfg.amplitude)
+    packed = rb.pack_triangles(verts, faces)
+    hcam = hcfg.camera()
+    light = rb.unit(hcfg.light_dir)
+    hcap = 4 * cap  # 4: 1.7k of 24k pixels hit; 8: 9.8k (both with truncated shadow/AO rays)
+    with rb.KDScene.from_mesh(verts, faces, rb.kd_params(max_leaf_visits=hcap)) as sc:
+        st, kd = _kd(sc)
+        hits, mask, nsec = sc.render_ao(hcam, hcfg.width, hcfg.height, light, hcfg.ao_length,
+                                        hcfg.bias, hcfg.ao_seed)
+        cut = sc.truncated()
+        rh, rm, rn, tot = po.frame_ao(kd, packed, hcam, hcfg.width, hcfg.height, light,
+                                      hcfg.ao_length, hcfg.bias, hcfg.ao_seed, max_visits=hcap,
+                                      totals=True)
+        assert np.array_equal(_hits(hits), rh.view(np.int32).reshape(-1, 4))
+        assert np.array_equal(mask.cpu().numpy().view(np.uint32), rm)
+        assert int(nsec.item()) == rn
+        assert cut == int(tot[8] + tot[9]) and tot[8] > 0 and tot[9] > 0
+        assert ((rm >> 6) & 1).sum() > 0
+    # without a cap in reach nothing is reported
+    with rb.KDScene.from_mesh(verts, faces) as sc:
+        _, mask, _ = sc.render_ao(hcam, hcfg.width, hcfg.height, light, hcfg.ao_length,
+                                  hcfg.bias, hcfg.ao_seed)
+        assert sc.truncated() == 0
+        assert not ((mask.cpu().numpy().view(np.uint32) >> 6) & 1).any()

@@ -16,8 +16,9 @@ import pytest
 
 import rayengine_b200 as rb
 from oracle import pyoracle as po
+from oracle.refpath import reference_file
 
-MESHES = "/root/reference/Sandbox/Meshes"
+MESHES = reference_file("Sandbox", "Meshes") or ""
 
 
 def _write_ply(path, verts, polys, fmt):

@@ -34,12 +34,17 @@ def _frame(entry, sc, cam, w, h, params):
     return primary.cpu().numpy(), mask.cpu().numpy(), int(nsec.item())
 
 
-def test_noalloc_matches_render_ao_twice(cuda):
+@pytest.mark.parametrize("kind_major", [0, 1])
+def test_noalloc_matches_render_ao_twice(cuda, kind_major):
+    """Both secondary-queue layouts (pixel-major and kind-major, whose kind
+    stride is w*h inside the fixed array)."""
     cfg = rb.configs.HeightfieldConfig(cells=128, width=320, height=180)
     verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
                                   cfg.amplitude)
     cam = cfg.camera()
     with rb.KDScene.from_mesh(verts, faces) as sc:
+        t = sc.tuning()
+        sc.set_tuning(t["stage_nodes"], kind_major, t["refill_min"])
         for seed in (cfg.ao_seed, cfg.ao_seed + 1):
             params = rb.ao_params(cfg.light_dir, cfg.ao_length, cfg.bias, seed)
             want = _frame("re_render_ao", sc, cam, cfg.width, cfg.height, params)
@@ -47,6 +52,30 @@ def test_noalloc_matches_render_ao_twice(cuda):
             assert np.array_equal(got[0], want[0]), seed
             assert np.array_equal(got[1], want[1]), seed
             assert got[2] == want[2] and got[2] > 0, seed
+
+
+@pytest.mark.parametrize("kind_major", [0, 1])
+def test_noalloc_largest_image(cuda, kind_major):
+    """An image of 1024 x 409 = 418,816 pixels, just under the limit, with
+    the camera close to the terrain so that almost every pixel hits: the
+    queue's last records are written and read."""
+    cfg = rb.configs.HeightfieldConfig(cells=128, width=1024, height=409,
+                                       campos=(0.0, 3.0, -6.0))
+    verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
+                                  cfg.amplitude)
+    cam = cfg.camera()
+    assert cfg.width * cfg.height <= MAX_PIXELS
+    with rb.KDScene.from_mesh(verts, faces) as sc:
+        t = sc.tuning()
+        sc.set_tuning(t["stage_nodes"], kind_major, t["refill_min"])
+        params = rb.ao_params(cfg.light_dir, cfg.ao_length, cfg.bias, cfg.ao_seed)
+        want = _frame("re_render_ao", sc, cam, cfg.width, cfg.height, params)
+        for _ in range(2):
+            got = _frame("re_render_ao_noalloc", sc, cam, cfg.width, cfg.height, params)
+            assert np.array_equal(got[0], want[0])
+            assert np.array_equal(got[1], want[1])
+            assert got[2] == want[2]
+        assert want[2] > 0.9 * 5 * cfg.width * cfg.height
 
 
 def test_noalloc_rejects_images_beyond_its_scratch(cuda):

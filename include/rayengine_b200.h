@@ -309,6 +309,61 @@ RE_API re_status re_sdf_trace(const re_sdf_params* p, const re_camera* cam,
                               uint32_t w, uint32_t h, re_sdf_hit* d_out,
                               void* stream);
 
+/* ---- shaded SDF terrain frame ----------------------------------------
+ * The reference's live render path: with `sphere_tracing` defined
+ * (RE/RayEngine/RayEngine.h:22) cuda_render_frame (renderer.cu:702-738)
+ * runs render_sphere_trace (renderer.cu:143-285): march, shade
+ * (paint_surface and the soft-shadowed light of sphere_trace_shadow,
+ * sphere_tracing.cuh:246-273,322-360,408-477), atmosphere sky for misses
+ * (compute_incident_light, material_functions.cuh:296-344), fog, gamma,
+ * vignetting, rgbaFloatToInt (cuda_helper_functions.h:61-68).  Here the
+ * terrain is the exact field of re_sdf_params, traced by re_sdf_trace.
+ * Output: W x H packed RGBA8 (R in the low byte, alpha 255). */
+#define RE_SDF_SHADE 1u      /* soft shadow + light terms (the reference's should_shade) */
+#define RE_SDF_FOG 2u        /* apply_fog (SceneSettings::enable_fog)                  */
+#define RE_SDF_GAMMA 4u      /* colour^(1/2.2) (RenderingSettings::gamma)               */
+#define RE_SDF_VIGNETTING 8u /* RenderingSettings::vignetting                           */
+
+typedef struct re_sdf_shade_params {
+  float light_pos[2];       /* SceneSettings::light_pos (x, y): the light is at (x, y, x) */
+  float light_intensity;    /* colour (0.86,0.80,0.45) * I / (4 pi |light|^2)           */
+  float soft_shadow_k;      /* penumbra factor, SceneSettings::soft_shadow_k (32)       */
+  float shadow_tmin;        /* shadow march start along the light direction (> 0)      */
+  float shadow_tmax;        /* shadow march end                                         */
+  uint32_t shadow_max_steps;/* field evaluations per shadow ray (<= 4096)              */
+  float sun_dir[3];         /* atmosphere sun direction, unit length                   */
+  float max_y;              /* terrain volume top: ocean below 0.2 max_y, snow above 0.8 */
+  float fog_density;        /* SceneSettings::fog_deisity (RE_SDF_FOG)                 */
+  float vignetting_k;       /* RenderingSettings::vignetting_k (RE_SDF_VIGNETTING)     */
+  uint32_t flags;           /* RE_SDF_*                                                 */
+} re_sdf_shade_params;
+
+RE_API void re_sdf_shade_params_default(re_sdf_shade_params* s);
+/* The shading pass alone over a hit record from re_sdf_trace (or
+ * re_nsdf_trace); d_evals (device, may be NULL) accumulates the shadow
+ * rays' field evaluations. */
+RE_API re_status re_sdf_shade(const re_sdf_params* field, const re_sdf_shade_params* shade,
+                              const re_camera* cam, uint32_t w, uint32_t h,
+                              const re_sdf_hit* d_hits, uint32_t* d_rgba,
+                              uint64_t* d_evals, void* stream);
+/* Trace (into the caller's w*h d_hits) and shade one frame. */
+RE_API re_status re_render_sdf_frame(const re_sdf_params* field,
+                                     const re_sdf_shade_params* shade,
+                                     const re_camera* cam, uint32_t w, uint32_t h,
+                                     re_sdf_hit* d_hits, uint32_t* d_rgba, void* stream);
+/* State for cuda_render_frame() in the reference's shipped mode, the
+ * counterpart of initialize_volume_render (sphere_tracing.cuh:617-755): the
+ * next cuda_render_frame calls render this terrain until re_frame_bind binds
+ * a mesh scene again.  animate_sun != 0 moves the sun after every frame as
+ * Craze does (renderer.cu:287-298). */
+RE_API re_status re_sdf_frame_bind(const re_sdf_params* field,
+                                   const re_sdf_shade_params* shade,
+                                   const re_camera* cam, int animate_sun);
+/* The frame's elementary functions over device arrays (fn 0: e^x, 1: ln x,
+ * 2: x^y), for checking them against CUDA's. */
+RE_API re_status re_fmath(uint32_t fn, const float* d_x, const float* d_y, uint32_t n,
+                          float* d_out, void* stream);
+
 /* ---- neural SDF surrogate ------------------------------------------
  * No counterpart in the reference (it has no learned component): a
  * Fourier-feature MLP (3 -> 128 features -> 4 x 64 softplus -> 1) that
@@ -619,8 +674,10 @@ RE_API re_status re_measure_l2_read(size_t bytes, uint32_t passes, float* gbs, v
 #ifdef __cplusplus
 }
 /* The reference's render call, same C++ signature (renderer.cu:701):
- * renders the state bound by re_frame_bind into `output` (device, W x H
- * RGBA8) and waits; errors go to re_last_error(). */
+ * renders the state bound by re_sdf_frame_bind (the reference's shipped
+ * SDF mode) or re_frame_bind (its kd-tree mode), whichever was bound last,
+ * into `output` (device, W x H RGBA8) and waits; errors go to
+ * re_last_error(). */
 void cuda_render_frame(unsigned int* output, const unsigned int& width,
                        const unsigned int& heigth);
 #endif

@@ -118,6 +118,30 @@ void o_sdf_trace(const uint32_t perm[512], const float o[3], const float d[3],
                  int octaves, float scale, float amp, float step_factor,
                  float eps, float tmax, uint32_t max_steps, o_sdf_hit* out);
 
+/* --- shaded SDF terrain frame (oracle_sdf_frame.c) ---------------------- */
+typedef struct {
+  uint32_t octaves;
+  float scale, amp, step_factor, eps, tmax;
+  uint32_t max_steps;
+} o_sdf_field;
+
+/* same field order as re_sdf_shade_params */
+typedef struct {
+  float light_pos[2];
+  float light_intensity, soft_shadow_k, shadow_tmin, shadow_tmax;
+  uint32_t shadow_max_steps;
+  float sun_dir[3];
+  float max_y, fog_density, vignetting_k;
+  uint32_t flags; /* 1 shade, 2 fog, 4 gamma, 8 vignetting */
+} o_sdf_shade;
+
+float o_fm_exp(float x);
+float o_fm_log(float x);
+float o_fm_pow(float x, float y);
+uint32_t o_sdf_shade_pixel(const uint32_t perm[512], const o_sdf_field* f, const o_sdf_shade* s,
+                           const float o[3], const float d[3], const o_sdf_hit* hit, float u,
+                           float v, uint32_t* evals);
+
 /* --- deterministic sampling shared with the kernels -------------------- */
 uint32_t o_hash_u32(uint32_t a, uint32_t b, uint32_t c);
 void o_sincos_2pi(float u, float* s, float* c);

@@ -388,6 +388,38 @@ def sdf_arbiter(p, cam, w, h, pixels, octaves=8, scale=0.25, amp=3.0, factor=0.6
     return out[:, :3], out[:, 3] > 0.5
 
 
+class OSdfField(ctypes.Structure):
+    _fields_ = [("octaves", ctypes.c_uint32), ("scale", ctypes.c_float), ("amp", ctypes.c_float),
+                ("step_factor", ctypes.c_float), ("eps", ctypes.c_float),
+                ("tmax", ctypes.c_float), ("max_steps", ctypes.c_uint32)]
+
+
+def sdf_frame(p, cam, w, h, field, shade, pixels=None, nthreads=0, evals=False):
+    """Oracle RGBA8 values (uint32) of the shaded terrain frame on `pixels`
+    (all pixels when None).  field: product re_sdf_params; shade: product
+    re_sdf_shade_params (the same bytes as o_sdf_shade)."""
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    n = w * h if pix is None else pix.shape[0]
+    out = np.zeros(n, np.uint32)
+    ev = np.zeros(n, np.uint32) if evals else None
+    f = OSdfField(field.octaves, field.scale, field.amplitude, field.step_factor, field.eps,
+                  field.tmax, field.max_steps)
+    oc = camera(cam)
+    lib().o_batch_sdf_frame(_p(p), ctypes.byref(oc), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                            ctypes.byref(f), ctypes.byref(shade), _p(pix), ctypes.c_int64(n),
+                            _p(out), _p(ev), ctypes.c_int(nthreads))
+    return (out, ev) if evals else out
+
+
+def fmath(fn, x, y=None):
+    """The oracle's elementary functions (0: e^x, 1: ln x, 2: x^y) over float32 arrays."""
+    x = np.ascontiguousarray(x, np.float32)
+    yy = None if y is None else np.ascontiguousarray(y, np.float32)
+    out = np.zeros_like(x)
+    lib().o_batch_fmath(ctypes.c_uint32(fn), _p(x), _p(yy), ctypes.c_int64(x.size), _p(out))
+    return out
+
+
 def hit_errors(sdf_out, arbiter_pos, arbiter_hit, pixels):
     """Per-pixel |p_gpu - p_fp64| where both hit, plus hit/miss disagreements."""
     o = np.asarray(sdf_out)

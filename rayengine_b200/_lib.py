@@ -121,6 +121,25 @@ class re_sdf_params(ctypes.Structure):
     ]
 
 
+class re_sdf_shade_params(ctypes.Structure):
+    _fields_ = [
+        ("light_pos", ctypes.c_float * 2),
+        ("light_intensity", ctypes.c_float),
+        ("soft_shadow_k", ctypes.c_float),
+        ("shadow_tmin", ctypes.c_float),
+        ("shadow_tmax", ctypes.c_float),
+        ("shadow_max_steps", ctypes.c_uint32),
+        ("sun_dir", ctypes.c_float * 3),
+        ("max_y", ctypes.c_float),
+        ("fog_density", ctypes.c_float),
+        ("vignetting_k", ctypes.c_float),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+SDF_SHADE, SDF_FOG, SDF_GAMMA, SDF_VIGNETTING = 1, 2, 4, 8
+
+
 class re_nsdf_config(ctypes.Structure):
     _fields_ = [
         ("box_min", ctypes.c_float * 3),
@@ -230,6 +249,11 @@ _SIGS = {
     "re_gen_soup": (ctypes.c_int, [ctypes.c_uint64, _U32, _P]),
     "re_gen_grid_faces": (ctypes.c_int, [_U32, _P]),
     "re_sdf_trace": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P]),
+    "re_sdf_shade_params_default": (None, [ctypes.POINTER(re_sdf_shade_params)]),
+    "re_sdf_shade": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_sdf_shade_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P, _P, _P]),
+    "re_render_sdf_frame": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_sdf_shade_params), ctypes.POINTER(re_camera), _U32, _U32, _P, _P, _P]),
+    "re_sdf_frame_bind": (ctypes.c_int, [ctypes.POINTER(re_sdf_params), ctypes.POINTER(re_sdf_shade_params), ctypes.POINTER(re_camera), ctypes.c_int]),
+    "re_fmath": (ctypes.c_int, [_U32, _P, _P, _U32, _P, _P]),
     "re_nsdf_num_params": (ctypes.c_uint32, []),
     "re_nsdf_box_for_camera": (ctypes.c_int, [ctypes.POINTER(re_camera), _U32, _U32, _F, _F, _F, _P, _P]),
     "re_nsdf_create": (ctypes.c_int, [ctypes.POINTER(re_nsdf_config), ctypes.POINTER(_P)]),

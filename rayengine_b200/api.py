@@ -390,6 +390,72 @@ def sphere_trace(params, cam: RCamera, w: int, h: int, out=None, stream=None):
     return out
 
 
+# ------------------------------------------------- shaded SDF terrain frame
+SDF_SHADE, SDF_FOG, SDF_GAMMA, SDF_VIGNETTING = (_lib.SDF_SHADE, _lib.SDF_FOG, _lib.SDF_GAMMA,
+                                                 _lib.SDF_VIGNETTING)
+
+
+def sdf_shade_params(**kw):
+    """re_sdf_shade_params: the library's defaults, overridden by keywords
+    (light_pos=(x, y), light_intensity, soft_shadow_k, shadow_tmin,
+    shadow_tmax, shadow_max_steps, sun_dir, max_y, fog_density,
+    vignetting_k, flags)."""
+    p = _lib.re_sdf_shade_params()
+    lib.re_sdf_shade_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if k in ("light_pos", "sun_dir"):
+            getattr(p, k)[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def render_sdf_frame(field, shade, cam: RCamera, w: int, h: int, hits=None, out=None,
+                     stream=None):
+    """The shaded terrain frame (render_sphere_trace): trace into `hits`
+    ((h*w, 8) int32 = re_sdf_hit) and shade into `out` ((h*w,) int32 RGBA8).
+    Returns (out, hits)."""
+    import torch
+
+    if hits is None:
+        hits = torch.empty((h * w, 8), dtype=torch.int32, device="cuda")
+    if out is None:
+        out = torch.empty(h * w, dtype=torch.int32, device="cuda")
+    call("re_render_sdf_frame", ctypes.byref(field), ctypes.byref(shade), ctypes.byref(cam), w, h,
+         _dptr(hits), _dptr(out), _stream_ptr(stream))
+    return out, hits
+
+
+def shade_sdf(field, shade, cam: RCamera, w: int, h: int, hits, out=None, evals=None,
+              stream=None):
+    """The shading pass alone over a hit record -> RGBA8 (h*w,) int32."""
+    import torch
+
+    if out is None:
+        out = torch.empty(h * w, dtype=torch.int32, device="cuda")
+    call("re_sdf_shade", ctypes.byref(field), ctypes.byref(shade), ctypes.byref(cam), w, h,
+         _dptr(hits), _dptr(out), _dptr(evals) if evals is not None else None,
+         _stream_ptr(stream))
+    return out
+
+
+def bind_sdf_frame(field, shade, cam: RCamera, animate_sun=False):
+    """State for cuda_render_frame() in the reference's shipped SDF mode."""
+    call("re_sdf_frame_bind", ctypes.byref(field), ctypes.byref(shade), ctypes.byref(cam),
+         1 if animate_sun else 0)
+
+
+def fmath(fn: int, x, y=None, out=None, stream=None):
+    """The frame's elementary functions on CUDA float tensors (0: e^x, 1: ln x, 2: x^y)."""
+    import torch
+
+    if out is None:
+        out = torch.empty_like(x)
+    call("re_fmath", fn, _dptr(x), _dptr(y) if y is not None else None, x.numel(), _dptr(out),
+         _stream_ptr(stream))
+    return out
+
+
 # ------------------------------------------------------ neural SDF surrogate
 def nsdf_trace_params(lipschitz=1.0, safety=0.9, switch_dist=0.05, min_step=1e-3,
                       max_network_steps=256, max_exact_steps=0, root_steps=4, relax=1.0,

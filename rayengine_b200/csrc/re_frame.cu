@@ -134,6 +134,10 @@ __device__ __forceinline__ void shade_pixel(const KdDev& kd, const uint2* snodes
 }  // namespace re
 
 namespace re {
+// SDF mode of cuda_render_frame (re_sdf_frame.cu)
+bool sdf_render_bound(unsigned int* output, unsigned int width, unsigned int height);
+void sdf_unbind();
+
 namespace {
 
 using namespace frame;
@@ -235,6 +239,7 @@ RE_API re_status re_frame_bind(re_scene* s, const re_camera* cam, const re_light
   if (!s || !cam || !sp || (num_lights && !lights))
     return re::fail(RE_ERR_INVALID_ARG, "re_frame_bind: bad arguments");
   if (num_lights > kMaxLights) return re::fail(RE_ERR_LIMIT, "re_frame_bind: more than %u lights", kMaxLights);
+  re::sdf_unbind();
   re::Bound& b = re::bound();
   std::lock_guard<std::mutex> lk(b.mu);
   b.scene = s;
@@ -258,10 +263,12 @@ RE_API re_status re_frame_bind(re_scene* s, const re_camera* cam, const re_light
 __attribute__((visibility("default"))) void cuda_render_frame(unsigned int* output,
                                                               const unsigned int& width,
                                                               const unsigned int& heigth) {
+  if (re::sdf_render_bound(output, width, heigth)) return;
   re::Bound& b = re::bound();
   std::lock_guard<std::mutex> lk(b.mu);
   if (!b.scene) {
-    re::fail(RE_ERR_INVALID_ARG, "cuda_render_frame: nothing bound (re_frame_bind)");
+    re::fail(RE_ERR_INVALID_ARG,
+             "cuda_render_frame: nothing bound (re_sdf_frame_bind or re_frame_bind)");
     return;
   }
   if (re_render_frame(b.scene, &b.cam, b.lights, b.num_lights, &b.sp, width, heigth, output,

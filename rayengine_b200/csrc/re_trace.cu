@@ -86,15 +86,17 @@ __device__ __forceinline__ void refill_walk(const KdDev& kd, const uint2* snodes
   }
 }
 
-// The primary and caller-ray kernels are bounded to 5 blocks of 256 threads
-// per SM (48 registers): measured faster on B200 than the 4 blocks their
-// unbounded 60-register builds reach, despite a few bytes of spills.
+// Launch bounds measured on B200: the primary and caller-ray kernels run 6
+// blocks of 256 threads per SM (40 registers, a few dozen bytes of spills):
+// the 2^20-triangle soup's primary pass is 3 % faster than at 5 blocks (48
+// registers) and 9 % faster than at 4; the AO frame's kernels keep 5 blocks
+// (at 6 its secondary pass is 2.6 % slower).
 //
 // Primary rays, persistent warps over 8x4 pixel tiles, each lane running its
 // ray to the end (ray_refill_min 32: no per-leaf bookkeeping; fastest when
 // rays of a tile take similar work).
 template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(256, 5) k_primary_tiles(KdDev kd, CamDev cam, uint32_t w,
+__global__ void __launch_bounds__(256, 6) k_primary_tiles(KdDev kd, CamDev cam, uint32_t w,
                                                        uint32_t h, re_hit* __restrict__ out,
                                                        uint4* __restrict__ counts,
                                                        uint32_t* __restrict__ tile_counter,
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(256, 5) k_primary_tiles(KdDev kd, CamDev cam, 
 // i % 32 of 8x4 pixel tile i / 32, so a warp's claims stay in one screen
 // region.
 template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(256, 5) k_primary(KdDev kd, CamDev cam, uint32_t w, uint32_t h,
+__global__ void __launch_bounds__(256, 6) k_primary(KdDev kd, CamDev cam, uint32_t w, uint32_t h,
                                                  re_hit* __restrict__ out,
                                                  uint4* __restrict__ counts,
                                                  uint32_t* __restrict__ tile_counter,
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(256, 5) k_primary(KdDev kd, CamDev cam, uint32
 // Caller rays (re_ray), persistent warps over 32-ray chunks, each lane
 // running its ray to the end (ray_refill_min 32).
 template <int MODE, bool ANYHIT>
-__global__ void __launch_bounds__(256, 5) k_rays_chunks(KdDev kd, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(256, 6) k_rays_chunks(KdDev kd, const float4* __restrict__ rays,
                                                      uint32_t n, re_hit* __restrict__ out,
                                                      uint32_t* __restrict__ counter, uint32_t) {
   extern __shared__ uint2 snodes[];
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(256, 5) k_rays_chunks(KdDev kd, const float4* 
 
 // Caller rays (re_ray), lane refill over ray indices (ray_refill_min < 32).
 template <int MODE, bool ANYHIT>
-__global__ void __launch_bounds__(256, 5) k_rays(KdDev kd, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(256, 6) k_rays(KdDev kd, const float4* __restrict__ rays,
                                               uint32_t n, re_hit* __restrict__ out,
                                               uint32_t* __restrict__ counter,
                                               uint32_t refill_min) {

@@ -15,6 +15,16 @@ Fixtures:
                      obj_index_list in order, keeping t < t_exit).
   ref_grid.npz       the same for a 16x16-cell heightfield (shared edges).
   noise.npz          fBm values of the restated Perlin noise at fixed points.
+  bunny.npz          real geometry: Sandbox/Meshes/bun_zipper.ply (the Stanford
+                     bunny the reference ships, 35,947 vertices, 69,451 faces)
+                     as the reference's own rply reader returns it, and the
+                     closest-hit distances of a 128x128 primary image of the
+                     mesh scaled by 10 (the reference's absolute triangle-test
+                     epsilons reject the raw metre-sized model's triangles),
+                     traced by the reference's compiled CPU query
+                     RKDTreeCPU::singleRayStacklessIntersect.
+
+    python tests/golden/make_golden.py [--only bunny]
 """
 from __future__ import annotations
 
@@ -61,9 +71,46 @@ def traced_reference(verts, faces, cam, w, h):
     return nodes, idx, root, levels, leaves, hits
 
 
+BUNNY_SCALE = 10.0
+BUNNY_CAM = ((0.0, 1.0, 2.5), 45.0)  # offset of the camera from the bunny's centre, fov
+
+
+def bunny_camera(verts):
+    c = (verts.min(0) + verts.max(0)) / 2
+    off, fov = BUNNY_CAM
+    return _Cam((float(c[0]) + off[0], float(c[1]) + off[1], float(c[2]) + off[2]),
+                (float(c[0]), float(c[1]), float(c[2])), (fov, fov))
+
+
+def bunny():
+    from oracle.refpath import reference_file
+
+    path = reference_file("Sandbox", "Meshes", "bun_zipper.ply")
+    if path is None or po.ref_ply_lib() is None:
+        raise SystemExit("the reference checkout (bun_zipper.ply) or oracle/_ref/libre_ply.so missing")
+    ok, verts, faces = po.ref_ply_load(path)
+    assert ok and verts.shape == (35947, 3) and faces.shape == (69451, 3)
+    sv = (verts * np.float32(BUNNY_SCALE)).astype(np.float32)
+    cam = bunny_camera(sv)
+    w = h = 128
+    o, d = po.camera_rays(cam, w, h, np.arange(w * h))
+    tree = po.RefTree(sv, faces)
+    t, _, _ = tree.trace(o, d)
+    tree.close()
+    np.savez_compressed(os.path.join(HERE, "bunny.npz"), verts=verts, faces=faces,
+                        scale=np.float32(BUNNY_SCALE), campos=cam.campos, view=cam.view,
+                        fov=cam.fov, w=w, h=h, ref_t=t)
+
+
 def main():
     if po.ref_lib() is None:
         raise SystemExit("oracle/_ref/libre_ref.so missing: make -f oracle/Makefile.ref")
+    if "--only" in sys.argv:
+        which = sys.argv[sys.argv.index("--only") + 1]
+        {"bunny": bunny}[which]()
+        print("golden fixture", which, "written to", HERE)
+        return
+    bunny()
     seeds = np.array([2016, 0, 1, 7, 12345], np.uint32)
     np.savez_compressed(os.path.join(HERE, "perm.npz"), seeds=seeds,
                         tables=np.stack([po.ref_perm(int(s)) for s in seeds]))

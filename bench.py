@@ -643,6 +643,114 @@ class TerrainSDF:
 
 
 
+class SdfFrame:
+    """The reference's shipped render path (render_sphere_trace behind
+    cuda_render_frame): the terrain of TerrainSDF marched, then shaded with
+    soft shadows toward the light and the atmosphere sky for misses, packed
+    RGBA8.  Rays per frame: one primary ray per pixel plus one shadow ray per
+    hit."""
+    name = "sdf_frame"
+
+    def __init__(self, torch):
+        import rayengine_b200 as rb
+
+        self.rb = rb
+        self.fcfg = rb.configs.SdfFrameConfig()
+        self.cfg = cfg = self.fcfg.terrain
+        self.cam = cfg.camera()
+        self.params = cfg.params()
+        self.shade = self.fcfg.shade()
+        W, H = cfg.width, cfg.height
+        self.hits = torch.empty((H * W, 8), dtype=torch.int32, device="cuda")
+        self.out = torch.empty(H * W, dtype=torch.int32, device="cuda")
+        ev = torch.zeros(1, dtype=torch.int64, device="cuda")
+        rb.sphere_trace(self.params, self.cam, W, H, self.hits)
+        rb.shade_sdf(self.params, self.shade, self.cam, W, H, self.hits, self.out, evals=ev)
+        o = self.hits.cpu().numpy()
+        self.steps = int(o[:, 6].astype(np.int64).sum())
+        self.nhits = int((o[:, 7] == 1).sum())
+        self.shadow_evals = int(ev.item())
+        self.rays_per_step = W * H + self.nhits
+        self.kernels_per_step = 2
+
+    def config(self):
+        sh = self.shade
+        return {"workload": "shaded exact-SDF terrain frame d(p)=p.y-3fBm(0.25p), 1920x1080: march, "
+                            "soft shadow toward the light, Phong-style light terms, atmosphere sky "
+                            "for misses, RGBA8 (render_sphere_trace)",
+                "field_evals_per_step": {"march": self.steps, "normals": 6 * self.nhits,
+                                         "shadow": self.shadow_evals},
+                "shade": {"light_pos": list(sh.light_pos), "light_intensity": sh.light_intensity,
+                          "soft_shadow_k": sh.soft_shadow_k, "shadow_max_steps": sh.shadow_max_steps,
+                          "flags": sh.flags},
+                "rays_per_step": self.rays_per_step, "l2": "flushed between steps (256 MB write)"}
+
+    def phases(self, stream):
+        W, H = self.cfg.width, self.cfg.height
+        rb = self.rb
+        return [("sdf", lambda: rb.sphere_trace(self.params, self.cam, W, H, self.hits, stream)),
+                ("shade", lambda: rb.shade_sdf(self.params, self.shade, self.cam, W, H, self.hits,
+                                               self.out, stream=stream))]
+
+    def roofline(self, phase_ms, peaks):
+        evals = self.steps + 6 * self.nhits
+        achieved = evals * SDF_OPS_PER_EVAL / (phase_ms["sdf"] / 1e3) / 1e12
+        return {"bound": "fp32-simt", "kernel": "sdf", "achieved": round(achieved, 3),
+                "peak": round(FP32_TOPS_NOMINAL, 2), "unit": "Tops/s",
+                "frac": round(achieved / FP32_TOPS_NOMINAL, 4),
+                "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1965 MHz",
+                "alg_ops_per_launch": evals * SDF_OPS_PER_EVAL,
+                "shade_kernel": {"shadow_field_evals": self.shadow_evals,
+                                 "ms": round(phase_ms["shade"], 4)},
+                "traffic": ncu_traffic(f"{self.name}:sdf")}
+
+    def e2e_compute(self, torch, stream):
+        W, H = self.cfg.width, self.cfg.height
+        self.rb.render_sdf_frame(self.params, self.shade, self.cam, W, H, self.hits, self.out,
+                                 stream)
+
+    def e2e_outputs(self):
+        return [self.out]
+
+    def e2e_bytes(self):
+        import ctypes
+
+        return (ctypes.sizeof(self.rb.RCamera) + ctypes.sizeof(self.params) +
+                ctypes.sizeof(self.shade), self.cfg.width * self.cfg.height * 4)
+
+    def cpu_baseline(self, budget_s=12.0):
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        rng = np.random.default_rng(0)
+        n = 2000
+        P = po.perm(self.cfg.seed)
+        while True:
+            pix = rng.choice(W * H, n, replace=False).astype(np.uint32)
+            t0 = time.perf_counter()
+            po.sdf_frame(P, self.cam, W, H, self.params, self.shade, pixels=pix)
+            dt = time.perf_counter() - t0
+            if dt > budget_s / 4 or n >= W * H:
+                break
+            n = min(W * H, int(n * min(8.0, budget_s / max(dt, 1e-3))))
+        rays = n * self.rays_per_step / (W * H)
+        return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": po.threads(),
+                "kind": "port", "sample": f"{n} seeded-random pixels (primary + shadow rays "
+                                          "scaled by the frame's hit fraction); oracle march + "
+                                          "shading, OpenMP"}
+
+    def parity(self):
+        from oracle import pyoracle as po
+
+        W, H = self.cfg.width, self.cfg.height
+        got = self.out.cpu().numpy().view(np.uint32)
+        pix = np.random.default_rng(12).choice(W * H, 3000, replace=False).astype(np.uint32)
+        want = po.sdf_frame(po.perm(self.cfg.seed), self.cam, W, H, self.params, self.shade,
+                            pixels=pix)
+        return {"rgba8_vs_oracle": {"pixels": int(pix.size),
+                                    "bitexact": int((got[pix] == want).sum())}}
+
+
 class NeuralTerrainSDF:
     """The terrain of TerrainSDF traced through the neural surrogate: the
     network is trained at set-up (8M points, 20k Adam steps of 65,536), then
@@ -943,6 +1051,22 @@ def reference_workload(name):
         return ("batched path tracing of the 32-scene batch (depth 4, 1 spp), seeded-random "
                 "pixels", "oracle restatement: single-leaf build (brute-force Moller-Trumbore) "
                 "and the exact SDF march", "port", step)
+    if name == "sdf_frame":
+        fcfg = C.SdfFrameConfig()
+        cfg = fcfg.terrain
+        W, H = cfg.width, cfg.height
+        P = po.perm(cfg.seed)
+        cam = cfg.camera()
+        field = cfg.params()
+        shade = fcfg.shade()
+
+        def step(npix):
+            pix = rng.choice(W * H, npix, replace=False).astype(np.uint32)
+            img, ev = po.sdf_frame(P, cam, W, H, field, shade, pixels=pix, evals=True)
+            return npix + int((ev > 0).sum())
+        return ("shaded exact-SDF terrain frame, 1920x1080 (march, soft shadow, sky, RGBA8)",
+                "oracle restatement of render_sphere_trace (renderer.cu:143-285; the "
+                "reference's device code does not compile for the host)", "port", step)
     if name in ("terrain_sdf", "nsdf_terrain"):
         cfg = C.TerrainConfig()
         W, H = cfg.width, cfg.height
@@ -1012,6 +1136,7 @@ WORKLOADS = {
     "soup": SoupPrimary,
     "soup1m": lambda torch, **kw: SoupPrimary(torch, num_tris=1 << 20, **kw),
     "terrain_sdf": TerrainSDF,
+    "sdf_frame": SdfFrame,
     "nsdf_terrain": NeuralTerrainSDF,
     "batch32": BatchWavefront,
 }

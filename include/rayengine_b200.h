@@ -677,7 +677,8 @@ RE_API re_status re_measure_l2_read(size_t bytes, uint32_t passes, float* gbs, v
  * renders the state bound by re_sdf_frame_bind (the reference's shipped
  * SDF mode) or re_frame_bind (its kd-tree mode), whichever was bound last,
  * into `output` (device, W x H RGBA8) and waits; errors go to
- * re_last_error(). */
+ * re_last_error(), which the call empties on entry (so an empty message
+ * after it means success). */
 void cuda_render_frame(unsigned int* output, const unsigned int& width,
                        const unsigned int& heigth);
 #endif

@@ -114,6 +114,45 @@ class TerrainConfig:
 
 
 @dataclass
+class SdfFrameConfig:
+    """The shaded terrain frame: TerrainConfig's field and camera with the
+    shading settings of re_sdf_shade_params_default (the light at (20, 40,
+    20) with intensity 30000, the reference's soft-shadow factor 32, shadow
+    rays from 0.05 to 40 in at most 128 steps, the sun at 0.18 pi from the
+    zenith, terrain top 2, soft shadows and light on)."""
+    terrain: TerrainConfig = None
+    light_pos: tuple = (20.0, 40.0)
+    light_intensity: float = 30000.0
+    soft_shadow_k: float = 32.0
+    shadow_tmin: float = 0.05
+    shadow_tmax: float = 40.0
+    shadow_max_steps: int = 128
+    sun_dir: tuple = (0.0, 0.844327926, 0.535826795)  # (0, cos a, sin a), a = 0.18 pi
+    max_y: float = 2.0
+    fog_density: float = 0.02
+    vignetting_k: float = 0.25
+    flags: int = 1  # RE_SDF_SHADE
+
+    def __post_init__(self):
+        if self.terrain is None:
+            self.terrain = TerrainConfig()
+
+    def shade(self):
+        """re_sdf_shade_params built in Python (no library call)."""
+        from ._lib import re_sdf_shade_params
+
+        p = re_sdf_shade_params()
+        p.light_pos[:] = [float(x) for x in self.light_pos]
+        p.light_intensity, p.soft_shadow_k = self.light_intensity, self.soft_shadow_k
+        p.shadow_tmin, p.shadow_tmax = self.shadow_tmin, self.shadow_tmax
+        p.shadow_max_steps = self.shadow_max_steps
+        p.sun_dir[:] = [float(x) for x in self.sun_dir]
+        p.max_y, p.fog_density, p.vignetting_k = self.max_y, self.fog_density, self.vignetting_k
+        p.flags = self.flags
+        return p
+
+
+@dataclass
 class NeuralTerrainConfig:
     """Neural SDF surrogate of the terrain field above: training set, network
     and tracer settings."""

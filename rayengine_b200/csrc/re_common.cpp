@@ -19,6 +19,8 @@ void set_error(const char* fmt, ...) {
   g_last_error = buf;
 }
 
+void clear_error() { g_last_error.clear(); }
+
 re_status fail(re_status s, const char* fmt, ...) {
   char buf[512];
   va_list ap;

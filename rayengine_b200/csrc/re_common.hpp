@@ -12,6 +12,9 @@ namespace re {
 
 void set_error(const char* fmt, ...);
 re_status fail(re_status s, const char* fmt, ...);
+// Empties this thread's last-error message (entry points whose only error
+// channel is re_last_error clear it first).
+void clear_error();
 
 inline re_status cuda_fail(cudaError_t e, const char* what) {
   return fail(e == cudaErrorMemoryAllocation ? RE_ERR_OUT_OF_MEMORY : RE_ERR_CUDA,

@@ -263,6 +263,7 @@ RE_API re_status re_frame_bind(re_scene* s, const re_camera* cam, const re_light
 __attribute__((visibility("default"))) void cuda_render_frame(unsigned int* output,
                                                               const unsigned int& width,
                                                               const unsigned int& heigth) {
+  re::clear_error();
   if (re::sdf_render_bound(output, width, heigth)) return;
   re::Bound& b = re::bound();
   std::lock_guard<std::mutex> lk(b.mu);

@@ -8,10 +8,13 @@
 //   data      k_nsdf_data: 50% points uniform in the view box, 50% near the
 //             surface (exact-traced camera hits + N(0, 0.02) offsets),
 //             labelled by the exact field's first-order distance d / |grad d|
-//   training  hand-written SIMT FP32 kernels with BF16-rounded weights and
-//             activations (the inference precision): k_fwd_first, k_fwd,
-//             k_fwd_head (L1 loss), k_bwd, k_reduce, k_adam; one step is
-//             captured once in a CUDA graph and replayed
+//   training  tcgen05 as well: k_tc_train_fwd (features, 4 MMA layers with
+//             FP32 bias + softplus epilogues, head, L1 loss) and
+//             k_tc_train_bwd per layer (dA_prev = dZ W and dW^T = A^T dZ, the
+//             weight gradient accumulated in tensor memory over the CTA's
+//             tiles), BF16 operands and FP32 accumulation; then k_reduce and
+//             hand-written Adam; one step is captured once in a CUDA graph
+//             and replayed
 //   inference tcgen05 (sm_100a): 128-point tiles, BF16 operands in shared
 //             memory (K-major canonical layout, no swizzle), FP32
 //             accumulators in tensor memory, one elected thread issues the
@@ -108,257 +111,25 @@ __global__ void __launch_bounds__(256) k_nsdf_data(PermTable perm, FieldDev f, C
 }
 
 // ------------------------------------------------------------- training
-// Activations are stored row-major [B][64] (A = BF16-rounded softplus(Z));
-// the features X0 [B][128].  GEMM tiles: 64 rows x 64 outputs per block of
-// 256 threads, 4x4 outputs per thread, operands staged in shared memory.
-constexpr int kRowsFwd = 64;
-constexpr int kRowsBwd = 512;  // rows per backward block (partial weight grads)
-constexpr size_t kFwdFirstSmem = (size_t)(kHidden + kRowsFwd) * (kIn + 1) * 4;
-template <int K>
-constexpr size_t bwd_smem() {
-  return (size_t)(kRowsFwd * (kHidden + 1) + kRowsFwd * (K + 1) + kHidden * (K + 1)) * 4;
-}
+// One step on a batch of B rows (a multiple of 512): k_pack_train packs the
+// BF16 weights, k_tc_train_fwd runs the four hidden layers and the head on
+// the tensor cores (128-row tiles) and stores what the backward pass needs,
+// then k_tc_train_bwd runs once per hidden layer (4 -> 1): dZ = dA softplus'(Z),
+// dA_prev = dZ W and the weight gradient dW^T = A_prev^T dZ, accumulated in
+// tensor memory over the CTA's tiles; k_reduce sums the CTAs' partial
+// gradients and k_adam updates the parameters.
+constexpr int kRowsBwd = 512;   // batch granularity of the training API
+constexpr int kTrRows = 128;    // rows per tensor-core tile (one thread each)
 
 struct TrainBufs {
-  float* x0;      // [B][128]
-  float* z[4];    // [B][64] pre-activations
-  float* a[4];    // [B][64] activations (BF16-rounded)
-  float* da;      // [B][64] gradient w.r.t. the current layer's output
-  float* da2;     // [B][64]
-  float* label;   // [B]
-  float* part;    // [nbwd][kNumParams] partial gradients (layers 1-4)
-  float* part_head;  // [nfwd][kHidden + 1] partial gradients of w5, b5
-  float* part_loss;  // [nfwd]
+  __nv_bfloat16* x0;  // [B][128] BF16 features (the first layer's input)
+  float* z[4];        // [B][64] pre-activations
+  __nv_bfloat16* a[3];  // [B][64] BF16 activations of layers 1-3 (inputs of 2-4)
+  float* da;          // [B][64] gradient w.r.t. the current layer's output
+  float* da2;         // [B][64]
+  float* part;        // [grid][kNumParams] partial gradients of W1..W4, b1..b4
+  float* part_head;   // [B / 128][kHidden + 2] partial gradients of w5, b5 and the loss
 };
-
-// features of point `p` for row r of a block: thread part 0 -> chain 0, part
-// 1 -> chain 1, part 2 -> q and zero padding
-__device__ __forceinline__ void features_part(const InputMap& m, float px, float py, float pz,
-                                              int part, float* row /* 128 */) {
-  float q[3];
-  normalise(m, px, py, pz, q);
-  if (part < 2) {
-    float v[48];
-    chain_features(m, q, part, v);
-#pragma unroll
-    for (int i = 0; i < 48; ++i) row[part * 48 + i] = bf16_round(v[i]);
-  } else if (part == 2) {
-    row[96] = bf16_round(q[0]);
-    row[97] = bf16_round(q[1]);
-    row[98] = bf16_round(q[2]);
-#pragma unroll
-    for (int i = 99; i < 128; ++i) row[i] = 0.f;
-  }
-}
-
-// Layer 1: sample (or take) the batch, compute features, Z1 = X0 W1^T + b1.
-__global__ void __launch_bounds__(256) k_fwd_first(InputMap m, const float4* __restrict__ data,
-                                                   uint32_t npts, const uint32_t* __restrict__ step_ctr,
-                                                   uint32_t seed, int direct,
-                                                   const float* __restrict__ params, TrainBufs tb) {
-  extern __shared__ float fsm[];
-  float(*Ws)[kIn + 1] = reinterpret_cast<float(*)[kIn + 1]>(fsm);
-  float(*Xs)[kIn + 1] = reinterpret_cast<float(*)[kIn + 1]>(fsm + kHidden * (kIn + 1));
-  int t = threadIdx.x;
-  for (int i = t; i < kHidden * kIn; i += 256) Ws[i / kIn][i % kIn] = bf16_round(params[OFF_W1 + i]);
-  uint32_t row0 = blockIdx.x * kRowsFwd;
-  {
-    int r = t >> 2, part = t & 3;
-    uint32_t b = row0 + r;
-    uint32_t idx = direct ? b : mix32(seed, *step_ctr, b) % npts;
-    float4 pt = __ldg(&data[idx]);
-    features_part(m, pt.x, pt.y, pt.z, part, &Xs[r][0]);
-    if (part == 3) tb.label[b] = pt.w;
-  }
-  __syncthreads();
-  for (int i = t; i < kRowsFwd * kIn; i += 256) tb.x0[(size_t)row0 * kIn + i] = Xs[i / kIn][i % kIn];
-  int ty = t >> 4, tx = t & 15;
-  float acc[4][4] = {};
-  for (int k = 0; k < kIn; ++k) {
-    float a[4], w[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = Xs[ty * 4 + i][k];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) w[j] = Ws[tx * 4 + j][k];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], w[j], acc[i][j]);
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int c = tx * 4 + j;
-      float z = acc[i][j] + params[OFF_B1 + c];
-      size_t o = (size_t)(row0 + ty * 4 + i) * kHidden + c;
-      tb.z[0][o] = z;
-      tb.a[0][o] = bf16_round(softplus_approx(z));
-    }
-}
-
-// Layers 2-4: Z = A W^T + b.
-__global__ void __launch_bounds__(256) k_fwd(int layer, const float* __restrict__ params,
-                                             TrainBufs tb) {
-  __shared__ float Ws[kHidden][kHidden + 1];
-  __shared__ float As[kRowsFwd][kHidden + 1];
-  int t = threadIdx.x;
-  const float* W = params + w_off(layer);
-  const float* bias = params + b_off(layer);
-  for (int i = t; i < kHidden * kHidden; i += 256) Ws[i / kHidden][i % kHidden] = bf16_round(W[i]);
-  uint32_t row0 = blockIdx.x * kRowsFwd;
-  const float* A = tb.a[layer - 1];
-  for (int i = t; i < kRowsFwd * kHidden; i += 256)
-    As[i / kHidden][i % kHidden] = A[(size_t)row0 * kHidden + i];
-  __syncthreads();
-  int ty = t >> 4, tx = t & 15;
-  float acc[4][4] = {};
-  for (int k = 0; k < kHidden; ++k) {
-    float a[4], w[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][k];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) w[j] = Ws[tx * 4 + j][k];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], w[j], acc[i][j]);
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int c = tx * 4 + j;
-      float z = acc[i][j] + bias[c];
-      size_t o = (size_t)(row0 + ty * 4 + i) * kHidden + c;
-      tb.z[layer][o] = z;
-      tb.a[layer][o] = bf16_round(softplus_approx(z));
-    }
-}
-
-// Head: out = A4 w5 + b5, L1 loss, dOut = sign(out - label) / B, dA4 =
-// dOut * w5, partial gradients of w5 and b5 and the loss per block.
-__global__ void __launch_bounds__(256) k_fwd_head(const float* __restrict__ params, uint32_t batch,
-                                                  TrainBufs tb, float* __restrict__ out_pred) {
-  __shared__ float red[kRowsFwd][kHidden + 1];
-  __shared__ float g_s[kRowsFwd];
-  __shared__ float loss_s[kRowsFwd];
-  int t = threadIdx.x;
-  uint32_t row0 = blockIdx.x * kRowsFwd;
-  int r = t >> 2, part = t & 3;  // 4 threads per row, 16 columns each
-  size_t base = (size_t)(row0 + r) * kHidden;
-  float s = 0.f;
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    int c = part * 16 + j;
-    s = __fmaf_rn(tb.a[3][base + c], bf16_round(params[OFF_W5 + c]), s);
-  }
-  s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
-  s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
-  float pred = s + params[OFF_B5];
-  float diff = pred - tb.label[row0 + r];
-  float g = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) / (float)batch;
-  if (part == 0) {
-    g_s[r] = g;
-    loss_s[r] = fabsf(diff);
-    if (out_pred) out_pred[row0 + r] = pred;
-  }
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    int c = part * 16 + j;
-    tb.da[base + c] = g * bf16_round(params[OFF_W5 + c]);
-    red[r][c] = g * tb.a[3][base + c];
-  }
-  __syncthreads();
-  float* ph = tb.part_head + (size_t)blockIdx.x * (kHidden + 2);
-  if (t < kHidden) {
-    float acc = 0.f;
-    for (int i = 0; i < kRowsFwd; ++i) acc += red[i][t];
-    ph[t] = acc;
-  } else if (t == kHidden) {
-    float acc = 0.f;
-    for (int i = 0; i < kRowsFwd; ++i) acc += g_s[i];
-    ph[kHidden] = acc;
-  } else if (t == kHidden + 1) {
-    float acc = 0.f;
-    for (int i = 0; i < kRowsFwd; ++i) acc += loss_s[i];
-    ph[kHidden + 1] = acc;
-  }
-}
-
-// Backward through hidden layer `layer` (0-based): dZ = dA * softplus'(Z),
-// partial dW = dZ^T A_prev and db = sum dZ over this block's 512 rows, and
-// dA_prev = dZ W (layers > 0).
-template <int K>
-__global__ void __launch_bounds__(256) k_bwd(int layer, const float* __restrict__ params,
-                                             TrainBufs tb, const float* __restrict__ da_in,
-                                             float* __restrict__ da_out) {
-  extern __shared__ float bsm[];
-  float(*dZs)[kHidden + 1] = reinterpret_cast<float(*)[kHidden + 1]>(bsm);
-  float(*As)[K + 1] = reinterpret_cast<float(*)[K + 1]>(bsm + kRowsFwd * (kHidden + 1));
-  float(*Ws)[K + 1] =
-      reinterpret_cast<float(*)[K + 1]>(bsm + kRowsFwd * (kHidden + 1) + kRowsFwd * (K + 1));
-  int t = threadIdx.x;
-  const float* W = params + w_off(layer);
-  if (layer > 0)
-    for (int i = t; i < kHidden * K; i += 256) Ws[i / K][i % K] = bf16_round(W[i]);
-  const float* Z = tb.z[layer];
-  const float* Aprev = layer > 0 ? tb.a[layer - 1] : tb.x0;
-  int ty = t >> 4, tx = t & 15;
-  constexpr int KC = K / 16;  // weight-gradient columns per thread
-  float gw[4][KC] = {};
-  float gb = 0.f;
-  for (int chunk = 0; chunk < kRowsBwd / kRowsFwd; ++chunk) {
-    uint32_t row0 = blockIdx.x * kRowsBwd + chunk * kRowsFwd;
-    __syncthreads();
-    for (int i = t; i < kRowsFwd * kHidden; i += 256) {
-      size_t o = (size_t)row0 * kHidden + i;
-      dZs[i / kHidden][i % kHidden] = da_in[o] * softplus_approx_deriv(Z[o]);
-    }
-    for (int i = t; i < kRowsFwd * K; i += 256) As[i / K][i % K] = Aprev[(size_t)row0 * K + i];
-    __syncthreads();
-    // weight gradient: rows n = ty*4+i, columns k = tx*KC + j
-    for (int r = 0; r < kRowsFwd; ++r) {
-      float dz[4], a[KC];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) dz[i] = dZs[r][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < KC; ++j) a[j] = As[r][tx * KC + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < KC; ++j) gw[i][j] = __fmaf_rn(dz[i], a[j], gw[i][j]);
-    }
-    if (t < kHidden)
-      for (int r = 0; r < kRowsFwd; ++r) gb += dZs[r][t];
-    if (layer > 0) {
-      // dA_prev = dZ W : rows ty*4+i, columns tx*4+j (K = 64)
-      float acc[4][4] = {};
-      for (int n = 0; n < kHidden; ++n) {
-        float dz[4], w[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) dz[i] = dZs[ty * 4 + i][n];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) w[j] = Ws[n][tx * 4 + j];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(dz[i], w[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          da_out[(size_t)(row0 + ty * 4 + i) * K + tx * 4 + j] = acc[i][j];
-    }
-  }
-  float* pp = tb.part + (size_t)blockIdx.x * kNumParams;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < KC; ++j) pp[w_off(layer) + (ty * 4 + i) * K + tx * KC + j] = gw[i][j];
-  if (t < kHidden) pp[b_off(layer) + t] = gb;
-}
 
 // grad[p] = sum of the partial gradients; the loss of the step is appended
 // to loss_hist.
@@ -813,6 +584,375 @@ __global__ void __launch_bounds__(128) k_ref_eval(InputMap m, const float* __res
   out[i] = d + params[OFF_B5];
 }
 
+// ------------------------------------------------ tensor-core training
+// Training weight pack: the forward's W1..W4 as in the inference pack but
+// without the first-layer bias columns (the training adds b1 in FP32), then
+// W2^T..W4^T (canonical rows = layer inputs), the B operands of dA_prev = dZ W.
+constexpr uint32_t kTrPackBytes = kPackWBytes + 3 * kPackWh;  // 65536
+
+__global__ void k_pack_train(const float* __restrict__ params, unsigned char* __restrict__ pack) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (uint32_t)(kHidden * kIn)) {
+    uint32_t n = i / kIn, k = i % kIn;
+    *reinterpret_cast<__nv_bfloat16*>(pack + canon_off(n, k, kIn)) =
+        __float2bfloat16_rn(params[OFF_W1 + i]);
+  }
+  if (i < (uint32_t)(3 * kHidden * kHidden)) {
+    uint32_t l = i / (kHidden * kHidden), e = i % (kHidden * kHidden);
+    uint32_t n = e / kHidden, k = e % kHidden;
+    __nv_bfloat16 w = __float2bfloat16_rn(params[w_off(1 + l) + e]);
+    *reinterpret_cast<__nv_bfloat16*>(pack + kPackW1 + l * kPackWh + canon_off(n, k, kHidden)) = w;
+    *reinterpret_cast<__nv_bfloat16*>(pack + kPackWBytes + l * kPackWh +
+                                      canon_off(k, n, kHidden)) = w;
+  }
+}
+
+// Issues `steps` MMAs of K = 16 (M 128, N 64): D (+)= A B^T, A and B K-major
+// canonical with rows of `ka` / `kb` elements.
+__device__ __forceinline__ void mma_chain(uint32_t d_tmem, uint32_t a, uint32_t ka, uint32_t b,
+                                          uint32_t kb, uint32_t steps, bool accumulate) {
+#pragma unroll 1
+  for (uint32_t kk = 0; kk < steps; ++kk)
+    mma_bf16(d_tmem, umma_desc(a + kk * 256u, ka * 16u), umma_desc(b + kk * 256u, kb * 16u),
+             (accumulate || kk > 0) ? 1u : 0u);
+}
+
+struct __align__(1024) TrFwdSmem {
+  unsigned char w[kPackWBytes];          // W1..W4, canonical
+  unsigned char x[kTrRows * kIn * 2];    // layer input (K 128 or 64); FP32 scratch for the head
+  float bias[4][kHidden];
+  float w5[kHidden];
+  float gs[kTrRows], ls[kTrRows];
+  float b5;
+  uint64_t bar;
+  uint32_t tmem;
+};
+constexpr size_t kTrFwdSmemBytes = sizeof(TrFwdSmem) + 1024;
+
+// Forward of one training step: features, four hidden layers (MMA + FP32
+// bias + softplus, Z kept in FP32 and the activations in BF16 for the
+// backward pass), head, L1 loss and its gradient dA4 = sign(out - label) / B
+// * w5; partial gradients of w5, b5 and the loss per tile.
+__global__ void __launch_bounds__(kTrRows) k_tc_train_fwd(InputMap m,
+                                                          const float4* __restrict__ data,
+                                                          uint32_t npts,
+                                                          const uint32_t* __restrict__ step_ctr,
+                                                          uint32_t seed, int direct,
+                                                          const unsigned char* __restrict__ pack,
+                                                          const float* __restrict__ params,
+                                                          TrainBufs tb, uint32_t batch,
+                                                          float* __restrict__ pred_out,
+                                                          int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  TrFwdSmem& s = *reinterpret_cast<TrFwdSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int row = threadIdx.x;
+  for (uint32_t i = row; i < kPackWBytes / 16; i += kTrRows)
+    reinterpret_cast<uint4*>(s.w)[i] = __ldg(reinterpret_cast<const uint4*>(pack) + i);
+  for (uint32_t i = row; i < 4 * kHidden; i += kTrRows)
+    s.bias[i / kHidden][i % kHidden] = params[b_off(i / kHidden) + i % kHidden];
+  if (row < kHidden) s.w5[row] = bf16_round(params[OFF_W5 + row]);
+  if (row == 0) {
+    s.b5 = params[OFF_B5];
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s.bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((row >> 5) == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s.tmem)),
+                 "r"(64));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tcol = s.tmem + ((32u * (uint32_t)(row >> 5)) << 16);
+  const uint32_t step = *step_ctr;
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint32_t tiles = batch / kTrRows;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    uint32_t b = tile * kTrRows + row;
+    uint32_t idx = direct ? b : mix32(seed, step, b) % npts;
+    float4 pt = __ldg(&data[idx]);
+    float q[3];
+    normalise(m, pt.x, pt.y, pt.z, q);
+    {
+      uint4* xg = reinterpret_cast<uint4*>(tb.x0 + (size_t)b * kIn);
+      float v[48];
+#pragma unroll
+      for (int chain = 0; chain < 2; ++chain) {
+        chain_features(m, q, chain, v);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          uint4 u = make_uint4(pack_bf16x2(v[c * 8 + 0], v[c * 8 + 1]),
+                               pack_bf16x2(v[c * 8 + 2], v[c * 8 + 3]),
+                               pack_bf16x2(v[c * 8 + 4], v[c * 8 + 5]),
+                               pack_bf16x2(v[c * 8 + 6], v[c * 8 + 7]));
+          store_chunk(s.x, row, (chain * 6 + c) * 8, kIn, u.x, u.y, u.z, u.w);
+          xg[chain * 6 + c] = u;
+        }
+      }
+      uint4 u = make_uint4(pack_bf16x2(q[0], q[1]), pack_bf16x2(q[2], 0.f), 0u, 0u);
+      store_chunk(s.x, row, 96, kIn, u.x, u.y, u.z, u.w);
+      xg[12] = u;
+#pragma unroll
+      for (int c = 13; c < 16; ++c) {
+        store_chunk(s.x, row, c * 8, kIn, 0u, 0u, 0u, 0u);
+        xg[c] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    float d = 0.f;
+    uint32_t a4[32];
+#pragma unroll 1
+    for (int layer = 0; layer < 4; ++layer) {
+      const uint32_t K = layer == 0 ? kIn : kHidden;
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      fence_after();
+      if (row == 0) {
+        mma_chain(s.tmem, smem_addr(s.x), K,
+                  smem_addr(s.w + (layer == 0 ? 0u : kPackW1 + (layer - 1) * kPackWh)), K, K / 16,
+                  false);
+        mma_commit(&s.bar);
+      }
+      ok = __syncthreads_and(mbar_wait(&s.bar, phase) && ok);  // CTA-uniform
+      phase ^= 1u;
+      fence_after();
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        float acc[32];
+        tmem_ld32(tcol + 32u * (uint32_t)half, acc);
+        float4* zg = reinterpret_cast<float4*>(tb.z[layer] + (size_t)b * kHidden + 32 * half);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += s.bias[layer][32 * half + j];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          zg[j] = make_float4(acc[4 * j], acc[4 * j + 1], acc[4 * j + 2], acc[4 * j + 3]);
+        uint32_t a[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          a[j] = pack_bf16x2(softplus_approx(acc[2 * j]), softplus_approx(acc[2 * j + 1]));
+        if (layer < 3) {
+          uint4* ag = reinterpret_cast<uint4*>(tb.a[layer] + (size_t)b * kHidden + 32 * half);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            store_chunk(s.x, row, 32 * half + 8 * c, kHidden, a[4 * c], a[4 * c + 1],
+                        a[4 * c + 2], a[4 * c + 3]);
+            ag[c] = make_uint4(a[4 * c], a[4 * c + 1], a[4 * c + 2], a[4 * c + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            a4[16 * half + j] = a[j];
+            int c = 32 * half + 2 * j;
+            d = __fmaf_rn(__uint_as_float(a[j] << 16), s.w5[c], d);
+            d = __fmaf_rn(__uint_as_float(a[j] & 0xFFFF0000u), s.w5[c + 1], d);
+          }
+        }
+      }
+      fence_before();
+    }
+    // head and L1 loss
+    float pred = d + s.b5;
+    float diff = pred - pt.w;
+    float g = (diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f)) / (float)batch;
+    if (pred_out) pred_out[b] = pred;
+    float4* dag = reinterpret_cast<float4*>(tb.da + (size_t)b * kHidden);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      dag[j] = make_float4(g * s.w5[4 * j], g * s.w5[4 * j + 1], g * s.w5[4 * j + 2],
+                           g * s.w5[4 * j + 3]);
+    // every MMA of the tile has completed: the input buffer is free for the
+    // head's reduction (row-major FP32 [128][64])
+    __syncthreads();
+    float* red = reinterpret_cast<float*>(s.x);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      red[row * kHidden + 2 * j] = g * __uint_as_float(a4[j] << 16);
+      red[row * kHidden + 2 * j + 1] = g * __uint_as_float(a4[j] & 0xFFFF0000u);
+    }
+    s.gs[row] = g;
+    s.ls[row] = fabsf(diff);
+    __syncthreads();
+    float* ph = tb.part_head + (size_t)tile * (kHidden + 2);
+    if (row < kHidden) {
+      float acc = 0.f;
+      for (int r = 0; r < kTrRows; ++r) acc += red[r * kHidden + row];
+      ph[row] = acc;
+    } else if (row == kHidden) {
+      float acc = 0.f;
+      for (int r = 0; r < kTrRows; ++r) acc += s.gs[r];
+      ph[kHidden] = acc;
+    } else if (row == kHidden + 1) {
+      float acc = 0.f;
+      for (int r = 0; r < kTrRows; ++r) acc += s.ls[r];
+      ph[kHidden + 1] = acc;
+    }
+    __syncthreads();  // the reduction has read the scratch before the next tile's features
+  }
+  if (!ok && row == 0) atomicExch(err, 1);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((row >> 5) == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"(64));
+}
+
+struct __align__(1024) TrBwdSmem {
+  unsigned char wt[kPackWh];                // W^T of this layer (rows = inputs), canonical
+  unsigned char dz[kTrRows * kHidden * 2];  // dZ, rows = batch rows, K = 64
+  unsigned char dzt[kHidden * kTrRows * 2]; // dZ^T, rows = outputs, K = 128 batch rows
+  unsigned char at[kIn * kTrRows * 2];      // A_prev^T, rows = inputs (128), K = 128 batch rows
+  uint64_t bar;
+  uint32_t tmem;
+};
+constexpr size_t kTrBwdSmemBytes = sizeof(TrBwdSmem) + 1024;
+
+__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, uint32_t bits16) {
+  *reinterpret_cast<uint16_t*>(base + off) = (uint16_t)bits16;
+}
+
+// Backward through hidden layer `layer` (0-based) over 128-row tiles:
+//   dZ      = dA * softplus'(Z)                      (FP32, then BF16)
+//   dA_prev = dZ W          (layers > 0)            TMEM columns [0, 64)
+//   dW^T   += A_prev^T dZ   over the CTA's tiles     TMEM columns [64, 128)
+// The bias gradient rides in dW^T: the A_prev^T row just past the inputs
+// (row 64; row 99, an always-zero feature, for the first layer) is all ones,
+// so that accumulator row is sum_b dZ.  The CTA's dW, db go to its slot of
+// the partial-gradient buffer.
+__global__ void __launch_bounds__(kTrRows) k_tc_train_bwd(int layer,
+                                                          const unsigned char* __restrict__ pack,
+                                                          TrainBufs tb,
+                                                          const float* __restrict__ da_in,
+                                                          float* __restrict__ da_out,
+                                                          uint32_t batch, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  TrBwdSmem& s = *reinterpret_cast<TrBwdSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int row = threadIdx.x;
+  const uint32_t Kin = layer == 0 ? kIn : kHidden;
+  const uint32_t ones_row = layer == 0 ? 99u : (uint32_t)kHidden;
+  const uint32_t one = 0x3F80u;  // BF16 1.0
+  if (layer > 0)
+    for (uint32_t i = row; i < kPackWh / 16; i += kTrRows)
+      reinterpret_cast<uint4*>(s.wt)[i] = __ldg(
+          reinterpret_cast<const uint4*>(pack + kPackWBytes + (layer - 1) * kPackWh) + i);
+  // rows of A_prev^T past the inputs: the ones row, then zeros (hidden layers)
+  if (layer > 0)
+    for (uint32_t k = kHidden; k < (uint32_t)kIn; ++k)
+      st_bf16(s.at, canon_off(k, row, kTrRows), k == ones_row ? one : 0u);
+  if (row == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s.bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((row >> 5) == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s.tmem)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t lane_off = (32u * (uint32_t)(row >> 5)) << 16;
+  uint32_t phase = 0;
+  bool ok = true, first = true;
+  const uint32_t tiles = batch / kTrRows;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    size_t b = (size_t)tile * kTrRows + row;
+    const float4* dg = reinterpret_cast<const float4*>(da_in + b * kHidden);
+    const float4* zg = reinterpret_cast<const float4*>(tb.z[layer] + b * kHidden);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {  // 8 dZ values per 16-byte chunk
+      float dz[8];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float4 dd = dg[2 * c + h], zz = zg[2 * c + h];
+        dz[4 * h] = dd.x * softplus_approx_deriv(zz.x);
+        dz[4 * h + 1] = dd.y * softplus_approx_deriv(zz.y);
+        dz[4 * h + 2] = dd.z * softplus_approx_deriv(zz.z);
+        dz[4 * h + 3] = dd.w * softplus_approx_deriv(zz.w);
+      }
+      uint32_t p0 = pack_bf16x2(dz[0], dz[1]), p1 = pack_bf16x2(dz[2], dz[3]);
+      uint32_t p2 = pack_bf16x2(dz[4], dz[5]), p3 = pack_bf16x2(dz[6], dz[7]);
+      store_chunk(s.dz, row, 8 * c, kHidden, p0, p1, p2, p3);
+      uint32_t pk[4] = {p0, p1, p2, p3};
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        st_bf16(s.dzt, canon_off(8 * c + e, row, kTrRows), (pk[e >> 1] >> (16 * (e & 1))) & 0xFFFFu);
+    }
+    const uint4* ag = layer == 0 ? reinterpret_cast<const uint4*>(tb.x0 + b * kIn)
+                                 : reinterpret_cast<const uint4*>(tb.a[layer - 1] + b * kHidden);
+    for (uint32_t c = 0; c < Kin / 8; ++c) {
+      uint4 u = ag[c];
+      uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        uint32_t k = 8 * c + e;
+        uint32_t v = (w4[e >> 1] >> (16 * (e & 1))) & 0xFFFFu;
+        st_bf16(s.at, canon_off(k, row, kTrRows), k == ones_row ? one : v);
+      }
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (row == 0) {
+      if (layer > 0)
+        mma_chain(s.tmem, smem_addr(s.dz), kHidden, smem_addr(s.wt), kHidden, kHidden / 16, false);
+      mma_chain(s.tmem + 64u, smem_addr(s.at), kTrRows, smem_addr(s.dzt), kTrRows, kTrRows / 16,
+                !first);
+      mma_commit(&s.bar);
+    }
+    ok = __syncthreads_and(mbar_wait(&s.bar, phase) && ok);  // CTA-uniform
+    phase ^= 1u;
+    fence_after();
+    if (layer > 0) {
+      float4* og = reinterpret_cast<float4*>(da_out + b * kHidden);
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        float acc[32];
+        tmem_ld32(s.tmem + lane_off + 32u * (uint32_t)half, acc);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          og[8 * half + j] = make_float4(acc[4 * j], acc[4 * j + 1], acc[4 * j + 2], acc[4 * j + 3]);
+      }
+    }
+    fence_before();
+    __syncthreads();  // the next tile overwrites the operands and dA_prev
+    fence_after();
+    first = false;
+  }
+  // this CTA's weight and bias gradients: TMEM lane = input index k', column = output n
+  float* pp = tb.part + (size_t)blockIdx.x * kNumParams;
+  const uint32_t k = (uint32_t)row;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    float acc[32];
+    if (!first) {
+      tmem_ld32(s.tmem + lane_off + 64u + 32u * (uint32_t)half, acc);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      uint32_t n = 32u * (uint32_t)half + (uint32_t)j;
+      if (k == ones_row)
+        pp[b_off(layer) + n] = acc[j];
+      if (k < Kin) pp[w_off(layer) + n * Kin + k] = k == ones_row ? 0.f : acc[j];
+    }
+  }
+  if (!ok && row == 0) atomicExch(err, 1);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((row >> 5) == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"(128));
+}
+
 // ------------------------------------------------------------- tracing
 struct MarchDev {
   float alpha;        // network step = alpha * network distance (safety / Lipschitz bound)
@@ -1196,6 +1336,8 @@ struct re_nsdf {
   re::nsdf::TrainBufs tb{};
   float* loss_hist = nullptr;
   uint32_t loss_cap = 0;
+  unsigned char* train_pack = nullptr;  // BF16 weights of the training kernels
+  int fwd_grid = 0, bwd_grid = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   float graph_lr = -1.f;
@@ -1222,39 +1364,51 @@ void free_train(re_nsdf* s) {
   s->graph_exec = nullptr;
   s->graph = nullptr;
   cudaFree(s->tb.x0);
-  for (int l = 0; l < 4; ++l) {
-    cudaFree(s->tb.z[l]);
-    cudaFree(s->tb.a[l]);
-  }
+  for (int l = 0; l < 4; ++l) cudaFree(s->tb.z[l]);
+  for (int l = 0; l < 3; ++l) cudaFree(s->tb.a[l]);
   cudaFree(s->tb.da);
   cudaFree(s->tb.da2);
-  cudaFree(s->tb.label);
   cudaFree(s->tb.part);
   cudaFree(s->tb.part_head);
+  cudaFree(s->train_pack);
+  s->train_pack = nullptr;
   s->tb = TrainBufs{};
   s->batch = 0;
+}
+
+// Persistent grids of the training kernels: occupancy-limited, and never
+// more CTAs per SM than tensor memory holds (512 columns: 64 per forward
+// CTA, 128 per backward CTA), so that no tcgen05.alloc has to wait.
+template <typename K>
+int train_grid(K kernel, size_t smem, int tmem_cols, uint32_t tiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTrRows, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  per_sm = std::min(per_sm, 512 / tmem_cols);
+  return (int)std::min<uint32_t>(tiles, (uint32_t)(per_sm * sm_count()));
 }
 
 re_status alloc_train(re_nsdf* s, uint32_t batch) {
   if (s->batch == batch) return RE_OK;
   free_train(s);
-  RE_CUDA(cudaFuncSetAttribute(k_fwd_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kFwdFirstSmem));
-  RE_CUDA(cudaFuncSetAttribute(k_bwd<kHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bwd_smem<kHidden>()));
-  RE_CUDA(cudaFuncSetAttribute(k_bwd<kIn>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bwd_smem<kIn>()));
+  RE_CUDA(cudaFuncSetAttribute(k_tc_train_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTrFwdSmemBytes));
+  RE_CUDA(cudaFuncSetAttribute(k_tc_train_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTrBwdSmemBytes));
   size_t B = batch;
-  RE_CUDA(cudaMalloc(&s->tb.x0, B * kIn * 4));
-  for (int l = 0; l < 4; ++l) {
-    RE_CUDA(cudaMalloc(&s->tb.z[l], B * kHidden * 4));
-    RE_CUDA(cudaMalloc(&s->tb.a[l], B * kHidden * 4));
-  }
+  uint32_t tiles = batch / kTrRows;
+  s->fwd_grid = train_grid(k_tc_train_fwd, kTrFwdSmemBytes, 64, tiles);
+  s->bwd_grid = train_grid(k_tc_train_bwd, kTrBwdSmemBytes, 128, tiles);
+  RE_CUDA(cudaMalloc(&s->tb.x0, B * kIn * 2));
+  for (int l = 0; l < 4; ++l) RE_CUDA(cudaMalloc(&s->tb.z[l], B * kHidden * 4));
+  for (int l = 0; l < 3; ++l) RE_CUDA(cudaMalloc(&s->tb.a[l], B * kHidden * 2));
   RE_CUDA(cudaMalloc(&s->tb.da, B * kHidden * 4));
   RE_CUDA(cudaMalloc(&s->tb.da2, B * kHidden * 4));
-  RE_CUDA(cudaMalloc(&s->tb.label, B * 4));
-  RE_CUDA(cudaMalloc(&s->tb.part, (B / kRowsBwd) * kNumParams * 4));
-  RE_CUDA(cudaMalloc(&s->tb.part_head, (B / kRowsFwd) * (kHidden + 2) * 4));
+  RE_CUDA(cudaMalloc(&s->tb.part, (size_t)s->bwd_grid * kNumParams * 4));
+  RE_CUDA(cudaMalloc(&s->tb.part_head, (size_t)tiles * (kHidden + 2) * 4));
+  RE_CUDA(cudaMalloc(&s->train_pack, kTrPackBytes));
   s->batch = batch;
   return RE_OK;
 }
@@ -1270,23 +1424,24 @@ re_status check(const re_nsdf* s, const char* fn) {
 }
 
 // One optimisation step on a batch (sampled from s->data, or given points
-// when direct): forward, L1 loss, backward, reduction, optional Adam.
+// when direct): pack, forward + L1 loss, backward, reduction, optional Adam.
 re_status enqueue_step(re_nsdf* s, const float4* data, uint32_t npts, int direct, float lr,
                        bool adam, float* pred, cudaStream_t st) {
   uint32_t B = s->batch;
-  uint32_t nfwd = B / kRowsFwd, nbwd = B / kRowsBwd;
-  k_fwd_first<<<nfwd, 256, kFwdFirstSmem, st>>>(s->map, data, npts, s->step_ctr, s->seed, direct,
-                                                s->params, s->tb);
-  for (int l = 1; l < 4; ++l) k_fwd<<<nfwd, 256, 0, st>>>(l, s->params, s->tb);
-  k_fwd_head<<<nfwd, 256, 0, st>>>(s->params, B, s->tb, pred);
+  uint32_t nfwd = B / kTrRows, nbwd = (uint32_t)s->bwd_grid;
+  k_pack_train<<<(3 * kHidden * kHidden + 255) / 256, 256, 0, st>>>(s->params, s->train_pack);
+  k_tc_train_fwd<<<s->fwd_grid, kTrRows, kTrFwdSmemBytes, st>>>(
+      s->map, data, npts, s->step_ctr, s->seed, direct, s->train_pack, s->params, s->tb, B, pred,
+      s->err);
   // backward: da holds dA4; alternate da / da2
   float* din = s->tb.da;
   float* dout = s->tb.da2;
-  for (int l = 3; l >= 1; --l) {
-    k_bwd<kHidden><<<nbwd, 256, bwd_smem<kHidden>(), st>>>(l, s->params, s->tb, din, dout);
+  for (int l = 3; l >= 0; --l) {
+    k_tc_train_bwd<<<s->bwd_grid, kTrRows, kTrBwdSmemBytes, st>>>(l, s->train_pack, s->tb, din,
+                                                                  l > 0 ? dout : nullptr, B,
+                                                                  s->err);
     std::swap(din, dout);
   }
-  k_bwd<kIn><<<nbwd, 256, bwd_smem<kIn>(), st>>>(0, s->params, s->tb, din, nullptr);
   k_reduce<<<(kNumParams + 2 + 255) / 256, 256, 0, st>>>(s->tb, nbwd, nfwd, s->grad,
                                                          adam ? s->loss_hist : nullptr,
                                                          s->step_ctr, B);
@@ -1585,14 +1740,18 @@ RE_API re_status re_nsdf_train(re_nsdf* s, uint32_t steps, uint32_t batch, float
     if (e != cudaSuccess) return re::cuda_fail(e, "re_nsdf_train: graph capture");
     s->graph_lr = lr;
   }
+  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
   for (uint32_t i = 0; i < steps; ++i) RE_CUDA(cudaGraphLaunch(s->graph_exec, cs));
   s->pack_valid = false;
   s->lipschitz = 0.f;
   if (loss_out)
     RE_CUDA(cudaMemcpyAsync(loss_out, s->loss_hist + done, (size_t)steps * 4,
                             cudaMemcpyDeviceToHost, cs));
+  int herr = 0;
+  RE_CUDA(cudaMemcpyAsync(&herr, s->err, 4, cudaMemcpyDeviceToHost, cs));
   RE_CUDA(cudaStreamSynchronize(cs));
   s->total_steps_done = done + steps;
+  if (herr) return re::fail(RE_ERR_INTERNAL, "re_nsdf_train: tensor-core wait bound reached");
   return RE_OK;
 }
 
@@ -1607,9 +1766,14 @@ RE_API re_status re_nsdf_loss_grad(re_nsdf* s, const float* d_xyzl, uint32_t n, 
   cudaStream_t cs = (cudaStream_t)stream;
   st = re::alloc_train(s, n);
   if (st != RE_OK) return st;
+  RE_CUDA(cudaMemsetAsync(s->err, 0, 4, cs));
   st = re::enqueue_step(s, reinterpret_cast<const float4*>(d_xyzl), n, 1, 0.f, false, d_pred, cs);
   if (st != RE_OK) return st;
   RE_CUDA(cudaMemcpyAsync(d_grad, s->grad, re::nsdf::kNumParams * 4, cudaMemcpyDeviceToDevice, cs));
+  int herr = 0;
+  RE_CUDA(cudaMemcpyAsync(&herr, s->err, 4, cudaMemcpyDeviceToHost, cs));
+  RE_CUDA(cudaStreamSynchronize(cs));
+  if (herr) return re::fail(RE_ERR_INTERNAL, "re_nsdf_loss_grad: tensor-core wait bound reached");
   return RE_OK;
 }
 

@@ -433,11 +433,11 @@ RE_API void re_sdf_shade_params_default(re_sdf_shade_params* s) {
   s->shadow_tmax = 40.0f;
   s->shadow_max_steps = 128;
   // the sun of Craze's first frame after start (renderer.cu:287-298) is
-  // straight up; a lower sun gives a visible sky gradient
-  float ang = 0.3f * 3.14159265f * 0.6f;
+  // straight up; a lower sun gives a visible sky gradient: (0, cos a, sin a)
+  // at Craze's angle 0.3 (a = 0.18 pi), rounded to float
   s->sun_dir[0] = 0.0f;
-  s->sun_dir[1] = std::cos(ang);
-  s->sun_dir[2] = std::sin(ang);
+  s->sun_dir[1] = 0.844327926f;
+  s->sun_dir[2] = 0.535826795f;
   s->max_y = 2.0f;  // the terrain's lowest ~30 % of hits are ocean
   s->fog_density = 0.02f;
   s->vignetting_k = 0.25f;

@@ -91,3 +91,13 @@ def test_plain_c_caller(tmp_path):
                    check=True)
     out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr
+
+
+def test_frame_config_matches_library_defaults():
+    """SdfFrameConfig builds re_sdf_shade_params in Python (the benchmark's
+    reference arm must not load the library); it equals the library's own
+    defaults field for field."""
+    a = rb.configs.SdfFrameConfig().shade()
+    b = _lib.re_sdf_shade_params()
+    _lib.lib.re_sdf_shade_params_default(ctypes.byref(b))
+    assert bytes(a) == bytes(b)

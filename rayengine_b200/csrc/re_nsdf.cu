@@ -1393,10 +1393,16 @@ int train_grid(K kernel, size_t smem, int tmem_cols, uint32_t tiles) {
 re_status alloc_train(re_nsdf* s, uint32_t batch) {
   if (s->batch == batch) return RE_OK;
   free_train(s);
+  // the whole shared-memory carveout, so that 2-3 of these 75 KB CTAs fit on
+  // an SM (measured: the default carveout held one, 4 warps per SM)
   RE_CUDA(cudaFuncSetAttribute(k_tc_train_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kTrFwdSmemBytes));
+  RE_CUDA(cudaFuncSetAttribute(k_tc_train_fwd, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               100));
   RE_CUDA(cudaFuncSetAttribute(k_tc_train_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kTrBwdSmemBytes));
+  RE_CUDA(cudaFuncSetAttribute(k_tc_train_bwd, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               100));
   size_t B = batch;
   uint32_t tiles = batch / kTrRows;
   s->fwd_grid = train_grid(k_tc_train_fwd, kTrFwdSmemBytes, 64, tiles);

@@ -110,30 +110,46 @@ __device__ __forceinline__ V3 paint(const PT& P, const ShadeDev& S, V3 p, V3 n) 
   return col;
 }
 
-// Soft shadow toward the light and the light terms of sphere_trace_shadow.
-template <class PT>
-__device__ __forceinline__ V3 lighting(const PT& P, const ShadeDev& S, V3 p, V3 n,
-                                       uint32_t& evals) {
+// The light of sphere_trace_shadow, in three parts so that the shading
+// kernel can advance the soft-shadow march one field evaluation per trip:
+// light_setup (illuminate: direction of the light from the hit), one march
+// step of single_shadow_ray_sphere_trace per call of shadow_step, and
+// light_terms (ambient, soft-shadowed diffuse and back light).
+__device__ __forceinline__ void light_setup(const ShadeDev& S, V3 p, V3& L, float& ldx,
+                                            float& ldz) {
   V3 ld = {(p.x - S.lightpos.x) / S.light_dist, (p.y - S.lightpos.y) / S.light_dist,
            (p.z - S.lightpos.z) / S.light_dist};
-  V3 L = normalize(v3(-ld.x, -ld.y, -ld.z));
-  float prel = 1.0f;
-  float t = S.shadow_tmin;
-  for (uint32_t i = 0; i < S.shadow_max_steps && t < S.shadow_tmax; ++i) {
-    V3 q = {__fmaf_rn(t, L.x, p.x), __fmaf_rn(t, L.y, p.y), __fmaf_rn(t, L.z, p.z)};
-    float dd = terrain_density(P, q, S.octaves, S.scale, S.amp);
-    ++evals;
-    if (prel < kEps || dd <= 1e-5f) {
-      prel = 0.0f;
-      break;
-    }
-    prel = fminf(prel, (S.soft_k * dd) / t);
-    t = __fmaf_rn(S.step_factor, dd, t);
+  L = normalize(v3(-ld.x, -ld.y, -ld.z));
+  ldx = ld.x;
+  ldz = ld.z;
+}
+
+// One step: returns false when the march is over (step bound, range, or the
+// ray is occluded: prel = 0).  The march starts with t = shadow_tmin,
+// prel = 1, i = 0.
+template <class PT>
+__device__ __forceinline__ bool shadow_step(const PT& P, const ShadeDev& S, V3 p, V3 L, float& t,
+                                            float& prel, uint32_t& i, uint32_t& evals) {
+  if (!(i < S.shadow_max_steps && t < S.shadow_tmax)) return false;
+  V3 q = {__fmaf_rn(t, L.x, p.x), __fmaf_rn(t, L.y, p.y), __fmaf_rn(t, L.z, p.z)};
+  float dd = terrain_density(P, q, S.octaves, S.scale, S.amp);
+  ++evals;
+  ++i;
+  if (prel < kEps || dd <= 1e-5f) {
+    prel = 0.0f;
+    return false;
   }
+  prel = fminf(prel, (S.soft_k * dd) / t);
+  t = __fmaf_rn(S.step_factor, dd, t);
+  return true;
+}
+
+__device__ __forceinline__ V3 light_terms(const ShadeDev& S, float prel, V3 n, V3 L, float ldx,
+                                          float ldz) {
   float amb = sat((float)(0.5 + 0.5 * (double)n.y));
   float soft = sat(prel);
   float dif = fmaxf(0.0f, dot(n, L));
-  V3 bv = normalize(v3(-ld.x, 0.0f, ld.z));
+  V3 bv = normalize(v3(-ldx, 0.0f, ldz));
   float bac = sat((float)(0.2 + 0.8 * (double)dot(bv, n)));
   V3 pc = {(soft * S.light_int.x) * dif, (soft * S.light_int.y) * dif,
            (soft * S.light_int.z) * dif};
@@ -241,25 +257,11 @@ __device__ __forceinline__ uint32_t rgba8(V3 c) {
          (uint32_t)(r * 255.0f);
 }
 
-// One pixel: hit record -> packed RGBA8.  Returns the shadow-march field
-// evaluations through `evals`.
-template <class PT>
-__device__ __forceinline__ uint32_t shade_pixel(const PT& P, const ShadeDev& S, V3 o, V3 d,
-                                                const float4 r0, const float4 r1, float u,
-                                                float v, uint32_t& evals) {
-  V3 col;
-  float dist = kInf;
-  if (__float_as_uint(r1.w) == 1u) {
-    V3 p = {r0.x, r0.y, r0.z}, n = {r0.w, r1.x, r1.y};
-    dist = vlen(sub(p, o));
-    col = paint(P, S, p, n);
-    if (S.flags & RE_SDF_SHADE) {
-      V3 pc = lighting(P, S, p, n, evals);
-      col = v3(col.x * pc.x, col.y * pc.y, col.z * pc.z);
-    }
-  } else {
-    col = sky(S, d);
-  }
+// Fog, gamma and vignetting of render_sphere_trace (renderer.cu:273-283)
+// on a shaded colour, then the RGBA8 pack.  dist: the hit's distance
+// (K_INFINITY for a miss).
+__device__ __forceinline__ uint32_t finish_pixel(const ShadeDev& S, V3 col, V3 o, V3 d, float dist,
+                                                 float u, float v) {
   if (S.flags & RE_SDF_FOG) {  // apply_fog (material_functions.cuh:53-63)
     float dens = S.fog_density;
     float e1 = fm_exp(-o.y * dens);
@@ -277,7 +279,16 @@ __device__ __forceinline__ uint32_t shade_pixel(const PT& P, const ShadeDev& S, 
   return rgba8(col);
 }
 
-// Persistent warps over 8x4 pixel tiles (the tile order of the tracer).
+// Shading as a per-lane state machine over the tracer's pixel order (lane i
+// & 31 of 8x4 tile i >> 5): a lane that takes a pixel paints it; a miss
+// (sky) or an unlit frame finishes at once, a lit hit then advances its soft
+// shadow by one field evaluation per loop trip, so the lanes of a warp stay
+// on the same code while their shadow rays take different numbers of
+// steps; when at least kShadeRefill lanes are idle the warp claims that many
+// new pixels with one atomic.  Same operations, in the same order, as one
+// loop per pixel.
+constexpr uint32_t kShadeRefill = 4;
+
 __global__ void __launch_bounds__(256) k_sdf_shade(PermTable perm, ShadeDev S, CamDev cam,
                                                    uint32_t w, uint32_t h,
                                                    const float4* __restrict__ hits,
@@ -287,23 +298,65 @@ __global__ void __launch_bounds__(256) k_sdf_shade(PermTable perm, ShadeDev S, C
   extern __shared__ uint32_t perm_smem[];
   load_perm(perm, perm_smem);
   Perm P = perm_view(perm_smem);
-  uint32_t lane = threadIdx.x & 31u;
-  uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
-  uint32_t evals = 0;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t tiles_x = (w + 7) / 8;
+  const uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
+  const bool lit = (S.flags & RE_SDF_SHADE) != 0u;
+  bool live = false, exhausted = false;
+  uint32_t x = 0, y = 0, i = 0, evals = 0;
+  V3 p = {0.f, 0.f, 0.f}, n = p, L = p, col = p;
+  float ldx = 0.f, ldz = 0.f, t = 0.f, prel = 0.f;
   for (;;) {
-    uint32_t tile = 0;
-    if (lane == 0) tile = atomicAdd(cursor, 1u);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile >= tiles) break;
-    uint32_t x = (tile % tiles_x) * 8 + (lane & 7u);
-    uint32_t y = (tile / tiles_x) * 4 + (lane >> 3);
-    if (x >= w || y >= h) continue;
-    V3 o, d;
-    generate_ray(cam, w, h, x, y, o, d);
-    size_t pix = (size_t)y * w + x;
-    float4 r0 = __ldg(&hits[2 * pix]), r1 = __ldg(&hits[2 * pix + 1]);
-    float u = (float)x / (float)w, v = (float)y / (float)h;
-    rgba[pix] = shade_pixel(P, S, o, d, r0, r1, u, v, evals);
+    uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
+    uint32_t nidle = __popc(idle);
+    if (!exhausted && (nidle >= kShadeRefill || nidle == 32u)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(cursor, nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= total) exhausted = true;
+      if (!live) {
+        uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
+        uint32_t tile = k >> 5, l = k & 31u;
+        x = (tile % tiles_x) * 8 + (l & 7u);
+        y = (tile / tiles_x) * 4 + (l >> 3);
+        if (k < total && x < w && y < h) {
+          size_t pix = (size_t)y * w + x;
+          float4 r0 = __ldg(&hits[2 * pix]), r1 = __ldg(&hits[2 * pix + 1]);
+          V3 o, d;
+          generate_ray(cam, w, h, x, y, o, d);
+          float u = (float)x / (float)w, v = (float)y / (float)h;
+          if (__float_as_uint(r1.w) == 1u) {
+            p = v3(r0.x, r0.y, r0.z);
+            n = v3(r0.w, r1.x, r1.y);
+            col = paint(P, S, p, n);
+            if (lit) {
+              light_setup(S, p, L, ldx, ldz);
+              t = S.shadow_tmin;
+              prel = 1.0f;
+              i = 0;
+              live = true;
+            } else {
+              rgba[pix] = finish_pixel(S, col, o, d, vlen(sub(p, o)), u, v);
+            }
+          } else {
+            rgba[pix] = finish_pixel(S, sky(S, d), o, d, kInf, u, v);
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, live) == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    if (live && !shadow_step(P, S, p, L, t, prel, i, evals)) {
+      V3 pc = light_terms(S, prel, n, L, ldx, ldz);
+      V3 o, d;
+      generate_ray(cam, w, h, x, y, o, d);
+      rgba[(size_t)y * w + x] =
+          finish_pixel(S, v3(col.x * pc.x, col.y * pc.y, col.z * pc.z), o, d, vlen(sub(p, o)),
+                       (float)x / (float)w, (float)y / (float)h);
+      live = false;
+    }
   }
   if (evals_out) {
     uint32_t s = __reduce_add_sync(0xFFFFFFFFu, evals);

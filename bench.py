@@ -864,10 +864,14 @@ class NeuralTerrainSDF:
         P = po.perm(self.cfg.seed)
         jp, jh = po.sdf_arbiter(P, self.cam, W, H, pix)
         err, disagree, both = po.hit_errors(out, jp, jh, pix)
+        # the whole frame's hit/miss against the exact tracer's frame
+        ex = self.rb.sphere_trace(self.params, self.cam, W, H).cpu().numpy()
+        frame_disagree = int(((out[:, 7] == 1) != (ex[:, 7] == 1)).sum())
         return {"vs_fp64_arbiter": {"pixels": int(pix.size), "hit_miss_disagree": disagree,
                                     "median_hit_error": float(np.median(err)) if both else None,
                                     "p95_hit_error": float(np.quantile(err, 0.95)) if both else None,
-                                    "target": "median <= 1e-3 scene units"}}
+                                    "target": "median <= 1e-3 scene units"},
+                "vs_exact_tracer_frame": {"pixels": W * H, "hit_miss_disagree": frame_disagree}}
 
 
 class BatchWavefront:

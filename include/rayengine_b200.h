@@ -100,7 +100,8 @@ typedef struct re_scene re_scene;
 /* Launch tuning of a scene (see re_autotune_ao, re_autotune_primary). */
 typedef struct re_tuning {
   uint32_t stage_nodes;      /* top nodes staged in shared memory per block (<= 8192) */
-  uint32_t queue_kind_major; /* secondary-ray queue: 0 pixel-major, 1 kind-major    */
+  uint32_t queue_kind_major; /* secondary-ray queue: 0 pixel-major, 1 kind-major,
+                                2 shadow rays first, then each pixel's AO rays    */
   uint32_t refill_min;       /* idle lanes before a warp claims new secondary rays, 1..32 */
   uint32_t ray_refill_min;   /* the same for primary and caller rays (re_trace_primary,
                                 re_count_primary, re_trace_rays), 1..32; 32 (default):

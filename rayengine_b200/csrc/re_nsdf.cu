@@ -1376,9 +1376,11 @@ void free_train(re_nsdf* s) {
   s->batch = 0;
 }
 
-// Persistent grids of the training kernels: occupancy-limited, and never
-// more CTAs per SM than tensor memory holds (512 columns: 64 per forward
-// CTA, 128 per backward CTA), so that no tcgen05.alloc has to wait.
+// Persistent grids of the training kernels: as many CTAs per SM as shared
+// memory holds (the occupancy API answers 1 for these tensor-memory kernels,
+// measured, where the SM fits 2 forward or 3 backward CTAs), and never more
+// than tensor memory holds (512 columns: 64 per forward CTA, 128 per
+// backward CTA), so that no tcgen05.alloc has to wait.
 template <typename K>
 int train_grid(K kernel, size_t smem, int tmem_cols, uint32_t tiles) {
   int per_sm = 0;
@@ -1386,6 +1388,13 @@ int train_grid(K kernel, size_t smem, int tmem_cols, uint32_t tiles) {
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
+  int dev = 0, smem_sm = 0, reserved = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) ==
+          cudaSuccess &&
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) ==
+          cudaSuccess)
+    per_sm = std::max(per_sm, smem_sm / (int)(smem + (size_t)reserved));
   per_sm = std::min(per_sm, 512 / tmem_cols);
   return (int)std::min<uint32_t>(tiles, (uint32_t)(per_sm * sm_count()));
 }

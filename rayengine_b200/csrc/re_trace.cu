@@ -219,16 +219,30 @@ struct AoDev {
   uint32_t seed;
 };
 
-// Secondary-ray queue and its tuning: ray kind k (0 shadow, 1..4 AO) of the
-// r-th hit is record k * kind_stride + r * rank_stride.  Pixel-major
-// (kind_stride 1, rank_stride 5) keeps a pixel's five rays together (better
-// cache reuse); kind-major (kind_stride = capacity, rank_stride 1) gives a
-// warp rays of one kind from neighbouring pixels.  refill_min: idle lanes a
-// warp waits for before claiming new rays (32 = whole warps only).
+// Secondary-ray queue and its tuning.  The r-th hit's shadow ray (kind 0)
+// and AO rays j = 0..3 (kinds 1..4) are stored, by `mode`:
+//   0 pixel-major   5r, 5r + 1 + j          a pixel's five rays together
+//                                          (one start leaf, cache reuse)
+//   1 kind-major    r, (1 + j) cap + r      a warp gets rays of one kind
+//                                          from neighbouring pixels
+//   2 shadow-first  r, cap + 4r + j         the shadow rays (one direction)
+//                                          side by side, then each pixel's
+//                                          four AO rays together
+// and traced in record order.  refill_min: idle lanes a warp waits for
+// before claiming new rays (32 = whole warps only).
 struct AoQueue {
   float4* q;
-  uint32_t kind_stride, rank_stride, refill_min;
+  uint32_t mode, cap, refill_min;
 };
+
+__device__ __forceinline__ size_t shadow_record(const AoQueue& aq, uint32_t r) {
+  return aq.mode == 0u ? 5 * (size_t)r : (size_t)r;
+}
+__device__ __forceinline__ size_t ao_record(const AoQueue& aq, uint32_t r, uint32_t j) {
+  return aq.mode == 0u   ? 5 * (size_t)r + 1 + j
+         : aq.mode == 1u ? (size_t)(1 + j) * aq.cap + r
+                         : (size_t)aq.cap + 4 * (size_t)r + j;
+}
 
 // Warp-sum of per-thread work counters, one 64-bit atomic per warp and field.
 __device__ __forceinline__ void flush_counts(const Counters& c, uint32_t rays,
@@ -306,7 +320,7 @@ __global__ void __launch_bounds__(256, 5) k_ao_primary(KdDev kd, CamDev cam, AoD
     // shadow ray (bit 1) is unbounded, AO rays (bits 2..5) have ao_length
     float start = __uint_as_float(hs.leaf_node);
     float4* queue = aq.q;
-    size_t q0 = (size_t)rank * aq.rank_stride;
+    size_t q0 = shadow_record(aq, rank);
     queue[2 * q0] = make_float4(org.x, org.y, org.z, start);
     queue[2 * q0 + 1] = make_float4(ao.light.x, ao.light.y, ao.light.z,
                                     __uint_as_float(pix * 8u + 1u));
@@ -332,7 +346,7 @@ __global__ void __launch_bounds__(256, 5) k_ao_primary(KdDev kd, CamDev cam, AoD
       V3 dir = {__fmaf_rn(lz, nt.x, __fmaf_rn(ly, n.x, lx * nb.x)),
                 __fmaf_rn(lz, nt.y, __fmaf_rn(ly, n.y, lx * nb.y)),
                 __fmaf_rn(lz, nt.z, __fmaf_rn(ly, n.z, lx * nb.z))};
-      size_t q = q0 + (size_t)(1 + j) * aq.kind_stride;
+      size_t q = ao_record(aq, rank, j);
       queue[2 * q] = make_float4(org.x, org.y, org.z, start);
       queue[2 * q + 1] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(pix * 8u + 2u + j));
     }
@@ -372,13 +386,18 @@ __global__ void __launch_bounds__(256, 5) k_ao_secondary(KdDev kd, AoDev ao, AoQ
       if (!s.live) {
         uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
         if (i < n) {
-          uint32_t kind, e;
-          if (aq.kind_stride == 1u) {
+          // claim index i -> record e in the layout's order; kind 0 = shadow
+          uint32_t kind;
+          size_t e;
+          if (aq.mode == 0u) {
             e = i;
             kind = i % 5u;
-          } else {
+          } else if (aq.mode == 1u) {
             kind = i / nh;
-            e = kind * aq.kind_stride + (i - kind * nh);
+            e = (size_t)kind * aq.cap + (i - kind * nh);
+          } else {
+            kind = i < nh ? 0u : 1u;
+            e = i < nh ? (size_t)i : (size_t)aq.cap + (i - nh);
           }
           float4 R0 = __ldg(&aq.q[2 * (size_t)e]), R1 = __ldg(&aq.q[2 * (size_t)e + 1]);
           tag = __float_as_uint(R1.w);
@@ -482,13 +501,8 @@ re_status upload(re_scene* s) {
 AoQueue ao_queue(const re_scene* s, float4* q, uint32_t capacity) {
   AoQueue aq;
   aq.q = q;
-  if (s->tune.queue_kind_major) {
-    aq.kind_stride = capacity;
-    aq.rank_stride = 1;
-  } else {
-    aq.kind_stride = 1;
-    aq.rank_stride = 5;
-  }
+  aq.mode = s->tune.queue_kind_major;
+  aq.cap = capacity;
   aq.refill_min = s->tune.refill_min;
   return aq;
 }
@@ -955,8 +969,8 @@ RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t) {
   if (t->refill_min < 1 || t->refill_min > 32 || t->ray_refill_min < 1 || t->ray_refill_min > 32)
     return re::fail(RE_ERR_INVALID_ARG,
                     "re_scene_set_tuning: refill_min and ray_refill_min must be in [1, 32]");
-  if (t->queue_kind_major > 1)
-    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0 or 1");
+  if (t->queue_kind_major > 2)
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0, 1 or 2");
   s->tune = *t;
   s->tune.stage_nodes = std::min(std::min(t->stage_nodes, s->host.bfs_nodes), re::kMaxStage);
   s->stage = s->tune.stage_nodes;
@@ -989,7 +1003,7 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
   const uint32_t refills[4] = {4u, 8u, 16u, 32u};
   for (int si = 0; si < 4 && ce == cudaSuccess && rs == RE_OK; ++si) {
     if (si > 0 && stages[si] == stages[si - 1]) continue;
-    for (uint32_t km = 0; km < 2 && rs == RE_OK; ++km) {
+    for (uint32_t km = 0; km < 3 && rs == RE_OK; ++km) {
       for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
         re_tuning t = {stages[si], km, refills[ri], keep.ray_refill_min};
         rs = re_scene_set_tuning(s, &t);

@@ -320,7 +320,8 @@ def test_tunings_give_identical_frames(cuda):
     light = rb.unit(cfg.light_dir)
     with rb.KDScene.from_mesh(verts, faces) as sc:
         ref = None
-        for stage, km, refill in ((0, 0, 32), (64, 1, 4), (4096, 0, 8), (4096, 1, 1), (1, 1, 32)):
+        for stage, km, refill in ((0, 0, 32), (64, 1, 4), (4096, 0, 8), (4096, 1, 1), (1, 1, 32),
+                                  (0, 2, 8), (4096, 2, 1), (64, 2, 32)):
             sc.set_tuning(stage, km, refill)
             got = [x.cpu().numpy() for x in sc.render_ao(cam, cfg.width, cfg.height, light,
                                                          cfg.ao_length, cfg.bias, cfg.ao_seed)]

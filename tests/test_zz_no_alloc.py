@@ -34,10 +34,10 @@ def _frame(entry, sc, cam, w, h, params):
     return primary.cpu().numpy(), mask.cpu().numpy(), int(nsec.item())
 
 
-@pytest.mark.parametrize("kind_major", [0, 1])
+@pytest.mark.parametrize("kind_major", [0, 1, 2])
 def test_noalloc_matches_render_ao_twice(cuda, kind_major):
-    """Both secondary-queue layouts (pixel-major and kind-major, whose kind
-    stride is w*h inside the fixed array)."""
+    """Every secondary-queue layout (pixel-major; kind-major and shadow-first,
+    whose AO records start at w*h inside the fixed array)."""
     cfg = rb.configs.HeightfieldConfig(cells=128, width=320, height=180)
     verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
                                   cfg.amplitude)
@@ -54,7 +54,7 @@ def test_noalloc_matches_render_ao_twice(cuda, kind_major):
             assert got[2] == want[2] and got[2] > 0, seed
 
 
-@pytest.mark.parametrize("kind_major", [0, 1])
+@pytest.mark.parametrize("kind_major", [0, 1, 2])
 def test_noalloc_largest_image(cuda, kind_major):
     """An image of 1024 x 409 = 418,816 pixels, just under the limit, with
     the camera close to the terrain so that almost every pixel hits: the

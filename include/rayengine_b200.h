@@ -106,6 +106,10 @@ typedef struct re_tuning {
   uint32_t ray_refill_min;   /* the same for primary and caller rays (re_trace_primary,
                                 re_count_primary, re_trace_rays), 1..32; 32 (default):
                                 each lane runs its ray to the end, no refill */
+  uint32_t ray_lanes;        /* lanes per primary ray in re_trace_primary: 1 (default; 0
+                                reads as 1), 2, 4 or 8.  Above 1 the lanes of a ray split
+                                each leaf's triangle tests (same hits); it shortens the
+                                longest walks of frames too small to fill the GPU */
 } re_tuning;
 
 typedef struct re_scene_stats {
@@ -245,7 +249,7 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w,
                                 uint32_t h, const re_ao_params* p,
                                 re_tuning* best, float* best_ms, void* stream);
 /* Autotuner of the primary pass: times re_trace_primary(flags) for each
- * combination of staging depth and ray_refill_min the same way and keeps
+ * combination of staging depth, ray_refill_min and ray_lanes the same way and keeps
  * the fastest (other fields unchanged).  Set-up time only. */
 RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w,
                                      uint32_t h, uint32_t flags, re_tuning* best,

@@ -85,6 +85,7 @@ class re_tuning(ctypes.Structure):
         ("queue_kind_major", ctypes.c_uint32),
         ("refill_min", ctypes.c_uint32),
         ("ray_refill_min", ctypes.c_uint32),
+        ("ray_lanes", ctypes.c_uint32),
     ]
 
 

@@ -299,13 +299,17 @@ class KDScene:
         t = _lib.re_tuning()
         call("re_scene_get_tuning", self._h, ctypes.byref(t))
         return {"stage_nodes": t.stage_nodes, "queue_kind_major": t.queue_kind_major,
-                "refill_min": t.refill_min, "ray_refill_min": t.ray_refill_min}
+                "refill_min": t.refill_min, "ray_refill_min": t.ray_refill_min,
+                "ray_lanes": t.ray_lanes}
 
     def set_tuning(self, stage_nodes: int, queue_kind_major: int, refill_min: int,
-                   ray_refill_min: int | None = None) -> None:
+                   ray_refill_min: int | None = None, ray_lanes: int | None = None) -> None:
+        cur = self.tuning()
         if ray_refill_min is None:
-            ray_refill_min = self.tuning()["ray_refill_min"]
-        t = _lib.re_tuning(stage_nodes, queue_kind_major, refill_min, ray_refill_min)
+            ray_refill_min = cur["ray_refill_min"]
+        if ray_lanes is None:
+            ray_lanes = cur["ray_lanes"]
+        t = _lib.re_tuning(stage_nodes, queue_kind_major, refill_min, ray_refill_min, ray_lanes)
         call("re_scene_set_tuning", self._h, ctypes.byref(t))
 
     def autotune_ao(self, cam: RCamera, w: int, h: int, params, stream=None) -> dict:
@@ -318,13 +322,14 @@ class KDScene:
                 "refill_min": t.refill_min, "frame_ms": round(ms.value, 4)}
 
     def autotune_primary(self, cam: RCamera, w: int, h: int, flags: int = 0, stream=None) -> dict:
-        """Pick staging depth and ray refill threshold by timing the primary pass."""
+        """Pick staging depth, ray refill threshold and lanes per ray by timing the
+        primary pass."""
         t = _lib.re_tuning()
         ms = ctypes.c_float()
         call("re_autotune_primary", self._h, ctypes.byref(cam), w, h, flags, ctypes.byref(t),
              ctypes.byref(ms), _stream_ptr(stream))
         return {"stage_nodes": t.stage_nodes, "ray_refill_min": t.ray_refill_min,
-                "frame_ms": round(ms.value, 4)}
+                "ray_lanes": t.ray_lanes, "frame_ms": round(ms.value, 4)}
 
     def render_frame(self, cam: RCamera, w: int, h: int, lights, shade, out=None, stream=None):
         """Shaded RGBA8 frame -> uint32-valued int32 CUDA tensor (h*w,).

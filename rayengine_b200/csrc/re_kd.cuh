@@ -27,6 +27,9 @@ struct KdDev {
   // rays stopped by the leaf-visit cap are counted here (may be null); the
   // reference stops at its cap silently (ray_functions.cuh:284)
   uint32_t* trunc;
+  // triangle slots in `tris`; lanes that share a ray fetch their first
+  // triangle of a leaf before its record only below this bound (0: never)
+  uint32_t num_refs = 0;
 };
 
 // Trav::visits of a walk that stopped at the leaf-visit cap.
@@ -139,9 +142,19 @@ __device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, 
   }
 }
 
-template <int MODE, bool ANYHIT, bool COUNT>
+// G > 1: G consecutive lanes walk the same ray in lockstep (same state,
+// same loads) and split each leaf's triangle tests, lane j taking slots
+// first + j, first + j + G, ...; the group then keeps the smallest (t, id)
+// of its lanes' bests.  The sequential acceptance rule (smaller t, or equal
+// t and smaller id, with id -1 for "no hit yet") is that same lexicographic
+// minimum, and a leaf holds each triangle once, so the merged best, its
+// slot and its leaf equal the one-lane walk's.  Closest hit only.
+template <int MODE, bool ANYHIT, bool COUNT, uint32_t G = 1>
 __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2* snodes,
                                           Counters& c) {
+  static_assert(G == 1 || G == 2 || G == 4 || G == 8, "lanes per ray: 1, 2, 4 or 8");
+  static_assert(G == 1 || (!ANYHIT && !COUNT), "shared rays: closest hit, no counters");
+  const uint32_t sub = G > 1 ? (threadIdx.x & (G - 1u)) : 0u;
   const V3 o = s.o, d = s.d, inv = s.inv;
   const float t_entry = s.t_entry;
   uint32_t node = s.node;
@@ -164,9 +177,12 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   // run faster without the extra live registers)
   constexpr bool kEarlyFirst = !ANYHIT;
   uint32_t first = nd.x & 0x7FFFFFFFu;
-  const float4* T = kd.tris + 3 * (size_t)first;
+  // this lane's first slot; with G > 1 it may lie past the leaf (fetched
+  // only inside the triangle array, and used only if the leaf reaches it)
+  const uint32_t mine = first + sub;
+  const float4* T = kd.tris + 3 * (size_t)mine;
   float4 T0 = make_float4(0.f, 0.f, 0.f, 0.f), T1 = T0, T2 = T0;
-  if (kEarlyFirst && !(nd.x >> 31)) {
+  if (kEarlyFirst && !(nd.x >> 31) && (G == 1 || mine < kd.num_refs)) {
     T0 = __ldg(T);
     T1 = __ldg(T + 1);
     T2 = __ldg(T + 2);
@@ -193,8 +209,8 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
     if (tz < texit) { texit = tz; face = d.z > 0.0f ? 5 : 4; }
   }
   int32_t rope = face >= 0 ? __ldg(reinterpret_cast<const int32_t*>(L + 2) + face) : -1;
-  for (uint32_t i = first, end = first + count; i < end; ++i) {
-    if (!kEarlyFirst || i != first) {
+  for (uint32_t i = mine, end = first + count; i < end; i += G) {
+    if (!kEarlyFirst || i != mine || (G > 1 && mine >= kd.num_refs)) {
       T = kd.tris + 3 * (size_t)i;
       T0 = __ldg(T);
       T1 = __ldg(T + 1);
@@ -218,6 +234,26 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
       }
     }
   }
+  if (G > 1) {
+    const uint32_t gmask = ((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(G - 1u));
+#pragma unroll
+    for (uint32_t off = 1; off < G; off <<= 1) {
+      float ot = __shfl_xor_sync(gmask, s.best_t, off);
+      int32_t oid = __shfl_xor_sync(gmask, s.best_id, off);
+      float ou = __shfl_xor_sync(gmask, s.best_u, off);
+      float ov = __shfl_xor_sync(gmask, s.best_v, off);
+      uint32_t oref = __shfl_xor_sync(gmask, s.best_ref, off);
+      // the other lane differs only if it accepted a triangle of this leaf
+      if (ot < s.best_t || (ot == s.best_t && oid < s.best_id)) {
+        s.best_t = ot;
+        s.best_id = oid;
+        s.best_u = ou;
+        s.best_v = ov;
+        s.best_ref = oref;
+        s.best_leaf = node;
+      }
+    }
+  }
   if (face < 0) {
     s.live = false;
     return;
@@ -236,7 +272,7 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
     c.status = 1;
     s.live = false;
     s.visits = kTruncated;
-    if (kd.trunc) atomicAdd(kd.trunc, 1u);
+    if (kd.trunc && sub == 0u) atomicAdd(kd.trunc, 1u);
   }
 }
 

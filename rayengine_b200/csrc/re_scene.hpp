@@ -28,5 +28,5 @@ struct re_scene {
   int blocks_per_sm = 0;
   float ao_length = 1.0f;    // AO ray length of the last primary pass
   uint32_t queue_stride = 0;  // record capacity per ray kind in d_queue
-  re_tuning tune = {0, 0, 32, 32};
+  re_tuning tune = {0, 0, 32, 32, 1};
 };

@@ -124,6 +124,41 @@ __global__ void __launch_bounds__(256, 6) k_primary_tiles(KdDev kd, CamDev cam, 
   }
 }
 
+// Primary rays with G lanes per ray (ray_lanes 2, 4 or 8): persistent warps
+// over tiles of 32 / G pixels, 4 wide; the lanes of a ray split each leaf's
+// triangle tests (trav_step with G).  For frames whose pass time is set by
+// the longest walks rather than by throughput (a 512x512 frame of a 2^20-
+// triangle soup takes as long as a 64x64 one), the G-fold shorter test
+// chain per leaf shortens the critical path.
+template <int MODE, uint32_t G>
+__global__ void __launch_bounds__(256, 6) k_primary_lanes(KdDev kd, CamDev cam, uint32_t w,
+                                                       uint32_t h, re_hit* __restrict__ out,
+                                                       uint4* __restrict__,
+                                                       uint32_t* __restrict__ tile_counter,
+                                                       uint32_t) {
+  constexpr uint32_t kRows = 32u / G / 4u;  // tile height; 4 pixels wide
+  extern __shared__ uint2 snodes[];
+  stage_nodes(kd, snodes);
+  const uint32_t lane = threadIdx.x & 31u, r = lane / G;
+  const uint32_t tiles_x = (w + 3) / 4, tiles = tiles_x * ((h + kRows - 1) / kRows);
+  for (;;) {
+    uint32_t tile = warp_fetch(tile_counter);
+    if (tile >= tiles) break;
+    uint32_t x = (tile % tiles_x) * 4 + (r & 3u);
+    uint32_t y = (tile / tiles_x) * kRows + (r >> 2);
+    if (x >= w || y >= h) continue;  // the whole group skips
+    V3 o, d;
+    generate_ray(cam, w, h, x, y, o, d);
+    Trav s;
+    Counters c = {0, 0, 0, 0};
+    trav_init(s, kd, o, d, __int_as_float(0x7f800000), 0u);
+    while (s.live) trav_step<MODE, false, false, G>(s, kd, snodes, c);
+    HitState hs;
+    trav_result(s, hs);
+    if ((lane & (G - 1u)) == 0u) store_hit(out, (size_t)y * w + x, hs);
+  }
+}
+
 // Primary rays with lane refill (ray_refill_min < 32).  Work index i is lane
 // i % 32 of 8x4 pixel tile i / 32, so a warp's claims stay in one screen
 // region.
@@ -448,6 +483,7 @@ KdDev kd_view(const re_scene* s) {
   kd.max_visits = s->max_visits;
   kd.stage = s->stage;
   kd.trunc = s->d_counters + RE_SCENE_TRUNC_SLOT;
+  kd.num_refs = s->host.num_refs;
   return kd;
 }
 
@@ -559,16 +595,21 @@ re_status create_from_packed(const float* tris, uint32_t n, const re_kd_params* 
 namespace re {
 namespace {
 
-// One primary pass: whole-warp tiles when ray_refill_min is 32, else lane
-// refill.  Both kernels take the same arguments.
+// One primary pass: G lanes per ray when ray_lanes > 1 (hits only), else
+// whole-warp tiles when ray_refill_min is 32, else lane refill.  All
+// kernels take the same arguments.
 template <int MODE, bool COUNT>
 re_status launch_primary(re_scene* s, const re_camera& cam, uint32_t w, uint32_t h, re_hit* out,
                          uint4* counts, cudaStream_t st) {
   KdDev kd = kd_view(s);
   CamDev cd = cam_view(cam);
   size_t smem = kd.stage * sizeof(uint2);
-  uint32_t refill = s->tune.ray_refill_min;
-  auto k = refill >= 32u ? k_primary_tiles<MODE, COUNT> : k_primary<MODE, COUNT>;
+  uint32_t refill = s->tune.ray_refill_min, lanes = COUNT ? 1u : s->tune.ray_lanes;
+  auto k = lanes == 2u   ? k_primary_lanes<MODE, 2>
+           : lanes == 4u ? k_primary_lanes<MODE, 4>
+           : lanes == 8u ? k_primary_lanes<MODE, 8>
+           : refill >= 32u ? k_primary_tiles<MODE, COUNT>
+                           : k_primary<MODE, COUNT>;
   RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<grid_for(k, smem), 256, smem, st>>>(kd, cd, w, h, out, counts, s->d_counters, refill);
@@ -971,7 +1012,10 @@ RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t) {
                     "re_scene_set_tuning: refill_min and ray_refill_min must be in [1, 32]");
   if (t->queue_kind_major > 2)
     return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0, 1 or 2");
+  if (t->ray_lanes > 8 || (t->ray_lanes & (t->ray_lanes - 1u)))
+    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: ray_lanes must be 0, 1, 2, 4 or 8");
   s->tune = *t;
+  if (s->tune.ray_lanes == 0) s->tune.ray_lanes = 1;
   s->tune.stage_nodes = std::min(std::min(t->stage_nodes, s->host.bfs_nodes), re::kMaxStage);
   s->stage = s->tune.stage_nodes;
   return RE_OK;
@@ -1005,7 +1049,10 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
     if (si > 0 && stages[si] == stages[si - 1]) continue;
     for (uint32_t km = 0; km < 3 && rs == RE_OK; ++km) {
       for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
-        re_tuning t = {stages[si], km, refills[ri], keep.ray_refill_min};
+        re_tuning t = keep;
+        t.stage_nodes = stages[si];
+        t.queue_kind_major = km;
+        t.refill_min = refills[ri];
         rs = re_scene_set_tuning(s, &t);
         if (rs != RE_OK) break;
         rs = re_render_ao(s, cam, w, h, p, hits, mask, nullptr, stream);
@@ -1045,9 +1092,10 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
 }
 
 // Times the primary pass (re_trace_primary with `flags`) for every
-// combination of staging depth and ray refill threshold (one warm-up and
-// three timed passes each, CUDA events on the caller's stream) and keeps the
-// fastest on the scene.  Set-up time only: it allocates its own output.
+// combination of staging depth and walk form (one lane per ray with each
+// refill threshold, or 2, 4 or 8 lanes per ray; one warm-up and three timed
+// passes each, CUDA events on the caller's stream) and keeps the fastest on
+// the scene.  Set-up time only: it allocates its own output.
 RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
                                      uint32_t flags, re_tuning* best_out, float* best_ms_out,
                                      void* stream) {
@@ -1067,13 +1115,16 @@ RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t
   float best_ms = 1e30f;
   uint32_t bfs = std::min(s->host.bfs_nodes, re::kMaxStage);
   const uint32_t stages[3] = {0u, std::min(1024u, bfs), std::min(4096u, bfs)};
-  const uint32_t refills[4] = {32u, 16u, 8u, 4u};
+  // {ray_lanes, ray_refill_min}
+  const uint32_t forms[7][2] = {{1u, 32u}, {1u, 16u}, {1u, 8u}, {1u, 4u},
+                                {2u, 32u}, {4u, 32u}, {8u, 32u}};
   for (int si = 0; si < 3 && ce == cudaSuccess && rs == RE_OK; ++si) {
     if (si > 0 && stages[si] == stages[si - 1]) continue;
-    for (int ri = 0; ri < 4 && rs == RE_OK; ++ri) {
+    for (int fi = 0; fi < 7 && rs == RE_OK; ++fi) {
       re_tuning t = keep;
       t.stage_nodes = stages[si];
-      t.ray_refill_min = refills[ri];
+      t.ray_lanes = forms[fi][0];
+      t.ray_refill_min = forms[fi][1];
       rs = re_scene_set_tuning(s, &t);
       if (rs != RE_OK) break;
       rs = re_trace_primary(s, cam, w, h, flags, hits, stream);

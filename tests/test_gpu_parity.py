@@ -177,6 +177,64 @@ def test_ray_refill_threshold_changes_only_speed(cuda):
         assert np.array_equal(_hits(sc.trace_primary(cam, 200, 120)), ref)
 
 
+@pytest.mark.parametrize("leaf,mode", [(8, 0), (8, 1), (32, 0)])
+def test_lanes_per_ray_same_hits(cuda, leaf, mode):
+    """2, 4 or 8 lanes per primary ray split each leaf's triangle tests and
+    keep the smallest (t, id): every hit (id, t, u, v) equals the oracle's
+    one-lane walk, on an image whose sides are no multiple of the tiles, with
+    leaves holding more references than lanes."""
+    cfg = rb.configs.SoupConfig(num_tris=16384, width=203, height=119)
+    packed = cfg.packed()
+    cam = cfg.camera()
+    W, H = cfg.width, cfg.height
+    with rb.KDScene.from_packed(packed, rb.kd_params(leaf_size=leaf, max_depth=24)) as sc:
+        st, kd = _kd(sc)
+        assert st["max_leaf_size"] > (8 if leaf > 8 else 1)
+        ref = po.primary_kd(kd, cam, W, H, mode=mode).view(np.int32).reshape(-1, 4)
+        assert (ref[:, 0] >= 0).mean() > 0.2
+        t = sc.tuning()
+        assert t["ray_lanes"] == 1
+        for lanes in (2, 4, 8, 1):
+            for stage in (0, 1024):
+                sc.set_tuning(stage, t["queue_kind_major"], t["refill_min"], 32, lanes)
+                got = _hits(sc.trace_primary(cam, W, H, mode))
+                assert np.array_equal(got, ref), (lanes, stage)
+        # the counting pass is one lane per ray whatever the setting
+        sc.set_tuning(t["stage_nodes"], t["queue_kind_major"], t["refill_min"], 32, 4)
+        _, rc = po.primary_kd(kd, cam, W, H, mode=mode, counts=True)
+        cnt = sc.count_primary(cam, W, H, mode).cpu().numpy()
+        assert np.array_equal(cnt, rc.view(np.uint32).reshape(-1, 4).astype(np.int32))
+
+
+@pytest.mark.parametrize("lanes", [2, 4])
+def test_lanes_per_ray_visit_cap(cuda, lanes):
+    """With several lanes per ray a walk stopped at the leaf-visit cap is
+    counted once and keeps the oracle's hit."""
+    cfg = rb.configs.SoupConfig(num_tris=8192, width=160, height=120)
+    cam = cfg.camera()
+    W, H = cfg.width, cfg.height
+    with rb.KDScene.from_packed(cfg.packed(), rb.kd_params(leaf_size=8, max_leaf_visits=2)) as sc:
+        st, kd = _kd(sc)
+        ref, rc = po.primary_kd(kd, cam, W, H, max_visits=2, counts=True)
+        t = sc.tuning()
+        sc.set_tuning(t["stage_nodes"], t["queue_kind_major"], t["refill_min"], 32, lanes)
+        got = _hits(sc.trace_primary(cam, W, H))
+        assert np.array_equal(got, ref.view(np.int32).reshape(-1, 4))
+        n_cut = int((rc["status"] == 1).sum())
+        assert n_cut > 100 and sc.truncated() == n_cut
+
+
+def test_autotune_primary_considers_lanes(cuda):
+    cfg = rb.configs.SoupConfig(num_tris=65536)
+    with rb.KDScene.from_packed(cfg.packed(), cfg.kd_params()) as sc:
+        st, kd = _kd(sc)
+        cam = cfg.camera()
+        best = sc.autotune_primary(cam, 128, 128)
+        assert best["ray_lanes"] in (1, 2, 4, 8) and sc.tuning()["ray_lanes"] == best["ray_lanes"]
+        ref = po.primary_kd(kd, cam, 128, 128).view(np.int32).reshape(-1, 4)
+        assert np.array_equal(_hits(sc.trace_primary(cam, 128, 128)), ref)
+
+
 def test_heightfield_kernel_bitexact(cuda):
     cfg = rb.configs.HeightfieldConfig()
     P = po.perm(cfg.seed)

@@ -71,6 +71,24 @@ def test_host_only_scene_refuses_to_trace():
     sc.close()
 
 
+def test_tuning_validation():
+    """ray_lanes: 1 by default, 0 reads as 1, powers of two up to 8 only."""
+    packed = rb.configs.SoupConfig(num_tris=64).packed()
+    with rb.KDScene.build_host(packed) as sc:
+        t = sc.tuning()
+        assert t["ray_lanes"] == 1 and t["ray_refill_min"] == 32
+        for lanes in (2, 4, 8, 1):
+            sc.set_tuning(t["stage_nodes"], 0, 8, 32, lanes)
+            assert sc.tuning()["ray_lanes"] == lanes
+        sc.set_tuning(t["stage_nodes"], 0, 8, 32, 0)
+        assert sc.tuning()["ray_lanes"] == 1
+        for bad in (3, 6, 16):
+            with pytest.raises(rb.RayEngineError) as e:
+                sc.set_tuning(t["stage_nodes"], 0, 8, 32, bad)
+            assert e.value.status == 1
+        assert sc.tuning()["ray_lanes"] == 1
+
+
 def test_plain_c_caller(tmp_path):
     """The header compiles as C11 and a C program drives the host-only
     entry points through the shared library (the ABI a C or FFI caller

@@ -249,8 +249,10 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w,
                                 uint32_t h, const re_ao_params* p,
                                 re_tuning* best, float* best_ms, void* stream);
 /* Autotuner of the primary pass: times re_trace_primary(flags) for each
- * combination of staging depth, ray_refill_min and ray_lanes the same way and keeps
- * the fastest (other fields unchanged).  Set-up time only. */
+ * combination of staging depth, ray_refill_min and ray_lanes and keeps the
+ * fastest (other fields unchanged).  Each timed pass follows a write of twice
+ * the L2 size (a frame whose tree is not cached).  Set-up time only: it
+ * allocates that scratch and its own output. */
 RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w,
                                      uint32_t h, uint32_t flags, re_tuning* best,
                                      float* best_ms, void* stream);

@@ -1095,7 +1095,11 @@ RE_API re_status re_autotune_ao(re_scene* s, const re_camera* cam, uint32_t w, u
 // combination of staging depth and walk form (one lane per ray with each
 // refill threshold, or 2, 4 or 8 lanes per ray; one warm-up and three timed
 // passes each, CUDA events on the caller's stream) and keeps the fastest on
-// the scene.  Set-up time only: it allocates its own output.
+// the scene.  Each timed pass follows a write of twice the L2 size, so the
+// forms are compared on a frame whose tree is not cached (as after other
+// work; back-to-back passes with a warm L2 favoured forms that lose on a
+// cold one).  Set-up time only: it allocates its own output and the
+// scratch it writes.
 RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t w, uint32_t h,
                                      uint32_t flags, re_tuning* best_out, float* best_ms_out,
                                      void* stream) {
@@ -1107,9 +1111,14 @@ RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t
     return re::fail(RE_ERR_LIMIT, "re_autotune_primary: image > 2^28 pixels");
   cudaStream_t st = (cudaStream_t)stream;
   re_hit* hits = nullptr;
+  void* scratch = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int l2 = 0;
+  RE_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->device));
+  const size_t scratch_bytes = 2 * (size_t)std::max(l2, 1 << 20);
   RE_CUDA(cudaMalloc(&hits, (size_t)w * h * sizeof(re_hit)));
-  cudaError_t ce = cudaEventCreate(&e0);
+  cudaError_t ce = cudaMalloc(&scratch, scratch_bytes);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
   if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
   re_tuning keep = s->tune, best = s->tune;
   float best_ms = 1e30f;
@@ -1129,13 +1138,18 @@ RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t
       if (rs != RE_OK) break;
       rs = re_trace_primary(s, cam, w, h, flags, hits, stream);
       if (rs != RE_OK) break;
-      ce = cudaEventRecord(e0, st);
-      for (int r = 0; r < 3 && rs == RE_OK; ++r) rs = re_trace_primary(s, cam, w, h, flags, hits, stream);
-      if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
-      if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
       float ms = 0.f;
-      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-      if (ce != cudaSuccess) break;
+      for (int r = 0; r < 3 && rs == RE_OK && ce == cudaSuccess; ++r) {
+        ce = cudaMemsetAsync(scratch, r, scratch_bytes, st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+        if (ce == cudaSuccess) rs = re_trace_primary(s, cam, w, h, flags, hits, stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float one = 0.f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&one, e0, e1);
+        ms += one;
+      }
+      if (ce != cudaSuccess || rs != RE_OK) break;
       if (ms < best_ms) {
         best_ms = ms;
         best = s->tune;
@@ -1145,6 +1159,7 @@ RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(hits);
+  cudaFree(scratch);
   if (ce != cudaSuccess || rs != RE_OK) {
     s->tune = keep;
     s->stage = keep.stage_nodes;

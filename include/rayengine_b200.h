@@ -677,6 +677,11 @@ RE_API re_status re_batch_autotune(re_batch* b, float* d_radiance, void* stream,
  * denominator of the traversal kernels' L2 roofline.  No reference
  * counterpart. */
 RE_API re_status re_measure_l2_read(size_t bytes, uint32_t passes, float* gbs, void* stream);
+/* FP32 fused multiply-add rate (8 independent chains of `iters` FMAs per
+ * thread, 8 blocks of 256 threads per SM, `iters` in [1024, 2^20]), in
+ * 10^12 FMAs per second: the denominator of the SIMT field kernels'
+ * roofline.  No reference counterpart. */
+RE_API re_status re_measure_fp32_fma(uint32_t iters, float* tops, void* stream);
 
 #ifdef __cplusplus
 }

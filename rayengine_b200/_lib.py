@@ -281,6 +281,7 @@ _SIGS = {
     "re_trace_instances": (ctypes.c_int, [ctypes.POINTER(re_instance), _U32, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P, _P]),
     "re_instance_trig": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
     "re_measure_l2_read": (ctypes.c_int, [ctypes.c_size_t, _U32, ctypes.POINTER(_F), _P]),
+    "re_measure_fp32_fma": (ctypes.c_int, [_U32, ctypes.POINTER(_F), _P]),
     "re_mesh_load": (ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(ctypes.c_void_p)]),
     "re_mesh_info": (ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "re_mesh_copy": (ctypes.c_int, [_P, _P, _P]),

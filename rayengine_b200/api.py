@@ -869,3 +869,11 @@ def measure_l2_read_gbs(nbytes: int = 32 << 20, passes: int = 100, stream=None) 
     v = ctypes.c_float()
     call("re_measure_l2_read", nbytes, passes, ctypes.byref(v), _stream_ptr(stream))
     return float(v.value)
+
+
+def measure_fp32_fma_tops(iters: int = 1 << 16, stream=None) -> float:
+    """FP32 fused multiply-adds per second of this GPU, in 10^12
+    (re_measure_fp32_fma; one FMA counts as one operation)."""
+    v = ctypes.c_float()
+    call("re_measure_fp32_fma", iters, ctypes.byref(v), _stream_ptr(stream))
+    return float(v.value)

@@ -1,6 +1,8 @@
-// L2 read-bandwidth probe: the denominator the benchmark uses for the
-// traversal kernels' L2 roofline (their node, leaf and triangle reads mostly
-// hit L2; no measured L2 figure is supplied with the hardware peaks).
+// Measurement probes: the denominators the benchmark uses where the hardware
+// peaks supplied with the pool have no figure.
+//   L2 read bandwidth  the traversal kernels' L2 roofline (their node, leaf
+//                      and triangle reads mostly hit L2)
+//   FP32 FMA rate      the SIMT field kernels (noise, sphere tracing)
 #include <cuda_runtime.h>
 
 #include "re_common.hpp"
@@ -24,6 +26,23 @@ __global__ void k_l2_read(const uint4* __restrict__ buf, size_t n, uint32_t pass
       acc.w ^= v.w;
     }
   if ((acc.x ^ acc.y ^ acc.z ^ acc.w) == 0x9E3779B9u) sink[0] = acc;
+}
+
+// Every thread runs 8 independent FMA chains of `iters` steps; the operands
+// come from the arguments so nothing folds, and the sum goes to `sink` only
+// if it equals an impossible value.
+__global__ void __launch_bounds__(256) k_fma(uint32_t iters, float a, float b, float* sink) {
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = (float)(threadIdx.x + k);
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = __fmaf_rn(x[k], a, b);
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc += x[k];
+  if (acc == -1.2345e-30f) sink[0] = acc;
 }
 
 }  // namespace
@@ -66,6 +85,42 @@ RE_API re_status re_measure_l2_read(size_t bytes, uint32_t passes, float* gbs, v
   cudaFree(sink);
   if (e != cudaSuccess) return re::cuda_fail(e, "re_measure_l2_read");
   *gbs = (float)((double)bytes * passes / (ms / 1e3) / 1e9);
+  return RE_OK;
+}
+
+// FP32 fused multiply-add rate: one launch of 8 blocks of 256 threads per
+// SM, each thread 8 independent chains of `iters` FMAs, after a warm-up
+// launch; *tops = FMAs (one operation each) / kernel time, in 10^12/s.
+RE_API re_status re_measure_fp32_fma(uint32_t iters, float* tops, void* stream) {
+  if (!tops || iters < 1024 || iters > (1u << 20))
+    return re::fail(RE_ERR_INVALID_ARG, "re_measure_fp32_fma: iters in [1024, 2^20]");
+  cudaStream_t st = (cudaStream_t)stream;
+  float* sink = nullptr;
+  RE_CUDA(cudaMalloc(&sink, sizeof(float)));
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  const int grid = 8 * re::sm_count(), block = 256;
+  // a = 1 - 2^-20 keeps the chains finite and away from denormals
+  const float fa = 0.99999905f, fb = 0.5f;
+  if (e == cudaSuccess) {
+    re::k_fma<<<grid, block, 0, st>>>(iters / 8u, fa, fb, sink);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(a, st);
+  if (e == cudaSuccess) {
+    re::k_fma<<<grid, block, 0, st>>>(iters, fa, fb, sink);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(b, st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return re::cuda_fail(e, "re_measure_fp32_fma");
+  *tops = (float)((double)grid * block * 8.0 * iters / (ms / 1e3) / 1e12);
   return RE_OK;
 }
 

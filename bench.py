@@ -815,8 +815,11 @@ class NeuralTerrainSDF:
         R = self.rays_per_step
         return {"workload": "neural-SDF surrogate of d(p)=p.y-3fBm(0.25p) (8 octaves), 1920x1080: "
                             "Fourier features (16 freqs) -> 4x64 softplus MLP, BF16 tcgen05 inference; "
-                            "network march then exact phase (bracket + 4 regula-falsi steps) + exact "
-                            "central-difference normal",
+                            f"network phase: one cone per {n.cone_tile}x{n.cone_tile} pixel tile "
+                            f"({n.cone_lanes} lanes per cone, speculative steps); exact phase from "
+                            "the cone's stop (the exact tracer's steps, grown up to "
+                            f"{n.relax}x along the secant; bracket + {n.root_steps} regula-falsi "
+                            "steps) + exact central-difference normal",
                 "training": {"points": n.num_points, "steps": n.train_steps, "batch": n.batch,
                              "lr": n.lr, "seconds": round(self.train_s, 2),
                              "final_l1_loss": round(self.final_loss, 5)},
@@ -824,7 +827,9 @@ class NeuralTerrainSDF:
                                  "lipschitz_quantile": n.lipschitz_quantile,
                                  "safety": n.safety, "switch_dist": n.switch_dist,
                                  "min_step": n.min_step, "max_network_steps": n.max_network_steps,
-                                 "root_steps": n.root_steps},
+                                 "root_steps": n.root_steps, "cone_tile": n.cone_tile,
+                                 "cone_lanes": n.cone_lanes, "relax": n.relax,
+                                 "normal_taps": n.normal_taps},
                 "per_ray": {"network_evals": round(st["network_evals"] / R, 3),
                             "network_rows": round(st["network_rows"] / R, 3),
                             "exact_evals": round(st["exact_evals"] / R, 3),
@@ -836,19 +841,28 @@ class NeuralTerrainSDF:
     def phases(self, stream):
         W, H = self.cfg.width, self.cfg.height
         m = self.model
-        return [("nsdf_march", lambda: m.trace(self.params, self.tp, self.cam, W, H, self.out, stream,
-                                               phase="network")),
+        return [("nsdf_network", lambda: m.trace(self.params, self.tp, self.cam, W, H, self.out,
+                                                 stream, phase="network")),
                 ("sdf_refine", lambda: m.trace(self.params, self.tp, self.cam, W, H, self.out, stream,
                                                phase="exact"))]
 
     def roofline(self, phase_ms, peaks):
+        """The dominant phase's roofline (the exact phase: FP32 field
+        evaluations against the measured FMA rate), with the network
+        phase's tensor-core fraction beside it."""
         rows = self.stats["network_rows"]
-        achieved = rows * NSDF_FLOPS_PER_EVAL / (phase_ms["nsdf_march"] / 1e3) / 1e12
-        return {"bound": "tensor", "kernel": "nsdf_march", "achieved": round(achieved, 2),
-                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                "frac": round(achieved / peaks["bf16_tflops"], 4), "peak_source": peaks["source"],
-                "alg_flops_per_launch": rows * NSDF_FLOPS_PER_EVAL,
-                "traffic": ncu_traffic(f"{self.name}:nsdf_march")}
+        achieved = rows * NSDF_FLOPS_PER_EVAL / (phase_ms["nsdf_network"] / 1e3) / 1e12
+        net = {"bound": "tensor", "kernel": "nsdf_network", "achieved": round(achieved, 2),
+               "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+               "frac": round(achieved / peaks["bf16_tflops"], 4), "peak_source": peaks["source"],
+               "alg_flops_per_launch": rows * NSDF_FLOPS_PER_EVAL,
+               "ms": round(phase_ms["nsdf_network"], 4),
+               "traffic": ncu_traffic(f"{self.name}:nsdf_network")}
+        if phase_ms["nsdf_network"] >= phase_ms["sdf_refine"]:
+            return net
+        evals = self.stats["exact_evals"] + self.stats["normal_evals"]
+        return fp32_roofline("sdf_refine", evals * SDF_OPS_PER_EVAL, phase_ms["sdf_refine"], peaks,
+                             self.name, network_phase=net)
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height

@@ -401,6 +401,16 @@ typedef struct re_nsdf_trace_params {
   float relax;          /* exact steps may grow along the secant up to     */
                         /* relax x step_factor * d; <= 1: the plain rule   */
   uint32_t flags;       /* RE_NSDF_EXACT_ONLY                              */
+  uint32_t cone_tile;   /* > 0 (<= 256): the network marches cones of      */
+                        /* cone_tile x cone_tile pixel tiles instead of    */
+                        /* single rays, and every pixel's exact phase      */
+                        /* starts where its tile's cone stopped; 0: the    */
+                        /* per-ray network march and hand-over queue       */
+  uint32_t cone_coarse; /* 0, or a multiple of cone_tile (<= 1024): a      */
+                        /* first cone level over tiles of this size        */
+  uint32_t normal_taps; /* 0 or 6: central differences; 4: tetrahedral    */
+  uint32_t cone_lanes;  /* 0 or 1, 2, 4, 8: lanes per cone; above 1 they   */
+                        /* evaluate successive guessed steps in one pass   */
 } re_nsdf_trace_params;
 
 RE_API uint32_t re_nsdf_num_params(void);
@@ -446,8 +456,12 @@ RE_API re_status re_nsdf_lipschitz(re_nsdf* s, uint32_t samples, float h,
                                    float quantile, float* out, void* stream);
 /* Neural march inside the network's box, then the exact phase: the exact
  * tracer's steps from the hand-over point, a bracketed crossing refined by
- * regula falsi, the exact tracer's central-difference normal.  Output as
- * re_sdf_trace (steps = network steps + exact evaluations). */
+ * regula falsi, the exact tracer's central-difference normal (or the
+ * reference's tetrahedral one).  With cone_tile > 0 the network phase
+ * marches one cone per pixel tile (the network distance less the cone's
+ * radius bounds the step of every ray of the tile) and each pixel's exact
+ * phase starts at its tile's stop.  Output as re_sdf_trace (steps =
+ * network steps + exact evaluations). */
 RE_API re_status re_nsdf_trace(re_nsdf* s, const re_sdf_params* field,
                                const re_nsdf_trace_params* tp,
                                const re_camera* cam, uint32_t w, uint32_t h,

@@ -161,6 +161,10 @@ class re_nsdf_trace_params(ctypes.Structure):
         ("root_steps", ctypes.c_uint32),
         ("relax", ctypes.c_float),
         ("flags", ctypes.c_uint32),
+        ("cone_tile", ctypes.c_uint32),
+        ("cone_coarse", ctypes.c_uint32),
+        ("normal_taps", ctypes.c_uint32),
+        ("cone_lanes", ctypes.c_uint32),
     ]
 
 

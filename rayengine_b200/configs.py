@@ -169,16 +169,30 @@ class NeuralTerrainConfig:
     lipschitz_samples: int = 200000
     lipschitz_h: float = 1e-2
     lipschitz_quantile: float = 0.5
-    # measured on B200 (1080p, 20k-step network): safety 1.2 with the
-    # hand-over at 0.6 gives 7.49 ms against 8.97 ms at (0.9, 0.3), with the
-    # same median error (8e-6) and ~45 of 2.07M pixels whose hit/miss differs
-    # from the exact tracer; larger steps (1.5-2.5) or the 0.25 gradient
-    # quantile run faster but let rays through thin ridges (550-3500 pixels)
+    # Network phase: one cone per 16x16 pixel tile, 8 lanes per cone
+    # evaluating guessed successive steps in one pass (measured on B200,
+    # 1080p, 20k-step network: cone + exact phase 3.21 ms against 7.62 ms
+    # for the per-ray network march below; the exact tracer 4.17 ms).
+    # Exact phase from the cone's stop: the exact tracer's steps allowed to
+    # grow 1.5x along the secant of the last two samples (median hit error
+    # 8e-5, ~850 of 2.07M pixels whose hit/miss differs from the exact
+    # tracer; relax 1.0: 27 pixels, 3.98 ms with 8x8 cones of one lane).
     safety: float = 1.2
-    switch_dist: float = 0.6
+    switch_dist: float = 0.3
     min_step: float = 0.05
     max_network_steps: int = 64
     root_steps: int = 4
+    cone_tile: int = 16
+    cone_lanes: int = 8
+    relax: float = 1.5
+    normal_taps: int = 6
+    # the per-ray network march (cone_tile 0), measured on B200: safety 1.2
+    # with the hand-over at 0.6 gives 7.49 ms against 8.97 ms at (0.9,
+    # 0.3), with the same median error (8e-6) and ~45 of 2.07M pixels whose
+    # hit/miss differs from the exact tracer; larger steps (1.5-2.5) or the
+    # 0.25 gradient quantile run faster but let rays through thin ridges
+    # (550-3500 pixels)
+    per_ray_switch_dist: float = 0.6
 
     def __post_init__(self):
         if self.terrain is None:
@@ -202,8 +216,17 @@ class NeuralTerrainConfig:
         return m, tp, losses
 
     def trace_params(self, lipschitz):
+        """The cone tracer's settings (the default method)."""
         return api.nsdf_trace_params(lipschitz, self.safety, self.switch_dist, self.min_step,
-                                     self.max_network_steps, 0, self.root_steps)
+                                     self.max_network_steps, 0, self.root_steps, self.relax,
+                                     cone_tile=self.cone_tile, cone_lanes=self.cone_lanes,
+                                     normal_taps=self.normal_taps)
+
+    def per_ray_params(self, lipschitz):
+        """The per-ray network march with its hand-over queue, the exact
+        tracer's plain steps and central-difference normal."""
+        return api.nsdf_trace_params(lipschitz, self.safety, self.per_ray_switch_dist,
+                                     self.min_step, self.max_network_steps, 0, self.root_steps)
 
 
 @dataclass

@@ -969,7 +969,21 @@ struct RefineDev {
   uint32_t root_steps;  // regula-falsi steps on a bracketed crossing
   float relax;          // an exact step may grow to relax x (step_factor * d) along a secant
   float ceiling;        // no surface above this height (bound of the field)
+  uint32_t normal_taps;  // 6: central differences; 4: tetrahedral
+  // cone starts (direct mode): pixel (x, y) starts at tile_t[(y / cone_tile)
+  // * cone_tiles_x + x / cone_tile]; null: every pixel starts at t = 0
+  const float* tile_t;
+  uint32_t cone_tile, cone_tiles_x;
 };
+
+// Tap k of the tetrahedral normal (compute_sdf_normal_tet,
+// sdf_functions.cuh:518-532): 0.5773 (2 b - 1) with b = (((k + 3) >> 1) & 1,
+// (k >> 1) & 1, k & 1), i.e. the corners (+,-,-), (-,-,+), (-,+,-), (+,+,+)
+// of a cube scaled to length ~1.
+__device__ __forceinline__ V3 tet_dir(uint32_t k) {
+  const float c = 0.5773f;
+  return v3((((k + 3u) >> 1) & 1u) ? c : -c, ((k >> 1) & 1u) ? c : -c, (k & 1u) ? c : -c);
+}
 
 // Slab test of the ray against the box: [t0, t1] with t0 >= 0 (empty if t0 >= t1).
 __device__ __forceinline__ void box_span(const MarchDev& md, const V3& o, const V3& d, float& t0,
@@ -1105,6 +1119,175 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_march(InputMap m,
   tc_teardown(s);
 }
 
+// Cone tiles of the network phase: tile x tile pixels, tiles_x x tiles_y of
+// them; parent (may be null): start parameters of coarser tiles of
+// parent_tile pixels (a multiple of tile), parent_tiles_x per row.
+struct ConeDev {
+  uint32_t tile, tiles_x, tiles_y;
+  const float* parent;
+  uint32_t parent_tile, parent_tiles_x;
+};
+
+// Cone phase.  Each tile's cone is marched by K consecutive lanes of a
+// warp.  The axis is the normalised sum of the tile's four corner rays, and
+// `s` the largest chord from the axis direction to a corner ray's.  The
+// angle to the axis is quasi-convex over the image plane, so the corners
+// bound it: every ray of the tile lies within t s of the axis point at the
+// same parameter t, and a point of a tile ray within a further dt lies
+// within dt + t s of the axis point.  The clearance c = d_net - t s (the
+// network distance shrunk by the cone's radius) therefore bounds a step of
+// alpha c for every ray of the tile, the per-ray rule's step.
+//
+// Speculation: in one pass lane j of a tile evaluates the axis at t + dt
+// (r + r^2 + ... + r^j), dt the last accepted step and r = 0.9 x the ratio
+// of the last two (the steps of a cone closing in on a surface shrink
+// geometrically, in open space they grow).  The lanes' spheres are chained
+// in order: a point that lies inside the part already cleared extends it to
+// t_j + alpha c_j, a point beyond it ends the chain, and the first chained
+// point whose clearance is below switch_dist stops the tile there.  Lane 0
+// is at t, so a pass advances at least one sequential step, and up to K
+// when the guesses land; K = 1 is plain cone marching.
+//
+// The axis starts at its entry into the network's box (or the parent tile's
+// start, if later); a tile whose axis leaves the box stops at the exit, and
+// one that makes max_steps passes stops where it is.  Every pixel of the
+// tile then starts its exact phase at the tile's parameter (k_sdf_refine).
+template <uint32_t K>
+__global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_cone(InputMap m,
+                                                             const unsigned char* __restrict__ pack,
+                                                             MarchDev md, ConeDev cd, CamDev cam,
+                                                             uint32_t w, uint32_t h,
+                                                             uint32_t* __restrict__ cursor,
+                                                             unsigned long long* __restrict__ totals,
+                                                             float* __restrict__ tile_t,
+                                                             int* __restrict__ err) {
+  static_assert(K == 1 || K == 2 || K == 4 || K == 8, "lanes per cone: 1, 2, 4 or 8");
+  extern __shared__ unsigned char smem_raw[];
+  TcSmem& s = tc_smem(smem_raw);
+  tc_setup(s, pack);
+  const int tid = threadIdx.x, g = tid >> 7, row = tid & 127;
+  const uint32_t lane = tid & 31u;
+  const uint32_t j = lane & (K - 1u), lead = lane & ~(K - 1u);
+  const uint32_t kmask = (K == 1 ? 1u : ((1u << K) - 1u)) << lead;
+  uint32_t phase = 0;
+  const uint32_t total = cd.tiles_x * cd.tiles_y;
+  bool live = false, exhausted = false, ok = true;
+  uint32_t tile = 0, passes = 0;
+  V3 o = {0.f, 0.f, 0.f}, ax = {0.f, 0.f, 1.f};
+  float t = 0.f, dt = 0.f, ratio = 1.f, t_end = 0.f, chord = 0.f;
+  uint32_t n_live = 0, n_rows = 0;
+  for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
+    // the K lanes of a tile share `live`, so a tile's first lane speaks for it
+    const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live && j == 0u);
+    const uint32_t nidle = __popc(idle);
+    if (!exhausted && nidle * K >= 8u) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(cursor, nidle);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + nidle >= total) exhausted = true;
+      const uint32_t i =
+          __shfl_sync(0xFFFFFFFFu, base + __popc(idle & ((1u << lane) - 1u)), lead);
+      if (!live && i < total) {
+        // every lane of the tile computes the same set-up
+        tile = i;
+        const uint32_t x0 = (i % cd.tiles_x) * cd.tile, y0 = (i / cd.tiles_x) * cd.tile;
+        const uint32_t x1 = min(x0 + cd.tile - 1u, w - 1u), y1 = min(y0 + cd.tile - 1u, h - 1u);
+        V3 c[4];
+        generate_ray(cam, w, h, x0, y0, o, c[0]);
+        generate_ray(cam, w, h, x1, y0, o, c[1]);
+        generate_ray(cam, w, h, x0, y1, o, c[2]);
+        generate_ray(cam, w, h, x1, y1, o, c[3]);
+        ax = normalize(v3(c[0].x + c[1].x + c[2].x + c[3].x, c[0].y + c[1].y + c[2].y + c[3].y,
+                          c[0].z + c[1].z + c[2].z + c[3].z));
+        chord = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          V3 e = sub(c[k], ax);
+          chord = fmaxf(chord, sqrtf(dot(e, e)));
+        }
+        // rounding of the corner rays and of the axis
+        chord = chord * 1.001f + 1e-6f;
+        float t0, t1;
+        box_span(md, o, ax, t0, t1);
+        float start =
+            cd.parent ? cd.parent[(y0 / cd.parent_tile) * cd.parent_tiles_x + x0 / cd.parent_tile]
+                      : 0.f;
+        t = fmaxf(t0, start);
+        t_end = t1;
+        dt = 0.f;
+        ratio = 1.f;
+        passes = 0;
+        if (t < t_end) live = true;
+        else if (j == 0u) tile_t[tile] = start;
+      }
+    }
+    if (!group_or(g, live || !exhausted)) break;
+    float off = 0.f;
+    {
+      const float r = 0.9f * ratio;
+      float rp = 1.f;
+      for (uint32_t i = 0; i < j; ++i) {
+        rp *= r;
+        off += rp;
+      }
+    }
+    const float tj = __fmaf_rn(off, dt, t);
+    float q[3];
+    normalise(m, __fmaf_rn(tj, ax.x, o.x), __fmaf_rn(tj, ax.y, o.y), __fmaf_rn(tj, ax.z, o.z), q);
+    float dn = mlp_row(s, m, g, row, q, phase, ok);
+    if (!group_and(g, ok)) break;
+    ++n_rows;
+    n_live += live ? 1u : 0u;
+    if (live) {
+      // all K lanes of the tile are here together and reach the same verdict
+      const float cj = dn - tj * chord;
+      float cov = t, t_stop = 0.f, s_last = dt, s_prev = dt;
+      bool chained = true, stop = false;
+#pragma unroll
+      for (uint32_t k = 0; k < K; ++k) {
+        const float tk = K == 1 ? tj : __shfl_sync(kmask, tj, lead + k);
+        const float ck = K == 1 ? cj : __shfl_sync(kmask, cj, lead + k);
+        if (chained && !stop) {
+          if (tk > cov) {
+            chained = false;
+          } else if (ck < md.switch_dist) {
+            stop = true;
+            t_stop = tk;
+          } else {
+            cov = fmaxf(cov, tk + md.alpha * ck);
+            s_prev = s_last;
+            s_last = md.alpha * ck;
+          }
+        }
+      }
+      ++passes;
+      if (stop) {
+        if (j == 0u) tile_t[tile] = t_stop;
+        live = false;
+      } else {
+        t = cov;
+        ratio = s_prev > 0.f ? fminf(fmaxf(s_last / s_prev, 0.25f), 4.f) : 1.f;
+        dt = s_last;
+        if (t >= t_end) {
+          if (j == 0u) tile_t[tile] = t_end;
+          live = false;
+        } else if (passes >= md.max_steps) {
+          if (j == 0u) tile_t[tile] = t;
+          live = false;
+        }
+      }
+    }
+  }
+  n_live = __reduce_add_sync(0xFFFFFFFFu, n_live);
+  n_rows = __reduce_add_sync(0xFFFFFFFFu, n_rows);
+  if (lane == 0) {
+    atomicAdd(&totals[0], (unsigned long long)n_live);
+    atomicAdd(&totals[3], (unsigned long long)n_rows);
+  }
+  if (!ok && row == 0) atomicExch(err, 1);
+  tc_teardown(s);
+}
+
 // Exact phase, one lane per ray with lane refill (from the queue, or from
 // the pixel cursor when `direct`: every pixel from t = 0, the same method
 // without the network).  One field evaluation per trip of a state machine:
@@ -1119,7 +1302,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_march(InputMap m,
 //          over the surface).
 //   root   Illinois regula falsi on the bracket, root_steps evaluations or
 //          until |d| < 1e-6.
-//   normal the exact tracer's central differences (delta = 0.002 t).
+//   normal the exact tracer's central differences (delta = 0.002 t), or,
+//          with normal_taps 4, the reference's tetrahedral normal
+//          (compute_sdf_normal_tet) at the same radius: sum of e_k d(p +
+//          delta e_k) over the four tetrahedron directions e_k.
+// With cone starts a ray begins its march where its tile's cone stopped; a
+// start that is already inside the terrain (the network overestimated the
+// distance) marches again from the camera.
 // The step count written is network steps + exact march/probe/root
 // evaluations (normals excluded, as in the exact tracer).
 enum : uint32_t { kMarch = 0, kProbe = 1, kRoot = 2, kNormal = 3 };
@@ -1134,7 +1323,10 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
   load_perm(perm, perm_smem);
   Perm P = perm_view(perm_smem);
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t total = direct ? w * h : counters[1];
+  // direct mode claims pixels in 8x4 tiles (claim i = lane i & 31 of tile
+  // i >> 5), so a warp's rays start close together
+  const uint32_t dtiles_x = (w + 7) / 8;
+  const uint32_t total = direct ? dtiles_x * ((h + 3) / 4) * 32u : counters[1];
   bool live = false, exhausted = false, have_lo = false, restarted = false;
   uint32_t pix = 0, steps = 0, base_steps = 0, mode = kMarch, tap = 0, iters = 0;
   int side = 0;
@@ -1152,12 +1344,21 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       if (base + nidle >= total) exhausted = true;
       if (!live) {
         uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
-        if (i < total) {
-          uint4 e = direct ? make_uint4(i, 0u, 0u, 0u) : queue[i];
+        uint32_t dx = 0, dy = 0;
+        if (direct) {
+          dx = ((i >> 5) % dtiles_x) * 8 + (i & 7u);
+          dy = ((i >> 5) / dtiles_x) * 4 + ((i >> 3) & 3u);
+        }
+        if (i < total && (!direct || (dx < w && dy < h))) {
+          uint4 e = direct ? make_uint4(dy * w + dx, 0u, 0u, 0u) : queue[i];
           pix = e.x;
           generate_ray(cam, w, h, pix % w, pix / w, o, d);
           t = __uint_as_float(e.y);
           t_lo = __uint_as_float(e.z);
+          if (direct && rd.tile_t) {
+            t = rd.tile_t[((pix / w) / rd.cone_tile) * rd.cone_tiles_x + (pix % w) / rd.cone_tile];
+            t_lo = t;
+          }
           base_steps = e.w;
           steps = 0;
           mode = kMarch;
@@ -1179,6 +1380,9 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       qp = v3(__fmaf_rn(a, d.x, o.x), __fmaf_rn(a, d.y, o.y), __fmaf_rn(a, d.z, o.z));
     } else if (mode == kRoot) {
       qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
+    } else if (rd.normal_taps == 4u) {
+      V3 e = tet_dir(tap);
+      qp = v3(__fmaf_rn(e.x, delta, p.x), __fmaf_rn(e.y, delta, p.y), __fmaf_rn(e.z, delta, p.z));
     } else {
       float sd = (tap & 1u) ? -delta : delta;
       qp = p;
@@ -1203,6 +1407,12 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
           vb = v;
           a = t_lo;
           mode = kProbe;
+        } else if (rd.tile_t && !restarted) {
+          // the cone start lies inside: march again from the camera
+          t = 0.f;
+          t_lo = 0.f;
+          restarted = true;
+          if (steps >= rd.max_steps) status = 2;
         } else {
           hit_here = true;
         }
@@ -1255,6 +1465,13 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
         }
         t = b - vb * (b - a) / (vb - va);
       }
+    } else if (rd.normal_taps == 4u) {
+      V3 e = tet_dir(tap);
+      nx = __fmaf_rn(e.x, v, nx);
+      ny = __fmaf_rn(e.y, v, ny);
+      nz = __fmaf_rn(e.z, v, nz);
+      if (tap == 3) status = 1;
+      else ++tap;
     } else {
       if ((tap & 1u) == 0u) {
         plus = v;
@@ -1278,6 +1495,7 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       delta = 0.002f * t;
       mode = kNormal;
       tap = 0;
+      nx = ny = nz = 0.f;
     }
     if (status != 3) {
       float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1;
@@ -1349,6 +1567,11 @@ struct re_nsdf {
   uint4* queue = nullptr;
   size_t queue_cap = 0;
   int* err = nullptr;
+  // cone phase: start parameters of the fine tiles, then of the coarse ones;
+  // the image and fine tile size of the last network phase that wrote them
+  float* cone_t = nullptr;
+  size_t cone_cap = 0;
+  uint32_t cone_w = 0, cone_h = 0, cone_tile = 0, cone_tiles_x = 0;
   float lipschitz = 0.f;
   uint32_t total_steps_done = 0;
 };
@@ -1641,6 +1864,7 @@ RE_API re_status re_nsdf_destroy(re_nsdf* s) {
   cudaFree(s->loss_hist);
   cudaFree(s->counters);
   cudaFree(s->queue);
+  cudaFree(s->cone_t);
   cudaFree(s->err);
   delete s;
   return RE_OK;
@@ -1885,6 +2109,16 @@ re_status trace_check(re_nsdf* s, const re_sdf_params* field, const re_nsdf_trac
   if ((uint64_t)w * h > (1ull << 28)) return fail(RE_ERR_LIMIT, "%s: image > 2^28 pixels", fn);
   if (!(tp->flags & RE_NSDF_EXACT_ONLY) && !(tp->lipschitz > 0.f && tp->safety > 0.f))
     return fail(RE_ERR_INVALID_ARG, "%s: lipschitz and safety must be > 0", fn);
+  if (tp->cone_tile > 256 ||
+      (tp->cone_coarse && (tp->cone_tile == 0 || tp->cone_coarse > 1024 ||
+                           tp->cone_coarse <= tp->cone_tile || tp->cone_coarse % tp->cone_tile)))
+    return fail(RE_ERR_INVALID_ARG,
+                "%s: cone_tile <= 256; cone_coarse 0 or a multiple of cone_tile above it, <= 1024",
+                fn);
+  if (tp->normal_taps != 0 && tp->normal_taps != 4 && tp->normal_taps != 6)
+    return fail(RE_ERR_INVALID_ARG, "%s: normal_taps 0, 4 or 6", fn);
+  if (tp->cone_lanes > 8 || (tp->cone_lanes & (tp->cone_lanes - 1u)))
+    return fail(RE_ERR_INVALID_ARG, "%s: cone_lanes 0, 1, 2, 4 or 8", fn);
   return RE_OK;
 }
 }  // namespace
@@ -1897,8 +2131,22 @@ RE_API re_status re_nsdf_trace_network(re_nsdf* s, const re_sdf_params* field,
   if (st != RE_OK) return st;
   cudaStream_t cs = (cudaStream_t)stream;
   const bool exact_only = (tp->flags & RE_NSDF_EXACT_ONLY) != 0u;
+  const bool cone = !exact_only && tp->cone_tile > 0;
   size_t need = (size_t)w * h;
-  if (!exact_only && s->queue_cap < need) {
+  const uint32_t T = tp->cone_tile, C = tp->cone_coarse;
+  const uint32_t ctx = cone ? (w + T - 1) / T : 0, cty = cone ? (h + T - 1) / T : 0;
+  const uint32_t pcx = cone && C ? (w + C - 1) / C : 0, pcy = cone && C ? (h + C - 1) / C : 0;
+  const size_t cone_need = (size_t)ctx * cty + (size_t)pcx * pcy;
+  if (cone && s->cone_cap < cone_need) {
+    RE_CUDA(cudaStreamSynchronize(cs));
+    cudaFree(s->cone_t);
+    s->cone_t = nullptr;
+    s->cone_cap = 0;
+    RE_CUDA(cudaMalloc(&s->cone_t, cone_need * sizeof(float)));
+    s->cone_cap = cone_need;
+  }
+  s->cone_w = s->cone_h = s->cone_tile = s->cone_tiles_x = 0;
+  if (!exact_only && !cone && s->queue_cap < need) {
     RE_CUDA(cudaStreamSynchronize(cs));
     cudaFree(s->queue);
     s->queue = nullptr;
@@ -1923,6 +2171,48 @@ RE_API re_status re_nsdf_trace_network(re_nsdf* s, const re_sdf_params* field,
     md.bmin[k] = s->map.center[k] - half;
     md.bmax[k] = s->map.center[k] + half;
   }
+  if (cone) {
+    const uint32_t K = tp->cone_lanes ? tp->cone_lanes : 1u;
+    auto kc = K == 8u   ? re::nsdf::k_nsdf_cone<8>
+              : K == 4u ? re::nsdf::k_nsdf_cone<4>
+              : K == 2u ? re::nsdf::k_nsdf_cone<2>
+                        : re::nsdf::k_nsdf_cone<1>;
+    RE_CUDA(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)re::kTcSmemBytes));
+    float* fine = s->cone_t;
+    float* coarse = s->cone_t + (size_t)ctx * cty;
+    re::nsdf::ConeDev cd{};
+    if (C) {
+      // coarse level from the box entry (cursor counters[0])
+      cd.tile = C;
+      cd.tiles_x = pcx;
+      cd.tiles_y = pcy;
+      cd.parent = nullptr;
+      const int grid = std::min<int>(re::tc_grid(kc),
+                                     (int)((pcx * pcy * K + re::nsdf::kTcThreads - 1) /
+                                           re::nsdf::kTcThreads));
+      kc<<<grid, re::nsdf::kTcThreads, re::kTcSmemBytes, cs>>>(
+          s->map, s->pack, md, cd, re::cam_dev(*cam), w, h, s->counters, totals, coarse, s->err);
+      RE_CHECK_LAUNCH("re_nsdf_trace_network: coarse cone launch");
+    }
+    // fine level, from the coarse tiles' starts (cursor counters[3])
+    cd.tile = T;
+    cd.tiles_x = ctx;
+    cd.tiles_y = cty;
+    cd.parent = C ? coarse : nullptr;
+    cd.parent_tile = C;
+    cd.parent_tiles_x = pcx;
+    const int grid = std::min<int>(
+        re::tc_grid(kc), (int)((ctx * cty * K + re::nsdf::kTcThreads - 1) / re::nsdf::kTcThreads));
+    kc<<<grid, re::nsdf::kTcThreads, re::kTcSmemBytes, cs>>>(
+        s->map, s->pack, md, cd, re::cam_dev(*cam), w, h, s->counters + 3, totals, fine, s->err);
+    RE_CHECK_LAUNCH("re_nsdf_trace_network: cone launch");
+    s->cone_w = w;
+    s->cone_h = h;
+    s->cone_tile = T;
+    s->cone_tiles_x = ctx;
+    return RE_OK;
+  }
   auto k = re::nsdf::k_nsdf_march;
   RE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)re::kTcSmemBytes));
@@ -1939,7 +2229,10 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
   re_status st = re::trace_check(s, field, tp, cam, w, h, d_out, "re_nsdf_trace_exact");
   if (st != RE_OK) return st;
   const bool exact_only = (tp->flags & RE_NSDF_EXACT_ONLY) != 0u;
-  if (!exact_only && s->queue_cap < (size_t)w * h)
+  const bool cone = !exact_only && tp->cone_tile > 0;
+  if (cone && !(s->cone_w == w && s->cone_h == h && s->cone_tile == tp->cone_tile))
+    return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace_exact: no cone phase for this image");
+  if (!exact_only && !cone && s->queue_cap < (size_t)w * h)
     return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace_exact: no network phase for this image");
   cudaStream_t cs = (cudaStream_t)stream;
   unsigned long long* totals = reinterpret_cast<unsigned long long*>(s->counters + 4);
@@ -1960,9 +2253,13 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
   // density is positive above this height
   rd.ceiling =
       2.0f * std::fabs(field->amplitude) * (2.0f - std::ldexp(1.0f, 1 - (int)field->octaves)) + 1e-3f;
+  rd.normal_taps = tp->normal_taps == 4u ? 4u : 6u;
+  rd.tile_t = cone ? s->cone_t : nullptr;
+  rd.cone_tile = cone ? s->cone_tile : 1u;
+  rd.cone_tiles_x = cone ? s->cone_tiles_x : 0u;
   kr<<<per_sm * re::sm_count(), 256, re::kPermSmemBytes, cs>>>(
       re::perm_of(field->seed), re::field_of(*field), rd, re::cam_dev(*cam), w, h,
-      exact_only ? 1 : 0, s->queue, s->counters, totals, reinterpret_cast<float4*>(d_out));
+      exact_only || cone ? 1 : 0, s->queue, s->counters, totals, reinterpret_cast<float4*>(d_out));
   RE_CHECK_LAUNCH("re_nsdf_trace_exact: refine launch");
   return RE_OK;
 }

@@ -110,31 +110,98 @@ def _sdf_errors(out, tc, pix):
     return po.hit_errors(out, jpos, jhit, pix)
 
 
+def _normals_from_positions(out, cam, pix, taps):
+    """The exact phase's normal recomputed on the host in FP64 from the
+    returned hit positions: central differences (taps 6) or the tetrahedral
+    stencil (taps 4), delta = 0.002 t with t = |p - camera|."""
+    tc = rb.configs.TerrainConfig()
+    P = po.perm(tc.seed)
+    f = out.view(np.float32)[pix]
+    p = f[:, 0:3].astype(np.float64)
+    t = np.linalg.norm(p - np.array(cam.campos, np.float64), axis=1)
+    delta = (0.002 * t)[:, None]
+    if taps == 6:
+        n = np.zeros_like(p)
+        for k in range(3):
+            e = np.zeros(3)
+            e[k] = 1.0
+            n[:, k] = po.density_d(P, p + delta * e) - po.density_d(P, p - delta * e)
+    else:
+        n = np.zeros_like(p)
+        c = 0.5773
+        for e in ([c, -c, -c], [-c, -c, c], [-c, c, -c], [c, c, c]):
+            e = np.array(e)
+            n += e[None, :] * po.density_d(P, p + delta * e)[:, None]
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    got = f[:, 3:6].astype(np.float64)
+    return np.degrees(np.arccos(np.clip((n * got).sum(1), -1.0, 1.0)))
+
+
 def test_neural_trace_accuracy_and_exact_evaluations_saved(cuda):
     tc = rb.configs.TerrainConfig(width=480, height=270)
     ncfg = rb.configs.NeuralTerrainConfig(terrain=tc, num_points=1 << 21, train_steps=3000)
     m, tp, losses = ncfg.build()
+    assert tp.cone_tile > 0  # the cone tracer is the configured method
     with m:
         assert np.all(np.isfinite(losses)) and losses[-100:].mean() < losses[:10].mean()
         W, H = tc.width, tc.height
         field, cam = tc.params(), tc.camera()
-        net = m.trace(field, tp, cam, W, H).cpu().numpy()
-        st_net = m.trace_status()
-        assert st_net["error"] == 0
-        assert st_net["network_evals"] > 0
         ex = m.trace(field, rb.nsdf_trace_params(exact_only=True), cam, W, H).cpu().numpy()
         st_ex = m.trace_status()
         assert st_ex["network_evals"] == 0 and st_ex["handed_over"] == 0
-        # every pixel written with a valid status
-        for o in (net, ex):
-            assert set(np.unique(o[:, 7])) <= {0, 1, 2}
         pix = np.random.default_rng(5).choice(W * H, 4000, replace=False).astype(np.uint32)
-        err_n, mism_n, both_n = _sdf_errors(net, tc, pix)
         err_e, mism_e, both_e = _sdf_errors(ex, tc, pix)
-        # the target: median hit error <= 1e-3 scene units against the FP64
-        # root, few silhouette (hit / miss) disagreements
-        assert np.median(err_n) <= 1e-3 and np.median(err_e) <= 1e-3
-        assert mism_n <= 0.01 * len(pix) and mism_e <= 0.01 * len(pix)
-        assert (net[:, 7] != ex[:, 7]).mean() < 0.01
-        # what the network gains: it replaces exact-field march steps
-        assert st_net["exact_evals"] < 0.8 * st_ex["exact_evals"]
+        assert np.median(err_e) <= 1e-3 and mism_e <= 0.01 * len(pix)
+        exact_tracer = rb.sphere_trace(field, cam, W, H).cpu().numpy()
+        lip = tp.lipschitz
+        variants = {
+            "cone": tp,
+            "cone, one lane, tetrahedral normal": rb.nsdf_trace_params(
+                lip, ncfg.safety, ncfg.switch_dist, ncfg.min_step, ncfg.max_network_steps, 0,
+                ncfg.root_steps, 1.0, cone_tile=8, cone_lanes=1, normal_taps=4),
+            "cone over a coarse level": rb.nsdf_trace_params(
+                lip, ncfg.safety, ncfg.switch_dist, ncfg.min_step, ncfg.max_network_steps, 0,
+                ncfg.root_steps, ncfg.relax, cone_tile=8, cone_coarse=32, cone_lanes=4),
+            "per-ray march": ncfg.per_ray_params(lip),
+        }
+        for name, params in variants.items():
+            net = m.trace(field, params, cam, W, H).cpu().numpy()
+            st = m.trace_status()
+            assert st["error"] == 0, name
+            assert st["network_evals"] > 0, name
+            # every pixel written with a valid status
+            assert set(np.unique(net[:, 7])) <= {0, 1, 2}, name
+            err_n, mism_n, both_n = _sdf_errors(net, tc, pix)
+            # the target: median hit error <= 1e-3 scene units against the
+            # FP64 root, few silhouette (hit / miss) disagreements
+            assert np.median(err_n) <= 1e-3, (name, np.median(err_n))
+            assert mism_n <= 0.01 * len(pix), (name, mism_n)
+            assert (net[:, 7] != ex[:, 7]).mean() < 0.01, name
+            assert ((net[:, 7] == 1) != (exact_tracer[:, 7] == 1)).mean() < 0.01, name
+            # what the network gains: it replaces exact-field march steps
+            assert st["exact_evals"] < 0.8 * st_ex["exact_evals"], (name, st, st_ex)
+            # the normal is the stated stencil at the returned position
+            hits = pix[net[pix, 7] == 1]
+            ang = _normals_from_positions(net, cam, hits[:400], params.normal_taps or 6)
+            assert np.quantile(ang, 0.99) < 0.05, (name, np.quantile(ang, 0.99))
+
+
+def test_trace_parameter_checks(cuda):
+    tc = rb.configs.TerrainConfig(width=64, height=36)
+    with _model() as m:
+        field, cam = tc.params(), tc.camera()
+        bad = [dict(cone_tile=8, cone_coarse=12), dict(cone_tile=8, cone_coarse=8),
+               dict(cone_tile=0, cone_coarse=32), dict(cone_tile=300),
+               dict(cone_tile=8, cone_lanes=3), dict(cone_tile=8, cone_lanes=16),
+               dict(normal_taps=5)]
+        for kw in bad:
+            with pytest.raises(rb.RayEngineError):
+                m.trace(field, rb.nsdf_trace_params(**kw), cam, tc.width, tc.height)
+        # the exact phase needs the network phase of the same image and mode
+        tp = rb.nsdf_trace_params(cone_tile=8, cone_lanes=2)
+        out = m.trace(field, tp, cam, tc.width, tc.height)
+        with pytest.raises(rb.RayEngineError):
+            m.trace(field, rb.nsdf_trace_params(cone_tile=4), cam, tc.width, tc.height, out,
+                    phase="exact")
+        with pytest.raises(rb.RayEngineError):
+            m.trace(field, tp, cam, tc.width + 8, tc.height, phase="exact")

@@ -829,7 +829,7 @@ class NeuralTerrainSDF:
                                  "min_step": n.min_step, "max_network_steps": n.max_network_steps,
                                  "root_steps": n.root_steps, "cone_tile": n.cone_tile,
                                  "cone_lanes": n.cone_lanes, "relax": n.relax,
-                                 "normal_taps": n.normal_taps},
+                                 "root_tol": n.root_tol, "normal_taps": n.normal_taps},
                 "per_ray": {"network_evals": round(st["network_evals"] / R, 3),
                             "network_rows": round(st["network_rows"] / R, 3),
                             "exact_evals": round(st["exact_evals"] / R, 3),

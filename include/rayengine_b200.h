@@ -411,6 +411,8 @@ typedef struct re_nsdf_trace_params {
   uint32_t normal_taps; /* 0 or 6: central differences; 4: tetrahedral    */
   uint32_t cone_lanes;  /* 0 or 1, 2, 4, 8: lanes per cone; above 1 they   */
                         /* evaluate successive guessed steps in one pass   */
+  float root_tol;       /* > 0: the root search ends when its next secant  */
+                        /* point moves less than this (scene units)        */
 } re_nsdf_trace_params;
 
 RE_API uint32_t re_nsdf_num_params(void);

@@ -165,6 +165,7 @@ class re_nsdf_trace_params(ctypes.Structure):
         ("cone_coarse", ctypes.c_uint32),
         ("normal_taps", ctypes.c_uint32),
         ("cone_lanes", ctypes.c_uint32),
+        ("root_tol", ctypes.c_float),
     ]
 
 

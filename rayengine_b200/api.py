@@ -464,7 +464,8 @@ def fmath(fn: int, x, y=None, out=None, stream=None):
 # ------------------------------------------------------ neural SDF surrogate
 def nsdf_trace_params(lipschitz=1.0, safety=0.9, switch_dist=0.05, min_step=1e-3,
                       max_network_steps=256, max_exact_steps=0, root_steps=4, relax=1.0,
-                      exact_only=False, cone_tile=0, cone_coarse=0, normal_taps=6, cone_lanes=1):
+                      exact_only=False, cone_tile=0, cone_coarse=0, normal_taps=6, cone_lanes=1,
+                      root_tol=0.0):
     """Neural march / exact phase settings (re_nsdf_trace_params).
 
     exact_only skips the network: every ray runs the exact phase from the
@@ -473,14 +474,15 @@ def nsdf_trace_params(lipschitz=1.0, safety=0.9, switch_dist=0.05, min_step=1e-3
     first level over cone_coarse tiles when that is set) and every pixel's
     exact phase starts where its tile stopped; cone_lanes lanes evaluate
     successive guessed steps of a cone in one pass.  normal_taps: 6 central
-    differences, 4 the tetrahedral normal."""
+    differences, 4 the tetrahedral normal.  root_tol > 0 ends the root
+    search once its secant point moves less than that."""
     p = _lib.re_nsdf_trace_params()
     p.lipschitz, p.safety, p.switch_dist, p.min_step = lipschitz, safety, switch_dist, min_step
     p.max_network_steps, p.max_exact_steps = max_network_steps, max_exact_steps
     p.root_steps, p.relax = root_steps, relax
     p.flags = _lib.NSDF_EXACT_ONLY if exact_only else 0
     p.cone_tile, p.cone_coarse, p.normal_taps = cone_tile, cone_coarse, normal_taps
-    p.cone_lanes = cone_lanes
+    p.cone_lanes, p.root_tol = cone_lanes, root_tol
     return p
 
 

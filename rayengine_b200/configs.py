@@ -176,7 +176,10 @@ class NeuralTerrainConfig:
     # Exact phase from the cone's stop: the exact tracer's steps allowed to
     # grow 1.5x along the secant of the last two samples (median hit error
     # 8e-5, ~850 of 2.07M pixels whose hit/miss differs from the exact
-    # tracer; relax 1.0: 27 pixels, 3.98 ms with 8x8 cones of one lane).
+    # tracer; relax 1.0: 27 pixels, 3.98 ms with 8x8 cones of one lane;
+    # relax 2.0: 2.94 ms, 2,100 pixels, median error 4e-4); the root search
+    # ends when its secant point moves less than 1e-4 (3.23 -> 3.17 ms, same
+    # median error).
     safety: float = 1.2
     switch_dist: float = 0.3
     min_step: float = 0.05
@@ -185,6 +188,7 @@ class NeuralTerrainConfig:
     cone_tile: int = 16
     cone_lanes: int = 8
     relax: float = 1.5
+    root_tol: float = 1e-4
     normal_taps: int = 6
     # the per-ray network march (cone_tile 0), measured on B200: safety 1.2
     # with the hand-over at 0.6 gives 7.49 ms against 8.97 ms at (0.9,
@@ -220,7 +224,7 @@ class NeuralTerrainConfig:
         return api.nsdf_trace_params(lipschitz, self.safety, self.switch_dist, self.min_step,
                                      self.max_network_steps, 0, self.root_steps, self.relax,
                                      cone_tile=self.cone_tile, cone_lanes=self.cone_lanes,
-                                     normal_taps=self.normal_taps)
+                                     normal_taps=self.normal_taps, root_tol=self.root_tol)
 
     def per_ray_params(self, lipschitz):
         """The per-ray network march with its hand-over queue, the exact

@@ -968,6 +968,7 @@ struct RefineDev {
   uint32_t max_steps;   // exact evaluations per ray (march + bracket + root)
   uint32_t root_steps;  // regula-falsi steps on a bracketed crossing
   float relax;          // an exact step may grow to relax x (step_factor * d) along a secant
+  float root_tol;       // the root search ends when the secant point moves less than this
   float ceiling;        // no surface above this height (bound of the field)
   uint32_t normal_taps;  // 6: central differences; 4: tetrahedral
   // cone starts (direct mode): pixel (x, y) starts at tile_t[(y / cone_tile)
@@ -1301,7 +1302,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_cone(InputMap m,
 //          [t_lo, t], else march again from t = 0 (the network skipped
 //          over the surface).
 //   root   Illinois regula falsi on the bracket, root_steps evaluations or
-//          until |d| < 1e-6.
+//          until |d| < 1e-6, or until the next secant point moves less than
+//          root_tol (that point is the hit, unevaluated; a bracket already
+//          narrower than root_tol gives its secant root at once).
 //   normal the exact tracer's central differences (delta = 0.002 t), or,
 //          with normal_taps 4, the reference's tetrahedral normal
 //          (compute_sdf_normal_tet) at the same radius: sum of e_k d(p +
@@ -1463,7 +1466,10 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
           if (side > 0) vb *= 0.5f;
           side = 1;
         }
-        t = b - vb * (b - a) / (vb - va);
+        const float tn = b - vb * (b - a) / (vb - va);
+        // the next secant point moves less than root_tol: take it unevaluated
+        if (fabsf(tn - t) < rd.root_tol) hit_here = true;
+        t = tn;
       }
     } else if (rd.normal_taps == 4u) {
       V3 e = tet_dir(tap);
@@ -1489,6 +1495,8 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       side = 0;
       iters = 0;
       t = b - vb * (b - a) / (vb - va);
+      // a bracket narrower than root_tol: its secant root is the hit
+      if (b - a < rd.root_tol) hit_here = true;
     }
     if (hit_here) {
       p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
@@ -2248,6 +2256,7 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
   rd.max_steps = tp->max_exact_steps ? tp->max_exact_steps : field->max_steps;
   rd.root_steps = tp->root_steps ? tp->root_steps : 4;
   rd.relax = tp->relax;
+  rd.root_tol = tp->root_tol > 0.f ? tp->root_tol : 0.f;
   // |Perlin| <= 2 (each corner term |g . r| <= |r_x| + |r_y| <= 2 and the
   // interpolation is convex), so fBm <= 2 (2 - 2^(1 - octaves)) and the
   // density is positive above this height

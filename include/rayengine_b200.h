@@ -109,7 +109,10 @@ typedef struct re_tuning {
   uint32_t ray_lanes;        /* lanes per primary ray in re_trace_primary: 1 (default; 0
                                 reads as 1), 2, 4 or 8.  Above 1 the lanes of a ray split
                                 each leaf's triangle tests (same hits); it shortens the
-                                longest walks of frames too small to fill the GPU */
+                                longest walks of frames too small to fill the GPU.  32:
+                                one ray per lane, and the warp tests the triangles of all
+                                its lanes' leaves together (finished lanes help; same
+                                hits) */
 } re_tuning;
 
 typedef struct re_scene_stats {

@@ -276,6 +276,135 @@ __device__ __forceinline__ void trav_step(Trav& s, const KdDev& kd, const uint2*
   }
 }
 
+// Warp-cooperative closest-hit step: every lane of the warp calls it, live
+// or not.  Each live lane descends to its next leaf as in trav_step; then the
+// warp tests the (ray, triangle) pairs of all its live lanes' leaves
+// together, 32 at a time, so a lane whose ray has finished helps the others
+// and a leaf's tests no longer run one after another on its own lane.  Pair
+// p belongs to the lane whose exclusive prefix of test counts is the last
+// one <= p.  Each owner's best is reduced in shared memory as the 64-bit key
+// (t bits << 32 | id): t > 0, so the key order is the (t, id) lexicographic
+// order, and seeding the owner's slot with (best t, best id) — or (best t,
+// 0) before any hit, so that an equal t is never accepted then — makes the
+// minimum exactly the sequential acceptance rule's result (strictly
+// smaller t, or equal t and smaller id once a hit exists; a leaf holds each
+// triangle once).  The tester whose key is the minimum writes u, v and the
+// triangle slot for its owner.  key and rec: this warp's 32 slots.
+template <int MODE>
+__device__ __forceinline__ void trav_step_warp(Trav& s, const KdDev& kd, const uint2* snodes,
+                                               unsigned long long* key, float4* rec) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool live = s.live;
+  const V3 o = s.o, d = s.d, inv = s.inv;
+  uint32_t node = s.node, first = 0, count = 0;
+  const float kInf = __int_as_float(0x7f800000);
+  float texit = kInf;
+  int face = -1;
+  int32_t rope = -1;
+  if (live) {
+    const float t_entry = s.t_entry;
+    uint2 nd = load_node(kd, snodes, node);
+    while ((nd.y & 3u) != 3u) {
+      uint32_t k = nd.y & 3u;
+      float split = __uint_as_float(nd.x);
+      float ok = comp(o, k), dk = comp(d, k), ik = comp(inv, k);
+      float ts = (split - ok) * ik;
+      bool left = dk > 0.0f ? (t_entry < ts) : (dk < 0.0f ? (t_entry >= ts) : (ok < split));
+      node = (nd.y >> 2) + (left ? 0u : 1u);
+      nd = load_node(kd, snodes, node);
+    }
+    first = nd.x & 0x7FFFFFFFu;
+    const float4* L = kd.leaves + 4 * (size_t)(nd.y >> 2);
+    float4 A = __ldg(L), B = __ldg(L + 1);
+    count = __float_as_uint(B.w);
+    float tx = d.x != 0.0f ? ((d.x > 0.0f ? A.w : A.x) - o.x) * inv.x : kInf;
+    float ty = d.y != 0.0f ? ((d.y > 0.0f ? B.x : A.y) - o.y) * inv.y : kInf;
+    float tz = d.z != 0.0f ? ((d.z > 0.0f ? B.y : A.z) - o.z) * inv.z : kInf;
+    if (tx < texit) { texit = tx; face = d.x > 0.0f ? 1 : 0; }
+    if (ty < texit) { texit = ty; face = d.y > 0.0f ? 3 : 2; }
+    if (tz < texit) { texit = tz; face = d.z > 0.0f ? 5 : 4; }
+    rope = face >= 0 ? __ldg(reinterpret_cast<const int32_t*>(L + 2) + face) : -1;
+  }
+  uint32_t incl = count;
+#pragma unroll
+  for (uint32_t off = 1; off < 32; off <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+    if (lane >= off) incl += y;
+  }
+  const uint32_t excl = incl - count, total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (total > 0u) {
+    unsigned long long seed = 0ull;
+    if (live) {
+      seed = ((unsigned long long)__float_as_uint(s.best_t) << 32) |
+             (uint32_t)(s.best_id >= 0 ? s.best_id : 0);
+      key[lane] = seed;
+    }
+    __syncwarp();
+    for (uint32_t base = 0; base < total; base += 32u) {
+      const uint32_t p = base + lane;
+      uint32_t own = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t cand = own + step;
+        if (__shfl_sync(0xFFFFFFFFu, excl, cand) <= p) own = cand;
+      }
+      const uint32_t oex = __shfl_sync(0xFFFFFFFFu, excl, own);
+      const uint32_t ofirst = __shfl_sync(0xFFFFFFFFu, first, own);
+      const V3 ro = {__shfl_sync(0xFFFFFFFFu, o.x, own), __shfl_sync(0xFFFFFFFFu, o.y, own),
+                     __shfl_sync(0xFFFFFFFFu, o.z, own)};
+      const V3 rd = {__shfl_sync(0xFFFFFFFFu, d.x, own), __shfl_sync(0xFFFFFFFFu, d.y, own),
+                     __shfl_sync(0xFFFFFFFFu, d.z, own)};
+      bool hit = false;
+      unsigned long long k = 0ull;
+      float u = 0.f, v = 0.f;
+      uint32_t ref = 0;
+      if (p < total) {
+        ref = ofirst + (p - oex);
+        const float4* T = kd.tris + 3 * (size_t)ref;
+        float4 T0 = __ldg(T), T1 = __ldg(T + 1), T2 = __ldg(T + 2);
+        float t;
+        if (ray_tri<MODE>(ro, rd, T0, T1, T2, t, u, v)) {
+          k = ((unsigned long long)__float_as_uint(t) << 32) | (uint32_t)__float_as_int(T0.w);
+          hit = true;
+          atomicMin(&key[own], k);
+        }
+      }
+      __syncwarp();
+      if (hit && key[own] == k) rec[own] = make_float4(u, v, __uint_as_float(ref), 0.f);
+      __syncwarp();
+    }
+    if (live) {
+      const unsigned long long k = key[lane];
+      if (k != seed) {
+        const float4 r = rec[lane];
+        s.best_t = __uint_as_float((uint32_t)(k >> 32));
+        s.best_id = (int32_t)(uint32_t)k;
+        s.best_u = r.x;
+        s.best_v = r.y;
+        s.best_ref = __float_as_uint(r.z);
+        s.best_leaf = node;
+      }
+    }
+    __syncwarp();
+  }
+  if (!live) return;
+  if (face < 0) {
+    s.live = false;
+    return;
+  }
+  s.t_entry = fmaxf(s.t_entry, texit);
+  if (!(s.t_entry < s.best_t) || rope < 0) {
+    s.live = false;
+    return;
+  }
+  s.node = (uint32_t)rope;
+  if (++s.visits >= kd.max_visits) {
+    s.live = false;
+    s.visits = kTruncated;
+    if (kd.trunc) atomicAdd(kd.trunc, 1u);
+  }
+}
+
 // The walk ended at the leaf-visit cap (its hit, if any, is the closest one
 // found among the leaves it reached).
 __device__ __forceinline__ bool trav_truncated(const Trav& s) { return s.visits == kTruncated; }

@@ -159,6 +159,45 @@ __global__ void __launch_bounds__(256, 6) k_primary_lanes(KdDev kd, CamDev cam, 
   }
 }
 
+// Primary rays, persistent warps over 8x4 pixel tiles, the warp testing the
+// triangles of all its lanes' leaves together (ray_lanes 32,
+// trav_step_warp): lanes whose rays have finished help the others, so the
+// longest walks of frames too small to fill the GPU get a shorter chain of
+// triangle tests.
+template <int MODE>
+__global__ void __launch_bounds__(256, 4) k_primary_warp(KdDev kd, CamDev cam, uint32_t w,
+                                                      uint32_t h, re_hit* __restrict__ out,
+                                                      uint4* __restrict__,
+                                                      uint32_t* __restrict__ tile_counter,
+                                                      uint32_t) {
+  extern __shared__ uint2 snodes[];
+  __shared__ unsigned long long wkey[8][32];
+  __shared__ float4 wrec[8][32];
+  stage_nodes(kd, snodes);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t tiles_x = (w + 7) / 8, tiles = tiles_x * ((h + 3) / 4);
+  for (;;) {
+    uint32_t tile = warp_fetch(tile_counter);
+    if (tile >= tiles) break;
+    uint32_t x = (tile % tiles_x) * 8 + (lane & 7u);
+    uint32_t y = (tile / tiles_x) * 4 + (lane >> 3);
+    const bool valid = x < w && y < h;
+    Trav s;
+    s.live = false;
+    if (valid) {
+      V3 o, d;
+      generate_ray(cam, w, h, x, y, o, d);
+      trav_init(s, kd, o, d, __int_as_float(0x7f800000), 0u);
+    }
+    while (__any_sync(0xFFFFFFFFu, s.live)) trav_step_warp<MODE>(s, kd, snodes, wkey[warp], wrec[warp]);
+    if (valid) {
+      HitState hs;
+      trav_result(s, hs);
+      store_hit(out, (size_t)y * w + x, hs);
+    }
+  }
+}
+
 // Primary rays with lane refill (ray_refill_min < 32).  Work index i is lane
 // i % 32 of 8x4 pixel tile i / 32, so a warp's claims stay in one screen
 // region.
@@ -605,9 +644,10 @@ re_status launch_primary(re_scene* s, const re_camera& cam, uint32_t w, uint32_t
   CamDev cd = cam_view(cam);
   size_t smem = kd.stage * sizeof(uint2);
   uint32_t refill = s->tune.ray_refill_min, lanes = COUNT ? 1u : s->tune.ray_lanes;
-  auto k = lanes == 2u   ? k_primary_lanes<MODE, 2>
-           : lanes == 4u ? k_primary_lanes<MODE, 4>
-           : lanes == 8u ? k_primary_lanes<MODE, 8>
+  auto k = lanes == 2u    ? k_primary_lanes<MODE, 2>
+           : lanes == 4u  ? k_primary_lanes<MODE, 4>
+           : lanes == 8u  ? k_primary_lanes<MODE, 8>
+           : lanes == 32u ? k_primary_warp<MODE>
            : refill >= 32u ? k_primary_tiles<MODE, COUNT>
                            : k_primary<MODE, COUNT>;
   RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
@@ -1012,8 +1052,9 @@ RE_API re_status re_scene_set_tuning(re_scene* s, const re_tuning* t) {
                     "re_scene_set_tuning: refill_min and ray_refill_min must be in [1, 32]");
   if (t->queue_kind_major > 2)
     return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: queue_kind_major must be 0, 1 or 2");
-  if (t->ray_lanes > 8 || (t->ray_lanes & (t->ray_lanes - 1u)))
-    return re::fail(RE_ERR_INVALID_ARG, "re_scene_set_tuning: ray_lanes must be 0, 1, 2, 4 or 8");
+  if ((t->ray_lanes > 8 && t->ray_lanes != 32) || (t->ray_lanes & (t->ray_lanes - 1u)))
+    return re::fail(RE_ERR_INVALID_ARG,
+                    "re_scene_set_tuning: ray_lanes must be 0, 1, 2, 4, 8 or 32");
   s->tune = *t;
   if (s->tune.ray_lanes == 0) s->tune.ray_lanes = 1;
   s->tune.stage_nodes = std::min(std::min(t->stage_nodes, s->host.bfs_nodes), re::kMaxStage);
@@ -1125,11 +1166,11 @@ RE_API re_status re_autotune_primary(re_scene* s, const re_camera* cam, uint32_t
   uint32_t bfs = std::min(s->host.bfs_nodes, re::kMaxStage);
   const uint32_t stages[3] = {0u, std::min(1024u, bfs), std::min(4096u, bfs)};
   // {ray_lanes, ray_refill_min}
-  const uint32_t forms[7][2] = {{1u, 32u}, {1u, 16u}, {1u, 8u}, {1u, 4u},
-                                {2u, 32u}, {4u, 32u}, {8u, 32u}};
+  const uint32_t forms[8][2] = {{1u, 32u}, {1u, 16u}, {1u, 8u}, {1u, 4u},
+                                {2u, 32u}, {4u, 32u}, {8u, 32u}, {32u, 32u}};
   for (int si = 0; si < 3 && ce == cudaSuccess && rs == RE_OK; ++si) {
     if (si > 0 && stages[si] == stages[si - 1]) continue;
-    for (int fi = 0; fi < 7 && rs == RE_OK; ++fi) {
+    for (int fi = 0; fi < 8 && rs == RE_OK; ++fi) {
       re_tuning t = keep;
       t.stage_nodes = stages[si];
       t.ray_lanes = forms[fi][0];

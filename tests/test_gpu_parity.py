@@ -180,9 +180,10 @@ def test_ray_refill_threshold_changes_only_speed(cuda):
 @pytest.mark.parametrize("leaf,mode", [(8, 0), (8, 1), (32, 0)])
 def test_lanes_per_ray_same_hits(cuda, leaf, mode):
     """2, 4 or 8 lanes per primary ray split each leaf's triangle tests and
-    keep the smallest (t, id): every hit (id, t, u, v) equals the oracle's
-    one-lane walk, on an image whose sides are no multiple of the tiles, with
-    leaves holding more references than lanes."""
+    keep the smallest (t, id), and with 32 the warp tests all its lanes'
+    leaves together: every hit (id, t, u, v) equals the oracle's one-lane
+    walk, on an image whose sides are no multiple of the tiles, with leaves
+    holding more references than lanes."""
     cfg = rb.configs.SoupConfig(num_tris=16384, width=203, height=119)
     packed = cfg.packed()
     cam = cfg.camera()
@@ -194,7 +195,7 @@ def test_lanes_per_ray_same_hits(cuda, leaf, mode):
         assert (ref[:, 0] >= 0).mean() > 0.2
         t = sc.tuning()
         assert t["ray_lanes"] == 1
-        for lanes in (2, 4, 8, 1):
+        for lanes in (2, 4, 8, 32, 1):
             for stage in (0, 1024):
                 sc.set_tuning(stage, t["queue_kind_major"], t["refill_min"], 32, lanes)
                 got = _hits(sc.trace_primary(cam, W, H, mode))
@@ -206,7 +207,7 @@ def test_lanes_per_ray_same_hits(cuda, leaf, mode):
         assert np.array_equal(cnt, rc.view(np.uint32).reshape(-1, 4).astype(np.int32))
 
 
-@pytest.mark.parametrize("lanes", [2, 4])
+@pytest.mark.parametrize("lanes", [2, 4, 32])
 def test_lanes_per_ray_visit_cap(cuda, lanes):
     """With several lanes per ray a walk stopped at the leaf-visit cap is
     counted once and keeps the oracle's hit."""
@@ -230,7 +231,8 @@ def test_autotune_primary_considers_lanes(cuda):
         st, kd = _kd(sc)
         cam = cfg.camera()
         best = sc.autotune_primary(cam, 128, 128)
-        assert best["ray_lanes"] in (1, 2, 4, 8) and sc.tuning()["ray_lanes"] == best["ray_lanes"]
+        assert best["ray_lanes"] in (1, 2, 4, 8, 32)
+        assert sc.tuning()["ray_lanes"] == best["ray_lanes"]
         ref = po.primary_kd(kd, cam, 128, 128).view(np.int32).reshape(-1, 4)
         assert np.array_equal(_hits(sc.trace_primary(cam, 128, 128)), ref)
 

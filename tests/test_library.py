@@ -72,17 +72,18 @@ def test_host_only_scene_refuses_to_trace():
 
 
 def test_tuning_validation():
-    """ray_lanes: 1 by default, 0 reads as 1, powers of two up to 8 only."""
+    """ray_lanes: 1 by default, 0 reads as 1, powers of two up to 8, or 32
+    (the warp-cooperative walk)."""
     packed = rb.configs.SoupConfig(num_tris=64).packed()
     with rb.KDScene.build_host(packed) as sc:
         t = sc.tuning()
         assert t["ray_lanes"] == 1 and t["ray_refill_min"] == 32
-        for lanes in (2, 4, 8, 1):
+        for lanes in (2, 4, 8, 32, 1):
             sc.set_tuning(t["stage_nodes"], 0, 8, 32, lanes)
             assert sc.tuning()["ray_lanes"] == lanes
         sc.set_tuning(t["stage_nodes"], 0, 8, 32, 0)
         assert sc.tuning()["ray_lanes"] == 1
-        for bad in (3, 6, 16):
+        for bad in (3, 6, 16, 64):
             with pytest.raises(rb.RayEngineError) as e:
                 sc.set_tuning(t["stage_nodes"], 0, 8, 32, bad)
             assert e.value.status == 1

@@ -483,7 +483,9 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
                                      const re_nsdf_trace_params* tp,
                                      const re_camera* cam, uint32_t w, uint32_t h,
                                      re_sdf_hit* d_out, void* stream);
-/* Of the last trace: rays handed to the exact phase, the device error flag
+/* Of the last trace: rays handed to the exact phase through the queue of
+ * the per-ray network march (0 with cone_tile > 0, where every pixel runs
+ * the exact phase from its tile's stop), the device error flag
  * (1 = a tensor-core wait reached its bound) and, when evals is not NULL,
  * four totals: network evaluations of rays, exact-field evaluations of the
  * march / bracket / root steps, exact normal taps, network rows computed

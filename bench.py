@@ -1054,13 +1054,15 @@ def _cosine_dirs(n, rng, k):
 
 
 def reference_workload(name):
-    """(workload description, built-by note, kind, step(npix) -> rays traced)
-    for the reference's own CPU path.
+    """(workload description, built-by note, kind, step(npix) -> rays traced,
+    as-shipped variant or None) for the reference's own CPU path.
 
-    Meshes: the reference's RKDTreeCPU and its CPU ray query
-    singleRayStacklessIntersect, compiled from its sources (oracle/_ref),
-    over the same seeded scene (generated by the CPU oracle's generators);
-    as shipped the tree is one leaf, so every query tests every triangle.
+    Meshes: the reference's CPU ray query singleRayStacklessIntersect,
+    compiled from its sources (oracle/_ref), over the same seeded scene
+    (generated by the CPU oracle's generators) and an SAH tree of the
+    configured parameters held as the reference's KDNodeCPU objects; as
+    shipped the reference's tree is one leaf (every query tests every
+    triangle), timed beside it.
     SDF and batch workloads: the reference's device march cannot be compiled
     for the host (texture hash, CUDA 10 texture references), so the arm
     times the oracle's restatement of it.  Nothing of this repository's
@@ -1082,7 +1084,7 @@ def reference_workload(name):
             return int(nr.sum())
         return ("batched path tracing of the 32-scene batch (depth 4, 1 spp), seeded-random "
                 "pixels", "oracle restatement: single-leaf build (brute-force Moller-Trumbore) "
-                "and the exact SDF march", "port", step)
+                "and the exact SDF march", "port", step, None)
     if name == "sdf_frame":
         fcfg = C.SdfFrameConfig()
         cfg = fcfg.terrain
@@ -1098,7 +1100,7 @@ def reference_workload(name):
             return npix + int((ev > 0).sum())
         return ("shaded exact-SDF terrain frame, 1920x1080 (march, soft shadow, sky, RGBA8)",
                 "oracle restatement of render_sphere_trace (renderer.cu:143-285; the "
-                "reference's device code does not compile for the host)", "port", step)
+                "reference's device code does not compile for the host)", "port", step, None)
     if name in ("terrain_sdf", "nsdf_terrain"):
         cfg = C.TerrainConfig()
         W, H = cfg.width, cfg.height
@@ -1110,7 +1112,7 @@ def reference_workload(name):
             return npix
         return ("exact-SDF sphere tracing of d(p)=p.y-3fBm(0.25p), 8 octaves, 1920x1080",
                 "oracle restatement of the exact-SDF march (sphere_tracing.cuh:183-216; the "
-                "reference's device code does not compile for the host)", "port", step)
+                "reference's device code does not compile for the host)", "port", step, None)
     if name.startswith("heightfield_ao"):
         cfg = C.HeightfieldConfig()
         verts, faces = po.heightfield(po.perm(cfg.seed), cfg.cells, cfg.lo, cfg.hi, cfg.octaves,
@@ -1125,40 +1127,63 @@ def reference_workload(name):
         desc = f"triangle soup {cfg.num_tris} tris; {cfg.width}x{cfg.height} primary rays"
     if po.ref_lib() is None:
         raise FileNotFoundError("oracle/_ref/libre_ref.so (the reference's compiled host code)")
-    tree = po.RefTree(verts, faces)
+    # The configured tree (SAH, depth <= 24, leaves of <= 8) cannot come from
+    # the reference's builder (MAX_DEPTH = 1, its SAH code commented out), so
+    # the checker's binned-SAH builder makes it and the reference's query
+    # runs over it as the reference's own KDNodeCPU objects.  The reference
+    # as shipped (one leaf: every query tests every triangle) is timed
+    # beside it on a small sample.
+    bonus = 0.15 if not name.startswith("heightfield_ao") else 0.1
+    t0 = time.perf_counter()
+    kdb = po.kdb_build(verts, faces, CONFIGURED_TREE["max_depth"], CONFIGURED_TREE["leaf_size"],
+                       2.0, 1.0, bonus)
+    kdb_s = time.perf_counter() - t0
+    sah_tree = po.RefTree.from_kd(verts, faces, kdb)
+    leaf_tree = po.RefTree(verts, faces)
     cam = cfg.camera()
     W, H = cfg.width, cfg.height
-    built_by = ("the reference's RKDTreeCPU (one leaf as shipped, KDTree.cpp:12,347) and its CPU "
-                "query RKDTreeCPU::singleRayStacklessIntersect (KDTree.cpp:993-1066), compiled "
-                "from its sources, OpenMP schedule(dynamic) over rays (RayTracer.cpp:154)")
+    built_by = ("the reference's CPU query RKDTreeCPU::singleRayStacklessIntersect "
+                "(KDTree.cpp:993-1066: box test, leaf triangles, both children), compiled from "
+                "its sources, OpenMP schedule(dynamic) over rays (RayTracer.cpp:154), over an SAH "
+                f"kd-tree of the configured parameters (depth <= {CONFIGURED_TREE['max_depth']}, "
+                f"leaves of <= {CONFIGURED_TREE['leaf_size']}, empty bonus {bonus}; "
+                f"{len(kdb.nodes)} nodes, {len(kdb.index)} references, built in {kdb_s:.1f} s by "
+                "the checker's builder and held as the reference's own KDNodeCPU objects: the "
+                "reference's builder ships with MAX_DEPTH = 1)")
 
-    def primary(npix):
-        o, d = po.camera_rays(cam, W, H, rng.choice(W * H, npix, replace=False))
-        t, nrm, _ = tree.trace(o, d)
-        return o, d, t, nrm
+    def make_step(tree):
+        def primary(npix):
+            o, d = po.camera_rays(cam, W, H, rng.choice(W * H, npix, replace=False))
+            t, nrm, _ = tree.trace(o, d)
+            return o, d, t, nrm
 
-    if name.startswith("heightfield_ao"):
-        light = np.array(api.unit(cfg.light_dir), np.float64)
+        if name.startswith("heightfield_ao"):
+            light = np.array(api.unit(cfg.light_dir), np.float64)
 
-        def step(npix):
-            o, d, t, nrm = primary(npix)
-            hit = t < 1e19
-            if not hit.any():
+            def step(npix):
+                o, d, t, nrm = primary(npix)
+                hit = t < 1e19
+                if not hit.any():
+                    return npix
+                n = nrm[hit].astype(np.float64)
+                n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+                flip = np.einsum("ij,ij->i", n, d[hit]) > 0.0
+                n[flip] = -n[flip]
+                p = o[hit] + t[hit, None].astype(np.float64) * d[hit] + cfg.bias * n
+                dirs = np.concatenate([np.broadcast_to(light, (n.shape[0], 1, 3)),
+                                       _cosine_dirs(n, rng, 4)], 1).reshape(-1, 3)
+                tree.trace(np.repeat(p, 5, axis=0), dirs)
+                return npix + 5 * n.shape[0]
+        else:
+            def step(npix):
+                primary(npix)
                 return npix
-            n = nrm[hit].astype(np.float64)
-            n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
-            flip = np.einsum("ij,ij->i", n, d[hit]) > 0.0
-            n[flip] = -n[flip]
-            p = o[hit] + t[hit, None].astype(np.float64) * d[hit] + cfg.bias * n
-            dirs = np.concatenate([np.broadcast_to(light, (n.shape[0], 1, 3)),
-                                   _cosine_dirs(n, rng, 4)], 1).reshape(-1, 3)
-            tree.trace(np.repeat(p, 5, axis=0), dirs)
-            return npix + 5 * n.shape[0]
-    else:
-        def step(npix):
-            primary(npix)
-            return npix
-    return desc, built_by, "reference", step
+        return step
+
+    as_shipped = {"step": make_step(leaf_tree),
+                  "what": "the reference as shipped: its RKDTreeCPU (one leaf, KDTree.cpp:12,347) "
+                          "and the same query, i.e. every triangle per ray"}
+    return desc, built_by, "reference", make_step(sah_tree), as_shipped
 
 
 TREE_WORKLOADS = ("heightfield_ao", "soup", "soup1m")
@@ -1184,7 +1209,7 @@ def run_reference(args):
         return 0
     from oracle import pyoracle as po
 
-    desc, built_by, kind, step = reference_workload(args.config)
+    desc, built_by, kind, step, shipped = reference_workload(args.config)
     # size one step to about a second of work on all host cores, less when
     # many steps are asked for, so that the whole run stays within minutes
     target_s = min(1.0, 90.0 / max(1, args.steps + args.warmup))
@@ -1202,6 +1227,17 @@ def run_reference(args):
         rays += step(npix)
     dt = time.perf_counter() - t0
     value = rays / dt / 1e6
+    extra = {}
+    if shipped is not None:
+        # about a second of the as-shipped query on a small sample
+        n2, r2, t2 = 4, 0, 0.0
+        while t2 < 1.0 and n2 <= 4096:
+            ta = time.perf_counter()
+            r2 += shipped["step"](n2)
+            t2 += time.perf_counter() - ta
+            n2 *= 2
+        extra["as_shipped"] = {"value": round(r2 / t2 / 1e6, 6), "unit": "Mrays/s",
+                               "what": shipped["what"]}
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1215,6 +1251,7 @@ def run_reference(args):
         "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     return 0
 

@@ -189,6 +189,29 @@ void o_trace_instances_pixel(const float* const* tris, const int32_t* ntris, con
                              int32_t* inst);
 void o_voxel_brush(float* v, const int dim[3], const float spacing[3], const float origin[3],
                    uint32_t type, const float c[3], const float e[3], float mat, float k);
+/* --- SAH kd-tree for the reference arm (oracle_kdbuild.c) -------------- */
+/* Pre-order nodes: axis 0..2 (inner: children left/right, split plane) or
+ * 3 (leaf: triangles index[first .. first + count)). */
+typedef struct {
+  int32_t axis;
+  float split;
+  int32_t left, right, first, count;
+} o_kdb_node;
+
+typedef struct {
+  o_kdb_node* nodes;
+  int32_t n_nodes;
+  int32_t* index;
+  int64_t n_index;
+  float bmin[3], bmax[3];
+} o_kdb_tree;
+
+/* Binned SAH (32 planes per axis) over an indexed mesh; 0 on success. */
+int o_kdb_build(const float* verts, int32_t nv, const uint32_t* faces, int32_t nf,
+                int max_depth, int leaf_size, float ci, float ct, float empty_bonus,
+                o_kdb_tree* out);
+void o_kdb_free(o_kdb_tree* t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -298,6 +298,33 @@ class RefTree:
         f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
         self._h = L.ref_tree_create(_p(v), ctypes.c_int(v.shape[0]), _p(f), ctypes.c_int(f.shape[0]))
 
+    @classmethod
+    def from_kd(cls, verts, faces, kd):
+        """The reference's RKDTreeCPU holding the SAH tree `kd` (a KdbTree)
+        as its own KDNodeCPU objects instead of the one leaf its builder
+        makes; queries run the reference's compiled code unchanged."""
+        self = cls.__new__(cls)
+        L = ref_lib()
+        if L is None:
+            raise FileNotFoundError(REF_LIB_PATH)
+        L.ref_tree_from_kd.restype = ctypes.c_void_p
+        L.ref_tree_from_kd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]
+        L.ref_tree_destroy.argtypes = [ctypes.c_void_p]
+        L.ref_tree_trace.restype = ctypes.c_int64
+        L.ref_tree_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.ref_max_threads.restype = ctypes.c_int
+        self._L = L
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+        bmin = np.asarray(kd.bmin, np.float32)
+        bmax = np.asarray(kd.bmax, np.float32)
+        self._h = L.ref_tree_from_kd(_p(v), ctypes.c_int(v.shape[0]), _p(f), ctypes.c_int(f.shape[0]),
+                                     _p(kd.nodes), _p(kd.index), _p(bmin), _p(bmax))
+        return self
+
     def threads(self) -> int:
         return int(self._L.ref_max_threads())
 
@@ -323,6 +350,54 @@ class RefTree:
             self.close()
         except Exception:
             pass
+
+
+KDB_NODE = np.dtype([("axis", "<i4"), ("split", "<f4"), ("left", "<i4"), ("right", "<i4"),
+                     ("first", "<i4"), ("count", "<i4")])
+
+
+class _OKdbTree(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int32),
+                ("index", ctypes.c_void_p), ("n_index", ctypes.c_int64),
+                ("bmin", ctypes.c_float * 3), ("bmax", ctypes.c_float * 3)]
+
+
+class KdbTree:
+    """The checker's binned-SAH kd-tree (oracle_kdbuild.c): pre-order nodes
+    (KDB_NODE), the leaves' triangle lists and the root box."""
+
+    def __init__(self, nodes, index, bmin, bmax):
+        self.nodes, self.index, self.bmin, self.bmax = nodes, index, bmin, bmax
+
+    def depth(self) -> int:
+        d = np.zeros(len(self.nodes), np.int32)
+        for i, n in enumerate(self.nodes):
+            if n["axis"] != 3:
+                d[n["left"]] = d[n["right"]] = d[i] + 1
+        return int(d.max())
+
+
+def kdb_build(verts, faces, max_depth=24, leaf_size=8, ci=2.0, ct=1.0, empty_bonus=0.15):
+    """SAH kd-tree over an indexed mesh (the reference arm's configured tree)."""
+    L = lib()
+    L.o_kdb_build.restype = ctypes.c_int
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+    t = _OKdbTree()
+    rc = L.o_kdb_build(_p(v), ctypes.c_int32(v.shape[0]), _p(f), ctypes.c_int32(f.shape[0]),
+                       ctypes.c_int(max_depth), ctypes.c_int(leaf_size), ctypes.c_float(ci),
+                       ctypes.c_float(ct), ctypes.c_float(empty_bonus), ctypes.byref(t))
+    if rc != 0:
+        raise MemoryError("o_kdb_build failed")
+    try:
+        nodes = np.ctypeslib.as_array(ctypes.cast(t.nodes, ctypes.POINTER(ctypes.c_int32)),
+                                      (t.n_nodes * 6,)).copy().view(KDB_NODE)
+        index = np.ctypeslib.as_array(ctypes.cast(t.index, ctypes.POINTER(ctypes.c_int32)),
+                                      (int(t.n_index),)).copy() if t.n_index else np.zeros(0, np.int32)
+        bmin, bmax = list(t.bmin), list(t.bmax)
+    finally:
+        L.o_kdb_free(ctypes.byref(t))
+    return KdbTree(nodes, index, bmin, bmax)
 
 
 def ref_perm(seed: int) -> np.ndarray:

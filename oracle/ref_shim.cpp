@@ -15,7 +15,9 @@
 //     own tree, run over many rays with OpenMP `parallel for
 //     schedule(dynamic)` as RRayTracer::trace does
 //     (RayEngine/src/Engine/RayTracer.cpp:154).  The benchmark's reference
-//     arm times this.
+//     arm times this, over the reference's own one-leaf tree and over an SAH
+//     tree of the configured parameters (oracle_kdbuild.c) turned into the
+//     reference's KDNodeCPU objects (ref_tree_from_kd).
 //
 // Nothing in the product links this file.
 #include "repch.h"
@@ -99,6 +101,96 @@ void* ref_tree_create(const float* verts, int num_verts, const uint32_t* faces, 
     x = l > 0.f ? make_float3(x.x / l, x.y / l, x.z / l) : make_float3(0.f, 1.f, 0.f);
   }
   return new RKDTreeCPU(v.data(), f.data(), n.data(), nullptr, num_verts, num_faces, num_verts, 0);
+}
+
+// An SAH tree made elsewhere (oracle_kdbuild.c: pre-order nodes {axis (3 =
+// leaf), split, left, right, first, count} and the leaves' triangle lists)
+// turned into the reference's own KDNodeCPU objects inside an RKDTreeCPU, so
+// that its CPU query runs over a tree of the configured parameters instead
+// of the one leaf its builder makes.  Node boxes are the root box cut at
+// the splits; the query (singleRayStacklessIntersect) tests each node's box
+// and recurses into both children, testing every leaf the ray's box test
+// reaches.
+struct RefKdbNode {
+  int32_t axis;
+  float split;
+  int32_t left, right, first, count;
+};
+
+static KDNodeCPU* ref_make_node(const RefKdbNode* nodes, const int32_t* index, int32_t id,
+                                float3 lo, float3 hi) {
+  const RefKdbNode& src = nodes[id];
+  KDNodeCPU* n = new KDNodeCPU();
+  n->box = RBoundingVolume(lo, hi);
+  n->numFaces = 0;
+  n->numVerts = 0;
+  n->objIndeces = nullptr;
+  n->split_val = src.split;
+  n->axis = src.axis == 0 ? X_Axis : (src.axis == 1 ? Y_Axis : Z_Axis);
+  if (src.axis == 3) {
+    n->isLeaf = true;
+    n->numFaces = src.count;
+    if (src.count > 0) {
+      n->objIndeces = new int[src.count];
+      for (int32_t i = 0; i < src.count; ++i) n->objIndeces[i] = index[src.first + i];
+    }
+    return n;
+  }
+  float3 lhi = hi, rlo = lo;
+  if (src.axis == 0) {
+    lhi.x = src.split;
+    rlo.x = src.split;
+  } else if (src.axis == 1) {
+    lhi.y = src.split;
+    rlo.y = src.split;
+  } else {
+    lhi.z = src.split;
+    rlo.z = src.split;
+  }
+  n->isLeaf = false;
+  n->LeftNode = ref_make_node(nodes, index, src.left, lo, lhi);
+  n->RightNode = ref_make_node(nodes, index, src.right, rlo, hi);
+  return n;
+}
+
+void* ref_tree_from_kd(const float* verts, int num_verts, const uint32_t* faces, int num_faces,
+                       const void* kd_nodes, const int32_t* kd_index, const float* bmin,
+                       const float* bmax) {
+  RKDTreeCPU* t = new RKDTreeCPU();
+  t->num_verts = num_verts;
+  t->num_norms = num_verts;
+  t->num_faces = num_faces;
+  t->num_uvs = 0;
+  t->uvs = nullptr;
+  t->verts = new float3[num_verts];
+  t->norms = new float3[num_verts];
+  t->faces = new uint3[num_faces];
+  for (int i = 0; i < num_verts; ++i) {
+    t->verts[i] = make_float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+    t->norms[i] = make_float3(0.f, 0.f, 0.f);
+  }
+  for (int i = 0; i < num_faces; ++i) {
+    t->faces[i] = make_uint3(faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]);
+    float3 a = t->verts[t->faces[i].x], b = t->verts[t->faces[i].y], c = t->verts[t->faces[i].z];
+    float3 e1 = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+    float3 e2 = make_float3(c.x - a.x, c.y - a.y, c.z - a.z);
+    float3 fn = make_float3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z,
+                            e1.x * e2.y - e1.y * e2.x);
+    for (uint32_t k : {t->faces[i].x, t->faces[i].y, t->faces[i].z}) {
+      t->norms[k].x += fn.x;
+      t->norms[k].y += fn.y;
+      t->norms[k].z += fn.z;
+    }
+  }
+  for (int i = 0; i < num_verts; ++i) {
+    float3& x = t->norms[i];
+    float l = std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z);
+    x = l > 0.f ? make_float3(x.x / l, x.y / l, x.z / l) : make_float3(0.f, 1.f, 0.f);
+  }
+  t->root = ref_make_node(static_cast<const RefKdbNode*>(kd_nodes), kd_index, 0,
+                          make_float3(bmin[0], bmin[1], bmin[2]),
+                          make_float3(bmax[0], bmax[1], bmax[2]));
+  return t;
 }
 
 void ref_tree_destroy(void* tree) { delete static_cast<RKDTreeCPU*>(tree); }

@@ -41,5 +41,9 @@ def test_reference_arm_prints_one_contract_line(config):
                         "d2h_bytes_per_step": 0}
     assert "PRODUCT_NOT_MAPPED" in out.stdout
     if config == "soup" and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libre_ref.so")):
-        # meshes: the reference's own compiled CPU query is what is timed
+        # meshes: the reference's own compiled CPU query is what is timed,
+        # over the configured SAH tree, with the as-shipped one-leaf tree
+        # beside it
         assert d["cpu_baseline"]["kind"] == "reference" and "REF_MAPPED" in out.stdout
+        assert "SAH kd-tree of the configured parameters" in d["cpu_baseline"]["sample"]
+        assert 0 < d["as_shipped"]["value"] < d["value"]

@@ -43,7 +43,9 @@ extern "C" {
 #endif
 
 #define RE_API __attribute__((visibility("default")))
-#define RE_ABI_VERSION 1
+/* 2: re_nsdf_trace_params gained the cone tracer's fields and root_tol;
+ *    re_tuning.ray_lanes accepts 32 (the warp-cooperative walk) */
+#define RE_ABI_VERSION 2
 
 typedef enum re_status {
   RE_OK = 0,

@@ -310,6 +310,9 @@ _SIGS = {
 
 EXPORTED = tuple(_SIGS)
 
+# RE_ABI_VERSION of include/rayengine_b200.h that the structures above mirror
+ABI_VERSION = 2
+
 
 class _Library:
     """librayengine_b200.so, loaded (and its signatures declared) on first use."""
@@ -324,6 +327,10 @@ class _Library:
                 fn = getattr(dll, name)
                 fn.restype = res
                 fn.argtypes = args
+            abi = dll.re_abi_version()
+            if abi != ABI_VERSION:
+                raise ImportError(f"{LIB_PATH} has ABI version {abi}, these bindings expect "
+                                  f"{ABI_VERSION}: rebuild the library")
             self._dll = dll
         return self._dll
 

@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version_and_status_strings():
-    assert _lib.lib.re_abi_version() == 1
+    assert _lib.lib.re_abi_version() == _lib.ABI_VERSION == 2
     assert _lib.lib.re_status_string(0) == b"ok"
     assert _lib.lib.re_status_string(4) == b"size limit exceeded"
 

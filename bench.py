@@ -819,7 +819,9 @@ class NeuralTerrainSDF:
                             f"({n.cone_lanes} lanes per cone, speculative steps); exact phase from "
                             "the cone's stop (the exact tracer's steps, grown up to "
                             f"{n.relax}x along the secant; bracket + {n.root_steps} regula-falsi "
-                            "steps) + exact central-difference normal",
+                            "steps) + the exact field's "
+                            + ("tetrahedral (compute_sdf_normal_tet)" if n.normal_taps == 4
+                               else "central-difference") + " normal at radius 0.002 t",
                 "training": {"points": n.num_points, "steps": n.train_steps, "batch": n.batch,
                              "lr": n.lr, "seconds": round(self.train_s, 2),
                              "final_l1_loss": round(self.final_loss, 5)},

@@ -120,3 +120,13 @@ def test_frame_config_matches_library_defaults():
     b = _lib.re_sdf_shade_params()
     _lib.lib.re_sdf_shade_params_default(ctypes.byref(b))
     assert bytes(a) == bytes(b)
+
+
+def test_measurement_probes_reject_bad_sizes():
+    """The roofline probes check their arguments before touching a device."""
+    v = ctypes.c_float()
+    for nbytes, passes in ((1 << 10, 10), (128 << 20, 10), (32 << 20, 0), (32 << 20, 5000)):
+        assert _lib.lib.re_measure_l2_read(nbytes, passes, ctypes.byref(v), None) == 1
+    for iters in (0, 1000, (1 << 20) + 1):
+        assert _lib.lib.re_measure_fp32_fma(iters, ctypes.byref(v), None) == 1
+    assert _lib.lib.re_measure_fp32_fma(1 << 16, None, None) == 1

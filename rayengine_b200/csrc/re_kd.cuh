@@ -114,6 +114,19 @@ struct Trav {
   bool live;
 };
 
+// Whether origin o lies in the region of leaf node `start` (the condition
+// under which a walk may begin there instead of at the root).
+__device__ __forceinline__ bool origin_in_leaf(const KdDev& kd, V3 o, uint32_t start) {
+  uint2 sn = __ldg(&kd.nodes[start]);
+  if ((sn.y & 3u) != 3u) return false;
+  const float4* SL = kd.leaves + 4 * (size_t)(sn.y >> 2);
+  float4 A = __ldg(SL), B = __ldg(SL + 1);
+  return o.x >= A.x && o.x <= A.w && o.y >= A.y && o.y <= B.x && o.z >= A.z && o.z <= B.y;
+}
+
+// CHECKED false: the caller has already established origin_in_leaf(start)
+// (or passes start 0), so the walk begins at `start` without loading it.
+template <bool CHECKED = true>
 __device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, float tmax,
                                           uint32_t start) {
   s.o = o;
@@ -131,14 +144,10 @@ __device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, 
   if (!s.live) return;
   s.best_t = fminf(t_root_exit, tmax);
   s.live = s.t_entry < s.best_t;
-  if (s.live && start != 0) {
-    uint2 sn = __ldg(&kd.nodes[start]);
-    if ((sn.y & 3u) == 3u) {
-      const float4* SL = kd.leaves + 4 * (size_t)(sn.y >> 2);
-      float4 A = __ldg(SL), B = __ldg(SL + 1);
-      if (o.x >= A.x && o.x <= A.w && o.y >= A.y && o.y <= B.x && o.z >= A.z && o.z <= B.y)
-        s.node = start;
-    }
+  if (CHECKED) {
+    if (s.live && start != 0 && origin_in_leaf(kd, o, start)) s.node = start;
+  } else {
+    s.node = start;
   }
 }
 

@@ -391,8 +391,10 @@ __global__ void __launch_bounds__(256, 5) k_ao_primary(KdDev kd, CamDev cam, AoD
               __fmaf_rn(n.z, ao.bias, p.z)};
     uint32_t pix = y * w + x;
     // record: {origin, start leaf node} {direction, pixel*8 + mask bit}; the
-    // shadow ray (bit 1) is unbounded, AO rays (bits 2..5) have ao_length
-    float start = __uint_as_float(hs.leaf_node);
+    // shadow ray (bit 1) is unbounded, AO rays (bits 2..5) have ao_length.
+    // The start leaf is checked here, once for the hit's five rays (0: the
+    // origin left the leaf, start at the root); the secondary pass trusts it.
+    float start = __uint_as_float(origin_in_leaf(kd, org, hs.leaf_node) ? hs.leaf_node : 0u);
     float4* queue = aq.q;
     size_t q0 = shadow_record(aq, rank);
     queue[2 * q0] = make_float4(org.x, org.y, org.z, start);
@@ -476,8 +478,8 @@ __global__ void __launch_bounds__(256, 5) k_ao_secondary(KdDev kd, AoDev ao, AoQ
           float4 R0 = __ldg(&aq.q[2 * (size_t)e]), R1 = __ldg(&aq.q[2 * (size_t)e + 1]);
           tag = __float_as_uint(R1.w);
           float tmax = kind == 0 ? K_INF : ao.ao_length;
-          trav_init(s, kd, v3(R0.x, R0.y, R0.z), v3(R1.x, R1.y, R1.z), tmax,
-                    __float_as_uint(R0.w));
+          trav_init<false>(s, kd, v3(R0.x, R0.y, R0.z), v3(R1.x, R1.y, R1.z), tmax,
+                           __float_as_uint(R0.w));
           ++rays;
           if (!s.live && !COUNT) atomicOr(&mask[tag >> 3], 1u << (tag & 7u));
         }

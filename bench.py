@@ -166,6 +166,12 @@ FP32_TOPS_NOMINAL = 148 * 128 * 1.965e9 / 1e12
 # 15 quintic, 3 offsets, 16 gradient dots, 19 for k1..k7, 11 interpolation)
 # + 5 fBm bookkeeping per octave, + 4 for the scale and the final FMA
 SDF_OPS_PER_EVAL = 8 * 75 + 4
+# one analytic gradient of the field (the neural tracer's normal): per
+# octave 3 floor, 3 frac, 15 quintic, 3 offsets, 12 fade derivatives, 16
+# gradient dots, 19 for k1..k7, 23 corner weights, 36 for the three
+# components, 3 accumulations, 3 coordinate doublings; + 6 for the scale
+# and the final FMA, + 8 to normalise
+SDF_GRAD_OPS_PER_EVAL = 8 * 136 + 14
 # BF16 tensor FLOPs of one network evaluation: 2 (128*64 + 3*64*64 + 64)
 NSDF_FLOPS_PER_EVAL = 41088
 
@@ -807,7 +813,8 @@ class NeuralTerrainSDF:
         torch.cuda.synchronize()
         self.exact_ms = a.elapsed_time(b) / 20
         self.rays_per_step = W * H
-        self.kernels_per_step = 2
+        # cone march, exact phase (+ the gradient-normal pass)
+        self.kernels_per_step = 3 if self.ncfg.normal_taps == 1 else 2
 
     def config(self):
         n = self.ncfg
@@ -820,8 +827,9 @@ class NeuralTerrainSDF:
                             "the cone's stop (the exact tracer's steps, grown up to "
                             f"{n.relax}x along the secant; bracket + {n.root_steps} regula-falsi "
                             "steps) + the exact field's "
-                            + ("tetrahedral (compute_sdf_normal_tet)" if n.normal_taps == 4
-                               else "central-difference") + " normal at radius 0.002 t",
+                            + ({4: "tetrahedral (compute_sdf_normal_tet) normal at radius 0.002 t",
+                                1: "analytic-gradient normal"}.get(
+                                   n.normal_taps, "central-difference normal at radius 0.002 t")),
                 "training": {"points": n.num_points, "steps": n.train_steps, "batch": n.batch,
                              "lr": n.lr, "seconds": round(self.train_s, 2),
                              "final_l1_loss": round(self.final_loss, 5)},
@@ -862,9 +870,15 @@ class NeuralTerrainSDF:
                "traffic": ncu_traffic(f"{self.name}:nsdf_network")}
         if phase_ms["nsdf_network"] >= phase_ms["sdf_refine"]:
             return net
-        evals = self.stats["exact_evals"] + self.stats["normal_evals"]
-        return fp32_roofline("sdf_refine", evals * SDF_OPS_PER_EVAL, phase_ms["sdf_refine"], peaks,
-                             self.name, network_phase=net)
+        # normal_taps 1: each normal is one analytic gradient evaluation
+        # (k_sdf_grad_normal, timed inside the exact phase)
+        grad = self.ncfg.normal_taps == 1
+        ops = (self.stats["exact_evals"] * SDF_OPS_PER_EVAL + self.stats["normal_evals"] *
+               (SDF_GRAD_OPS_PER_EVAL if grad else SDF_OPS_PER_EVAL))
+        return fp32_roofline("sdf_refine", ops, phase_ms["sdf_refine"], peaks, self.name,
+                             network_phase=net,
+                             exact_phase_kernels=["k_sdf_refine"] + (["k_sdf_grad_normal"]
+                                                                     if grad else []))
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height

@@ -413,7 +413,9 @@ typedef struct re_nsdf_trace_params {
                         /* per-ray network march and hand-over queue       */
   uint32_t cone_coarse; /* 0, or a multiple of cone_tile (<= 1024): a      */
                         /* first cone level over tiles of this size        */
-  uint32_t normal_taps; /* 0 or 6: central differences; 4: tetrahedral    */
+  uint32_t normal_taps; /* 0 or 6: central differences; 4: tetrahedral;   */
+                        /* 1: the exact field's analytic gradient, in a   */
+                        /* second pass over the hits                      */
   uint32_t cone_lanes;  /* 0 or 1, 2, 4, 8: lanes per cone; above 1 they   */
                         /* evaluate successive guessed steps in one pass   */
   float root_tol;       /* > 0: the root search ends when its next secant  */

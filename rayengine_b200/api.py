@@ -474,7 +474,8 @@ def nsdf_trace_params(lipschitz=1.0, safety=0.9, switch_dist=0.05, min_step=1e-3
     first level over cone_coarse tiles when that is set) and every pixel's
     exact phase starts where its tile stopped; cone_lanes lanes evaluate
     successive guessed steps of a cone in one pass.  normal_taps: 6 central
-    differences, 4 the tetrahedral normal.  root_tol > 0 ends the root
+    differences, 4 the tetrahedral normal, 1 the exact field's analytic
+    gradient (a second pass over the hits).  root_tol > 0 ends the root
     search once its secant point moves less than that."""
     p = _lib.re_nsdf_trace_params()
     p.lipschitz, p.safety, p.switch_dist, p.min_step = lipschitz, safety, switch_dist, min_step

@@ -152,4 +152,83 @@ __device__ __forceinline__ float terrain_density(const PT& P, V3 p,
   return __fmaf_rn(-amp, f, p.y);
 }
 
+// Gradient of perlin() at (x, y, z), from the same lattice, fade and blend
+// differentiated in closed form.  With corner values a..h (corner gradient
+// vector ga..gh dotted with the offset to the corner) the blend is
+//   n = a + k1 u + k2 v + k3 w + k4 uv + k5 uw + k6 vw + k7 uvw,
+// u = fade(tx) etc., so
+//   dn/dx = [sum over corners of (its trilinear weight in u, v, w) g].x
+//           + fade'(tx) (k1 + k4 v + k5 w + k7 vw),
+// likewise for y and z, with fade'(t) = 30 t^2 (t - 1)^2.  Each component of
+// a corner's gradient vector is +1, -1 or 0; the case bit of grad() tells
+// which (bit masks over the 16 cases, the same vectors as grad_dot's), so
+// the weighted sum adds or subtracts the weight instead of multiplying.
+template <class PT>
+__device__ __forceinline__ V3 perlin_grad(const PT& P, float x, float y, float z) {
+  float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  uint32_t xi0 = ((int)fx) & 255, yi0 = ((int)fy) & 255, zi0 = ((int)fz) & 255;
+  uint32_t xi1 = xi0 + 1, yi1 = yi0 + 1, zi1 = zi0 + 1;
+  float tx = x - fx, ty = y - fy, tz = z - fz;
+  float u = quintic(tx), v = quintic(ty), w = quintic(tz);
+  float x1 = tx - 1.0f, y1 = ty - 1.0f, z1 = tz - 1.0f;
+  float du = 30.0f * (tx * tx) * (x1 * x1);
+  float dv = 30.0f * (ty * ty) * (y1 * y1);
+  float dw = 30.0f * (tz * tz) * (z1 * z1);
+  uint32_t px0 = P.idx(xi0), px1 = P.idx(xi1);
+  uint32_t p00 = P.idx(px0 + yi0), p10 = P.idx(px1 + yi0);
+  uint32_t p01 = P.idx(px0 + yi1), p11 = P.idx(px1 + yi1);
+  const uint32_t G[8] = {P.grad(p00 + zi0), P.grad(p10 + zi0), P.grad(p01 + zi0),
+                         P.grad(p11 + zi0), P.grad(p00 + zi1), P.grad(p10 + zi1),
+                         P.grad(p01 + zi1), P.grad(p11 + zi1)};
+  const float a = grad_dot(G[0], tx, ty, tz), b = grad_dot(G[1], x1, ty, tz);
+  const float c = grad_dot(G[2], tx, y1, tz), d = grad_dot(G[3], x1, y1, tz);
+  const float e = grad_dot(G[4], tx, ty, z1), f = grad_dot(G[5], x1, ty, z1);
+  const float g = grad_dot(G[6], tx, y1, z1), h = grad_dot(G[7], x1, y1, z1);
+  float k1 = b - a, k2 = c - a, k3 = e - a;
+  float k4 = ((a + d) - b) - c;
+  float k5 = ((a + f) - b) - e;
+  float k6 = ((a + g) - c) - e;
+  float k7 = ((((((b + c) + e) + h) - a) - d) - f) - g;
+  float uv = u * v, uw = u * w, vw = v * w, uvw = uv * w;
+  // trilinear weights of the corners (order a..h: x fastest, then y, z)
+  const float cw[8] = {1.0f - u - v - w + uv + uw + vw - uvw, u - uv - uw + uvw,
+                       v - uv - vw + uvw, uv - uvw, w - uw - vw + uvw, uw - uvw, vw - uvw, uvw};
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    // gradient vector components by case: x +1 for cases 0 2 4 6 12, -1
+    // for 1 3 5 7 13; y +1 for 0 1 8 10 12 13, -1 for 2 3 9 11 14 15; z +1
+    // for 4 5 8 9 14, -1 for 6 7 10 11 15
+    const uint32_t gk = G[k];
+    const float ck = cw[k];
+    sx += (gk & (0x1055u << 16)) ? ck : ((gk & (0x20AAu << 16)) ? -ck : 0.0f);
+    sy += (gk & (0x3503u << 16)) ? ck : ((gk & (0xCA0Cu << 16)) ? -ck : 0.0f);
+    sz += (gk & (0x4330u << 16)) ? ck : ((gk & (0x8CC0u << 16)) ? -ck : 0.0f);
+  }
+  V3 r;
+  r.x = sx + du * (k1 + k4 * v + k5 * w + k7 * vw);
+  r.y = sy + dv * (k2 + k4 * u + k6 * w + k7 * uw);
+  r.z = sz + dw * (k3 + k5 * u + k6 * v + k7 * uv);
+  return r;
+}
+
+// Gradient of terrain_density: (0, 1, 0) - amp * scale * sum_i gain^i
+// lacunarity^i grad perlin(lacunarity^i scale p), lacunarity 2, gain 0.5
+// (each octave's amplitude x frequency is 1).
+template <class PT>
+__device__ __forceinline__ V3 terrain_gradient(const PT& P, V3 p, uint32_t octaves, float scale,
+                                               float amp) {
+  float x = scale * p.x, y = scale * p.y, z = scale * p.z;
+  V3 s = v3(0.f, 0.f, 0.f);
+  for (uint32_t i = 0; i < octaves; ++i) {
+    V3 gi = perlin_grad(P, x, y, z);
+    s = v3(s.x + gi.x, s.y + gi.y, s.z + gi.z);
+    x *= 2.0f;
+    y *= 2.0f;
+    z *= 2.0f;
+  }
+  const float k = -amp * scale;
+  return v3(k * s.x, __fmaf_rn(k, s.y, 1.0f), k * s.z);
+}
+
 }  // namespace re

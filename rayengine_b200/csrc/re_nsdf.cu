@@ -970,7 +970,7 @@ struct RefineDev {
   float relax;          // an exact step may grow to relax x (step_factor * d) along a secant
   float root_tol;       // the root search ends when the secant point moves less than this
   float ceiling;        // no surface above this height (bound of the field)
-  uint32_t normal_taps;  // 6: central differences; 4: tetrahedral
+  uint32_t normal_taps;  // 6: central differences; 4: tetrahedral; 1: none here (k_sdf_grad_normal)
   // cone starts (direct mode): pixel (x, y) starts at tile_t[(y / cone_tile)
   // * cone_tiles_x + x / cone_tile]; null: every pixel starts at t = 0
   const float* tile_t;
@@ -1308,7 +1308,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_cone(InputMap m,
 //   normal the exact tracer's central differences (delta = 0.002 t), or,
 //          with normal_taps 4, the reference's tetrahedral normal
 //          (compute_sdf_normal_tet) at the same radius: sum of e_k d(p +
-//          delta e_k) over the four tetrahedron directions e_k.
+//          delta e_k) over the four tetrahedron directions e_k.  With
+//          normal_taps 1 the hit is written without a normal and
+//          k_sdf_grad_normal adds the field's analytic gradient afterwards.
 // With cone starts a ray begins its march where its tile's cone stopped; a
 // start that is already inside the terrain (the network overestimated the
 // distance) marches again from the camera.
@@ -1316,6 +1318,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_cone(InputMap m,
 // evaluations (normals excluded, as in the exact tracer).
 enum : uint32_t { kMarch = 0, kProbe = 1, kRoot = 2, kNormal = 3 };
 
+// NT: the normal (RefineDev::normal_taps), fixed at compile time so that
+// the analytic-gradient form (1) carries no stencil state.
+template <uint32_t NT>
 __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, RefineDev rd,
                                                     CamDev cam, uint32_t w, uint32_t h, int direct,
                                                     const uint4* __restrict__ queue,
@@ -1381,9 +1386,9 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
     } else if (mode == kProbe) {
       qp = v3(__fmaf_rn(a, d.x, o.x), __fmaf_rn(a, d.y, o.y), __fmaf_rn(a, d.z, o.z));
-    } else if (mode == kRoot) {
+    } else if (NT == 1u || mode == kRoot) {
       qp = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
-    } else if (rd.normal_taps == 4u) {
+    } else if (NT == 4u) {
       V3 e = tet_dir(tap);
       qp = v3(__fmaf_rn(e.x, delta, p.x), __fmaf_rn(e.y, delta, p.y), __fmaf_rn(e.z, delta, p.z));
     } else {
@@ -1394,7 +1399,7 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
       else qp.z = p.z + sd;
     }
     float v = terrain_density(P, qp, f.octaves, f.scale, f.amp);
-    if (mode == kNormal) ++n_normal;
+    if (NT != 1u && mode == kNormal) ++n_normal;
     else ++n_exact;
     uint32_t status = 3;  // 3 = still running
     bool begin_root = false, hit_here = false;
@@ -1450,7 +1455,7 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
         mode = kMarch;
         if (steps >= rd.max_steps) status = 2;
       }
-    } else if (mode == kRoot) {
+    } else if (NT == 1u || mode == kRoot) {
       ++steps;
       if (fabsf(v) < 1e-6f || ++iters >= rd.root_steps) {
         hit_here = true;
@@ -1471,7 +1476,7 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
         if (fabsf(tn - t) < rd.root_tol) hit_here = true;
         t = tn;
       }
-    } else if (rd.normal_taps == 4u) {
+    } else if (NT == 4u) {
       V3 e = tet_dir(tap);
       nx = __fmaf_rn(e.x, v, nx);
       ny = __fmaf_rn(e.y, v, ny);
@@ -1500,16 +1505,21 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
     }
     if (hit_here) {
       p = v3(__fmaf_rn(t, d.x, o.x), __fmaf_rn(t, d.y, o.y), __fmaf_rn(t, d.z, o.z));
-      delta = 0.002f * t;
-      mode = kNormal;
-      tap = 0;
-      nx = ny = nz = 0.f;
+      if (NT == 1u) {
+        // the hit is final here; k_sdf_grad_normal adds the normal
+        status = 1;
+      } else {
+        delta = 0.002f * t;
+        mode = kNormal;
+        tap = 0;
+        nx = ny = nz = 0.f;
+      }
     }
     if (status != 3) {
       float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1;
       uint32_t total_steps = base_steps + steps;
       if (status == 1) {
-        V3 n = normalize(v3(nx, ny, nz));
+        V3 n = NT == 1u ? v3(0.f, 0.f, 0.f) : normalize(v3(nx, ny, nz));
         r0 = make_float4(p.x, p.y, p.z, n.x);
         r1 = make_float4(n.y, n.z, __uint_as_float(total_steps), __uint_as_float(status));
       } else {
@@ -1526,6 +1536,36 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
     atomicAdd(&totals[1], (unsigned long long)n_exact);
     atomicAdd(&totals[2], (unsigned long long)n_normal);
   }
+}
+
+// normal_taps 1: the normal of every hit in `out` (status 1) is the exact
+// field's analytic gradient at the hit position, normalised
+// (terrain_gradient: one lattice walk per octave, about 1.5 field
+// evaluations of work, against 4 or 6 for the finite-difference stencils,
+// which at radius 0.002 t are coarse estimates of this gradient).  A
+// separate pass, so that the exact phase's state machine keeps a single
+// field call site and the gradient's lanes do not diverge from the march.
+__global__ void __launch_bounds__(256) k_sdf_grad_normal(PermTable perm, FieldDev f, uint32_t n,
+                                                         float4* __restrict__ out,
+                                                         unsigned long long* __restrict__ totals) {
+  extern __shared__ uint32_t perm_smem[];
+  load_perm(perm, perm_smem);
+  Perm P = perm_view(perm_smem);
+  uint32_t count = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 r1 = out[2 * (size_t)i + 1];
+    if (__float_as_uint(r1.w) != 1u) continue;
+    float4 r0 = out[2 * (size_t)i];
+    V3 nn = normalize(terrain_gradient(P, v3(r0.x, r0.y, r0.z), f.octaves, f.scale, f.amp));
+    r0.w = nn.x;
+    r1.x = nn.y;
+    r1.y = nn.z;
+    out[2 * (size_t)i] = r0;
+    out[2 * (size_t)i + 1] = r1;
+    ++count;
+  }
+  count = __reduce_add_sync(0xFFFFFFFFu, count);
+  if ((threadIdx.x & 31u) == 0u && count) atomicAdd(&totals[2], (unsigned long long)count);
 }
 
 // Finite-difference gradient norm of the network at n sample points (vals
@@ -2123,8 +2163,9 @@ re_status trace_check(re_nsdf* s, const re_sdf_params* field, const re_nsdf_trac
     return fail(RE_ERR_INVALID_ARG,
                 "%s: cone_tile <= 256; cone_coarse 0 or a multiple of cone_tile above it, <= 1024",
                 fn);
-  if (tp->normal_taps != 0 && tp->normal_taps != 4 && tp->normal_taps != 6)
-    return fail(RE_ERR_INVALID_ARG, "%s: normal_taps 0, 4 or 6", fn);
+  if (tp->normal_taps != 0 && tp->normal_taps != 1 && tp->normal_taps != 4 &&
+      tp->normal_taps != 6)
+    return fail(RE_ERR_INVALID_ARG, "%s: normal_taps 0, 1, 4 or 6", fn);
   if (tp->cone_lanes > 8 || (tp->cone_lanes & (tp->cone_lanes - 1u)))
     return fail(RE_ERR_INVALID_ARG, "%s: cone_lanes 0, 1, 2, 4 or 8", fn);
   return RE_OK;
@@ -2244,7 +2285,9 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
     return re::fail(RE_ERR_INVALID_ARG, "re_nsdf_trace_exact: no network phase for this image");
   cudaStream_t cs = (cudaStream_t)stream;
   unsigned long long* totals = reinterpret_cast<unsigned long long*>(s->counters + 4);
-  auto kr = re::nsdf::k_sdf_refine;
+  auto kr = tp->normal_taps == 1u   ? re::nsdf::k_sdf_refine<1u>
+            : tp->normal_taps == 4u ? re::nsdf::k_sdf_refine<4u>
+                                    : re::nsdf::k_sdf_refine<6u>;
   RE_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)re::kPermSmemBytes));
   int per_sm = 0;
@@ -2262,7 +2305,7 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
   // density is positive above this height
   rd.ceiling =
       2.0f * std::fabs(field->amplitude) * (2.0f - std::ldexp(1.0f, 1 - (int)field->octaves)) + 1e-3f;
-  rd.normal_taps = tp->normal_taps == 4u ? 4u : 6u;
+  rd.normal_taps = tp->normal_taps == 4u || tp->normal_taps == 1u ? tp->normal_taps : 6u;
   rd.tile_t = cone ? s->cone_t : nullptr;
   rd.cone_tile = cone ? s->cone_tile : 1u;
   rd.cone_tiles_x = cone ? s->cone_tiles_x : 0u;
@@ -2270,6 +2313,18 @@ RE_API re_status re_nsdf_trace_exact(re_nsdf* s, const re_sdf_params* field,
       re::perm_of(field->seed), re::field_of(*field), rd, re::cam_dev(*cam), w, h,
       exact_only || cone ? 1 : 0, s->queue, s->counters, totals, reinterpret_cast<float4*>(d_out));
   RE_CHECK_LAUNCH("re_nsdf_trace_exact: refine launch");
+  if (rd.normal_taps == 1u) {
+    auto kg = re::nsdf::k_sdf_grad_normal;
+    int gper_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gper_sm, kg, 256, re::kPermSmemBytes) !=
+            cudaSuccess ||
+        gper_sm < 1)
+      gper_sm = 1;
+    kg<<<gper_sm * re::sm_count(), 256, re::kPermSmemBytes, cs>>>(
+        re::perm_of(field->seed), re::field_of(*field), w * h, reinterpret_cast<float4*>(d_out),
+        totals);
+    RE_CHECK_LAUNCH("re_nsdf_trace_exact: normal launch");
+  }
   return RE_OK;
 }
 

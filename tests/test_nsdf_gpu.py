@@ -113,14 +113,16 @@ def _sdf_errors(out, tc, pix):
 def _normals_from_positions(out, cam, pix, taps):
     """The exact phase's normal recomputed on the host in FP64 from the
     returned hit positions: central differences (taps 6) or the tetrahedral
-    stencil (taps 4), delta = 0.002 t with t = |p - camera|."""
+    stencil (taps 4), delta = 0.002 t with t = |p - camera|; taps 1: the
+    field's gradient (FP64 central differences of radius 1e-5, whose error
+    is far below FP32's).  Returns the angles in degrees."""
     tc = rb.configs.TerrainConfig()
     P = po.perm(tc.seed)
     f = out.view(np.float32)[pix]
     p = f[:, 0:3].astype(np.float64)
     t = np.linalg.norm(p - np.array(cam.campos, np.float64), axis=1)
-    delta = (0.002 * t)[:, None]
-    if taps == 6:
+    delta = (0.002 * t)[:, None] if taps != 1 else np.full((len(p), 1), 1e-5)
+    if taps in (6, 1):
         n = np.zeros_like(p)
         for k in range(3):
             e = np.zeros(3)
@@ -134,7 +136,11 @@ def _normals_from_positions(out, cam, pix, taps):
             n += e[None, :] * po.density_d(P, p + delta * e)[:, None]
     n /= np.linalg.norm(n, axis=1, keepdims=True)
     got = f[:, 3:6].astype(np.float64)
-    return np.degrees(np.arccos(np.clip((n * got).sum(1), -1.0, 1.0)))
+    # the angle from atan2(|a x b|, a . b) of the renormalised vectors: an
+    # arccos of the dot product would read FP32's normalisation error
+    # (|n| = 1 +- 6e-8) as angles of ~0.02 degrees
+    got /= np.linalg.norm(got, axis=1, keepdims=True)
+    return np.degrees(np.arctan2(np.linalg.norm(np.cross(n, got), axis=1), (n * got).sum(1)))
 
 
 def test_neural_trace_accuracy_and_exact_evaluations_saved(cuda):
@@ -184,6 +190,40 @@ def test_neural_trace_accuracy_and_exact_evaluations_saved(cuda):
             hits = pix[net[pix, 7] == 1]
             ang = _normals_from_positions(net, cam, hits[:400], params.normal_taps or 6)
             assert np.quantile(ang, 0.99) < 0.05, (name, np.quantile(ang, 0.99))
+
+
+def test_gradient_normal_pass(cuda):
+    """normal_taps 1: the exact phase writes the same hits (position, step
+    count, status) as with the tetrahedral normal, and the second pass adds
+    the field's analytic gradient, which agrees with the FP64 gradient."""
+    tc = rb.configs.TerrainConfig(width=320, height=180)
+    with _model() as m:
+        field, cam = tc.params(), tc.camera()
+        W, H = tc.width, tc.height
+        tet = m.trace(field, rb.nsdf_trace_params(exact_only=True, normal_taps=4), cam, W, H)
+        tet = tet.cpu().numpy()
+        st4 = m.trace_status()
+        grad = m.trace(field, rb.nsdf_trace_params(exact_only=True, normal_taps=1), cam, W, H)
+        grad = grad.cpu().numpy()
+        st1 = m.trace_status()
+        assert st1["error"] == 0
+        for col in (0, 1, 2, 6, 7):
+            assert np.array_equal(tet[:, col], grad[:, col]), col
+        hits = np.nonzero(grad[:, 7] == 1)[0]
+        assert len(hits) > 0.5 * W * H
+        assert st1["exact_evals"] == st4["exact_evals"]
+        assert st1["normal_evals"] == len(hits)  # one gradient per hit
+        nrm = grad.view(np.float32)[hits, 3:6]
+        assert np.allclose(np.linalg.norm(nrm, axis=1), 1.0, atol=1e-5)
+        assert np.all(grad.view(np.float32)[grad[:, 7] != 1, 3:6] == 0)
+        sample = np.random.default_rng(3).choice(hits, 3000, replace=False).astype(np.uint32)
+        ang = _normals_from_positions(grad, cam, sample, 1)
+        assert np.median(ang) < 1e-3 and np.quantile(ang, 0.99) < 1e-2, (
+            np.median(ang), np.quantile(ang, 0.99), ang.max())
+        # against it the finite-difference stencils at radius 0.002 t are
+        # coarse (several degrees)
+        tet_ang = _normals_from_positions(tet, cam, sample, 1)
+        assert np.median(tet_ang) > 1.0
 
 
 def test_trace_parameter_checks(cuda):

@@ -25,12 +25,17 @@ struct PermTable {
 // same parity).  512 entries x 16 copies x 4 B = 32 KB; measured on B200 2 %
 // faster on the SDF march than 32 conflict-free copies (64 KB), which allow
 // one block per SM fewer.  Each
-// word holds P[j] in bits 0-7 and the gradient case of P[j] as the bit
-// 1 << (16 + (P[j] & 15)), so a corner's gradient lookup needs no decoding.
+// word holds P[j] in bits 0-7 and the gradient case h = P[j] & 15 decoded
+// for grad_dot: bit 8 set when its first operand is y (else x), bit 9 when
+// its second operand is y (else z), bit 10 when the second operand is
+// negated and bit 31 when the first one is (so that negation is an XOR of
+// the operand's sign bit with the word).
 constexpr uint32_t kPermSmemBytes = 512 * 16 * 4;
 
 __host__ __device__ __forceinline__ uint32_t perm_word(uint32_t p) {
-  return p | (1u << (16u + (p & 15u)));
+  const uint32_t h = p & 15u;
+  return p | (((0xCF00u >> h) & 1u) << 8) | (((0x300Fu >> h) & 1u) << 9) |
+         (((0x8CCCu >> h) & 1u) << 10) | (((0xEAAAu >> h) & 1u) << 31);
 }
 
 __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
@@ -39,7 +44,7 @@ __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
 }
 
 // Permutation-table views: idx(j) = P[j] (a lattice index), grad(j) = the
-// gradient case bit of P[j] (1 << (16 + (P[j] & 15))).
+// perm_word() of P[j] (its gradient case decoded).
 struct Perm {
   const uint32_t* __restrict__ s;
   uint32_t lane;
@@ -67,18 +72,23 @@ struct PermBytes {
 };
 
 // gradientDotV (sdf_functions.cuh:26-47) without branches: each case is a
-// sum of two signed coordinates, picked here with selects from bit masks
-// (bit h set = property holds for case h).  The operands and their signs are
-// exactly the reference's, so the single rounded addition is unchanged.
-//   first operand is y for cases 8-12, 14, 15 (x otherwise), negated for
-//   1, 3, 5, 7, 9, 11, 13, 14, 15; second operand is y for 0-3 and 13, x for
-//   12 (z otherwise), negated for 2, 3, 6, 7, 10, 11, 15.
-// g: the case bit 1 << (16 + h) (a grad() lookup).
+// sum of two signed coordinates, picked here from the decoded case bits of
+// perm_word().  The operands and their signs are exactly the reference's,
+// so the single rounded addition is unchanged:
+//   first operand is y for cases 8-11, 14, 15 (x otherwise), negated for
+//   1, 3, 5, 7, 9, 11, 13, 14, 15; second operand is y for 0-3, 12 and 13
+//   (z otherwise), negated for 2, 3, 6, 7, 10, 11, 15.
+// Case 12 is the reference's y + x, taken here as x + y: IEEE addition is
+// commutative, so the sum is the same, and the second operand needs one
+// select instead of two.  Negating the first operand flips its sign bit
+// with the word's bit 31.  (Measured on B200: the field evaluation is bound
+// by the ALU pipe, where these selects run.)
+// g: a grad() lookup.
 __device__ __forceinline__ float grad_dot(uint32_t g, float x, float y, float z) {
-  float u = (g & (0xDF00u << 16)) ? y : x;
-  u = (g & (0xEAAAu << 16)) ? -u : u;
-  float v = (g & (0x200Fu << 16)) ? y : ((g & (0x1000u << 16)) ? x : z);
-  v = (g & (0x8CCCu << 16)) ? -v : v;
+  float u = (g & 0x100u) ? y : x;
+  u = __uint_as_float(__float_as_uint(u) ^ (g & 0x80000000u));
+  float v = (g & 0x200u) ? y : z;
+  v = (g & 0x400u) ? -v : v;
   return u + v;
 }
 
@@ -159,10 +169,10 @@ __device__ __forceinline__ float terrain_density(const PT& P, V3 p,
 // u = fade(tx) etc., so
 //   dn/dx = [sum over corners of (its trilinear weight in u, v, w) g].x
 //           + fade'(tx) (k1 + k4 v + k5 w + k7 vw),
-// likewise for y and z, with fade'(t) = 30 t^2 (t - 1)^2.  Each component of
-// a corner's gradient vector is +1, -1 or 0; the case bit of grad() tells
-// which (bit masks over the 16 cases, the same vectors as grad_dot's), so
-// the weighted sum adds or subtracts the weight instead of multiplying.
+// likewise for y and z, with fade'(t) = 30 t^2 (t - 1)^2.  A corner's
+// gradient vector is s1 e_op1 + s2 e_op2 (grad_dot's operands and signs), so
+// the weighted sum adds the signed weight to the operands' components
+// instead of multiplying.
 template <class PT>
 __device__ __forceinline__ V3 perlin_grad(const PT& P, float x, float y, float z) {
   float fx = floorf(x), fy = floorf(y), fz = floorf(z);
@@ -196,14 +206,13 @@ __device__ __forceinline__ V3 perlin_grad(const PT& P, float x, float y, float z
   float sx = 0.f, sy = 0.f, sz = 0.f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    // gradient vector components by case: x +1 for cases 0 2 4 6 12, -1
-    // for 1 3 5 7 13; y +1 for 0 1 8 10 12 13, -1 for 2 3 9 11 14 15; z +1
-    // for 4 5 8 9 14, -1 for 6 7 10 11 15
     const uint32_t gk = G[k];
-    const float ck = cw[k];
-    sx += (gk & (0x1055u << 16)) ? ck : ((gk & (0x20AAu << 16)) ? -ck : 0.0f);
-    sy += (gk & (0x3503u << 16)) ? ck : ((gk & (0xCA0Cu << 16)) ? -ck : 0.0f);
-    sz += (gk & (0x4330u << 16)) ? ck : ((gk & (0x8CC0u << 16)) ? -ck : 0.0f);
+    const float c1 = __uint_as_float(__float_as_uint(cw[k]) ^ (gk & 0x80000000u));  // s1 w
+    const float c2 = (gk & 0x400u) ? -cw[k] : cw[k];                               // s2 w
+    // first operand x or y, second y or z
+    sx += (gk & 0x100u) ? 0.0f : c1;
+    sy += ((gk & 0x100u) ? c1 : 0.0f) + ((gk & 0x200u) ? c2 : 0.0f);
+    sz += (gk & 0x200u) ? 0.0f : c2;
   }
   V3 r;
   r.x = sx + du * (k1 + k4 * v + k5 * w + k7 * vw);

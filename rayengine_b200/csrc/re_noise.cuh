@@ -26,16 +26,18 @@ struct PermTable {
 // faster on the SDF march than 32 conflict-free copies (64 KB), which allow
 // one block per SM fewer.  Each
 // word holds P[j] in bits 0-7 and the gradient case h = P[j] & 15 decoded
-// for grad_dot: bit 8 set when its first operand is y (else x), bit 9 when
-// its second operand is y (else z), bit 10 when the second operand is
-// negated and bit 31 when the first one is (so that negation is an XOR of
-// the operand's sign bit with the word).
+// for grad_dot in bits 28-31: bit 28 set when its first operand is y (else
+// x), bit 29 when its second operand is y (else z), bit 30 when the second
+// operand is negated and bit 31 when the first one is (so that negation is
+// an XOR of the operand's sign bit with the word).  Bits 28-31 fall out of
+// the interleaved table's 32-bit index arithmetic (Perm::word), so chained
+// lookups use the word unmasked.
 constexpr uint32_t kPermSmemBytes = 512 * 16 * 4;
 
 __host__ __device__ __forceinline__ uint32_t perm_word(uint32_t p) {
   const uint32_t h = p & 15u;
-  return p | (((0xCF00u >> h) & 1u) << 8) | (((0x300Fu >> h) & 1u) << 9) |
-         (((0x8CCCu >> h) & 1u) << 10) | (((0xEAAAu >> h) & 1u) << 31);
+  return p | (((0xCF00u >> h) & 1u) << 28) | (((0x300Fu >> h) & 1u) << 29) |
+         (((0x8CCCu >> h) & 1u) << 30) | (((0xEAAAu >> h) & 1u) << 31);
 }
 
 __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
@@ -48,8 +50,11 @@ __device__ __forceinline__ void load_perm(const PermTable& t, uint32_t* s) {
 struct Perm {
   const uint32_t* __restrict__ s;
   uint32_t lane;
+  // j may carry a word's bits 28-31: the 32-bit shift drops them, and the
+  // rest (an index below 512) stays inside the 8192-word table
   __device__ __forceinline__ uint32_t word(uint32_t j) const { return s[(j << 4) + lane]; }
-  __device__ __forceinline__ uint32_t idx(uint32_t j) const { return word(j) & 255u; }
+  // the raw word: as the next lookup's index its bits 28-31 do not count
+  __device__ __forceinline__ uint32_t idx(uint32_t j) const { return word(j); }
   __device__ __forceinline__ uint32_t grad(uint32_t j) const { return word(j); }
 };
 
@@ -85,10 +90,10 @@ struct PermBytes {
 // by the ALU pipe, where these selects run.)
 // g: a grad() lookup.
 __device__ __forceinline__ float grad_dot(uint32_t g, float x, float y, float z) {
-  float u = (g & 0x100u) ? y : x;
+  float u = (g & 0x10000000u) ? y : x;
   u = __uint_as_float(__float_as_uint(u) ^ (g & 0x80000000u));
-  float v = (g & 0x200u) ? y : z;
-  v = (g & 0x400u) ? -v : v;
+  float v = (g & 0x20000000u) ? y : z;
+  v = (g & 0x40000000u) ? -v : v;
   return u + v;
 }
 
@@ -208,11 +213,11 @@ __device__ __forceinline__ V3 perlin_grad(const PT& P, float x, float y, float z
   for (int k = 0; k < 8; ++k) {
     const uint32_t gk = G[k];
     const float c1 = __uint_as_float(__float_as_uint(cw[k]) ^ (gk & 0x80000000u));  // s1 w
-    const float c2 = (gk & 0x400u) ? -cw[k] : cw[k];                               // s2 w
+    const float c2 = (gk & 0x40000000u) ? -cw[k] : cw[k];                          // s2 w
     // first operand x or y, second y or z
-    sx += (gk & 0x100u) ? 0.0f : c1;
-    sy += ((gk & 0x100u) ? c1 : 0.0f) + ((gk & 0x200u) ? c2 : 0.0f);
-    sz += (gk & 0x200u) ? 0.0f : c2;
+    sx += (gk & 0x10000000u) ? 0.0f : c1;
+    sy += ((gk & 0x10000000u) ? c1 : 0.0f) + ((gk & 0x20000000u) ? c2 : 0.0f);
+    sz += (gk & 0x20000000u) ? 0.0f : c2;
   }
   V3 r;
   r.x = sx + du * (k1 + k4 * v + k5 * w + k7 * vw);

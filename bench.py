@@ -697,7 +697,8 @@ class SdfFrame:
         self.nhits = int((o[:, 7] == 1).sum())
         self.shadow_evals = int(ev.item())
         self.rays_per_step = W * H + self.nhits
-        self.kernels_per_step = 2
+        # march, shadow pass, finish pass
+        self.kernels_per_step = 3
 
     def config(self):
         sh = self.shade
@@ -721,8 +722,9 @@ class SdfFrame:
     def roofline(self, phase_ms, peaks):
         evals = self.steps + 6 * self.nhits
         return fp32_roofline("sdf", evals * SDF_OPS_PER_EVAL, phase_ms["sdf"], peaks, self.name,
-                             shade_kernel={"shadow_field_evals": self.shadow_evals,
-                                           "ms": round(phase_ms["shade"], 4)})
+                             shade_kernels={"kernels": ["k_sdf_shadow", "k_sdf_finish"],
+                                            "shadow_field_evals": self.shadow_evals,
+                                            "ms": round(phase_ms["shade"], 4)})
 
     def e2e_compute(self, torch, stream):
         W, H = self.cfg.width, self.cfg.height

@@ -353,7 +353,9 @@ typedef struct re_sdf_shade_params {
 RE_API void re_sdf_shade_params_default(re_sdf_shade_params* s);
 /* The shading pass alone over a hit record from re_sdf_trace (or
  * re_nsdf_trace); d_evals (device, may be NULL) accumulates the shadow
- * rays' field evaluations. */
+ * rays' field evaluations.  Two kernels: the soft-shadow march of the lit
+ * hits, whose shadow factors d_rgba holds in between, then the paint of
+ * every pixel into d_rgba. */
 RE_API re_status re_sdf_shade(const re_sdf_params* field, const re_sdf_shade_params* shade,
                               const re_camera* cam, uint32_t w, uint32_t h,
                               const re_sdf_hit* d_hits, uint32_t* d_rgba,

@@ -279,32 +279,43 @@ __device__ __forceinline__ uint32_t finish_pixel(const ShadeDev& S, V3 col, V3 o
   return rgba8(col);
 }
 
-// Shading as a per-lane state machine over the tracer's pixel order (lane i
-// & 31 of 8x4 tile i >> 5): a lane that takes a pixel paints it; a miss
-// (sky) or an unlit frame finishes at once, a lit hit then advances its soft
-// shadow by one field evaluation per loop trip, so the lanes of a warp stay
-// on the same code while their shadow rays take different numbers of
-// steps; when at least kShadeRefill lanes are idle the warp claims that many
-// new pixels with one atomic.  Same operations, in the same order, as one
-// loop per pixel.
+// Shading in two passes over the tracer's pixel order (lane i & 31 of 8x4
+// tile i >> 5).
+//
+// k_sdf_shadow: the soft-shadow march of every lit hit, as a per-lane state
+// machine: a lane takes a pixel, a lit hit then advances its shadow ray by
+// one field evaluation per loop trip, so the lanes of a warp stay on the
+// same code while their shadow rays take different numbers of steps; when
+// at least kShadeRefill lanes are idle the warp claims that many new pixels
+// with one atomic.  The pass writes each lit hit's shadow factor (prel, as
+// float bits) into that pixel's word of the RGBA8 output, which the second
+// pass reads and overwrites.
+//
+// k_sdf_finish: one thread per pixel paints it: the surface colour, the
+// light with the shadow factor, or the atmosphere for a miss, then fog,
+// gamma, vignetting and the pack.  Neighbouring pixels take the same branch
+// (sky above the horizon, terrain below), so the warps stay converged; in
+// one fused state machine the sky's 32 x 8 in-scattering samples and the
+// surface shading of a refilled lane ran while the rest of its warp waited.
+//
+// Same operations, in the same order per pixel, as one loop per pixel.
 constexpr uint32_t kShadeRefill = 4;
 
-__global__ void __launch_bounds__(256) k_sdf_shade(PermTable perm, ShadeDev S, CamDev cam,
-                                                   uint32_t w, uint32_t h,
-                                                   const float4* __restrict__ hits,
-                                                   uint32_t* __restrict__ rgba,
-                                                   uint32_t* __restrict__ cursor,
-                                                   unsigned long long* __restrict__ evals_out) {
+__global__ void __launch_bounds__(256) k_sdf_shadow(PermTable perm, ShadeDev S, uint32_t w,
+                                                    uint32_t h, const float4* __restrict__ hits,
+                                                    uint32_t* __restrict__ rgba,
+                                                    uint32_t* __restrict__ cursor,
+                                                    unsigned long long* __restrict__ evals_out) {
   extern __shared__ uint32_t perm_smem[];
   load_perm(perm, perm_smem);
   Perm P = perm_view(perm_smem);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t tiles_x = (w + 7) / 8;
   const uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
-  const bool lit = (S.flags & RE_SDF_SHADE) != 0u;
   bool live = false, exhausted = false;
-  uint32_t x = 0, y = 0, i = 0, evals = 0;
-  V3 p = {0.f, 0.f, 0.f}, n = p, L = p, col = p;
+  uint32_t i = 0, evals = 0;
+  size_t pix = 0;
+  V3 p = {0.f, 0.f, 0.f}, L = p;
   float ldx = 0.f, ldz = 0.f, t = 0.f, prel = 0.f;
   for (;;) {
     uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
@@ -317,29 +328,18 @@ __global__ void __launch_bounds__(256) k_sdf_shade(PermTable perm, ShadeDev S, C
       if (!live) {
         uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
         uint32_t tile = k >> 5, l = k & 31u;
-        x = (tile % tiles_x) * 8 + (l & 7u);
-        y = (tile / tiles_x) * 4 + (l >> 3);
+        uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
         if (k < total && x < w && y < h) {
-          size_t pix = (size_t)y * w + x;
-          float4 r0 = __ldg(&hits[2 * pix]), r1 = __ldg(&hits[2 * pix + 1]);
-          V3 o, d;
-          generate_ray(cam, w, h, x, y, o, d);
-          float u = (float)x / (float)w, v = (float)y / (float)h;
+          pix = (size_t)y * w + x;
+          float4 r1 = __ldg(&hits[2 * pix + 1]);
           if (__float_as_uint(r1.w) == 1u) {
+            float4 r0 = __ldg(&hits[2 * pix]);
             p = v3(r0.x, r0.y, r0.z);
-            n = v3(r0.w, r1.x, r1.y);
-            col = paint(P, S, p, n);
-            if (lit) {
-              light_setup(S, p, L, ldx, ldz);
-              t = S.shadow_tmin;
-              prel = 1.0f;
-              i = 0;
-              live = true;
-            } else {
-              rgba[pix] = finish_pixel(S, col, o, d, vlen(sub(p, o)), u, v);
-            }
-          } else {
-            rgba[pix] = finish_pixel(S, sky(S, d), o, d, kInf, u, v);
+            light_setup(S, p, L, ldx, ldz);
+            t = S.shadow_tmin;
+            prel = 1.0f;
+            i = 0;
+            live = true;
           }
         }
       }
@@ -349,18 +349,54 @@ __global__ void __launch_bounds__(256) k_sdf_shade(PermTable perm, ShadeDev S, C
       continue;
     }
     if (live && !shadow_step(P, S, p, L, t, prel, i, evals)) {
-      V3 pc = light_terms(S, prel, n, L, ldx, ldz);
-      V3 o, d;
-      generate_ray(cam, w, h, x, y, o, d);
-      rgba[(size_t)y * w + x] =
-          finish_pixel(S, v3(col.x * pc.x, col.y * pc.y, col.z * pc.z), o, d, vlen(sub(p, o)),
-                       (float)x / (float)w, (float)y / (float)h);
+      rgba[pix] = __float_as_uint(prel);
       live = false;
     }
   }
   if (evals_out) {
     uint32_t s = __reduce_add_sync(0xFFFFFFFFu, evals);
     if (lane == 0) atomicAdd(evals_out, (unsigned long long)s);
+  }
+}
+
+// The second pass; the permutation table (for the snow band's noise) as one
+// word copy per entry: a pixel reads it at most once.
+__global__ void __launch_bounds__(256) k_sdf_finish(PermTable perm, ShadeDev S, CamDev cam,
+                                                    uint32_t w, uint32_t h,
+                                                    const float4* __restrict__ hits,
+                                                    uint32_t* __restrict__ rgba) {
+  __shared__ uint32_t words[512];
+  for (uint32_t j = threadIdx.x; j < 512u; j += blockDim.x) words[j] = perm_word(perm.p[j]);
+  __syncthreads();
+  PermWords P{words};
+  const bool lit = (S.flags & RE_SDF_SHADE) != 0u;
+  const uint32_t tiles_x = (w + 7) / 8;
+  const uint32_t total = tiles_x * ((h + 3) / 4) * 32u;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += gridDim.x * blockDim.x) {
+    uint32_t tile = k >> 5, l = k & 31u;
+    uint32_t x = (tile % tiles_x) * 8 + (l & 7u), y = (tile / tiles_x) * 4 + (l >> 3);
+    if (x >= w || y >= h) continue;
+    size_t pix = (size_t)y * w + x;
+    float4 r1 = __ldg(&hits[2 * pix + 1]);
+    V3 o, d;
+    generate_ray(cam, w, h, x, y, o, d);
+    float u = (float)x / (float)w, v = (float)y / (float)h;
+    if (__float_as_uint(r1.w) == 1u) {
+      float4 r0 = __ldg(&hits[2 * pix]);
+      V3 p = v3(r0.x, r0.y, r0.z), n = v3(r0.w, r1.x, r1.y);
+      V3 col = paint(P, S, p, n);
+      if (lit) {
+        V3 L;
+        float ldx, ldz;
+        light_setup(S, p, L, ldx, ldz);
+        V3 pc = light_terms(S, __uint_as_float(rgba[pix]), n, L, ldx, ldz);
+        col = v3(col.x * pc.x, col.y * pc.y, col.z * pc.z);
+      }
+      rgba[pix] = finish_pixel(S, col, o, d, vlen(sub(p, o)), u, v);
+    } else {
+      rgba[pix] = finish_pixel(S, sky(S, d), o, d, kInf, u, v);
+    }
   }
 }
 
@@ -437,18 +473,29 @@ re_status shade(const re_sdf_params& f, const re_sdf_shade_params& s, const re_c
   cd.horizontal = {b.horizontal[0], b.horizontal[1], b.horizontal[2]};
   cd.vertical = {b.vertical[0], b.vertical[1], b.vertical[2]};
   cd.focal = b.focal;
-  RE_CUDA(cudaMemsetAsync(ctr, 0, 4, st));
-  RE_CUDA(cudaFuncSetAttribute(k_sdf_shade, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kPermSmemBytes));
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sdf_shade, 256, kPermSmemBytes) !=
+  if (s.flags & RE_SDF_SHADE) {
+    RE_CUDA(cudaMemsetAsync(ctr, 0, 4, st));
+    RE_CUDA(cudaFuncSetAttribute(k_sdf_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPermSmemBytes));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sdf_shadow, 256,
+                                                      kPermSmemBytes) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    k_sdf_shadow<<<per_sm * sm_count(), 256, kPermSmemBytes, st>>>(
+        perm_table(f.seed), shade_dev(f, s), w, h, reinterpret_cast<const float4*>(d_hits),
+        d_rgba, ctr, reinterpret_cast<unsigned long long*>(d_evals));
+    RE_CHECK_LAUNCH("re_render_sdf_frame: shadow launch");
+  }
+  int fin_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fin_sm, k_sdf_finish, 256, 0) !=
           cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  k_sdf_shade<<<per_sm * sm_count(), 256, kPermSmemBytes, st>>>(
+      fin_sm < 1)
+    fin_sm = 1;
+  k_sdf_finish<<<fin_sm * sm_count(), 256, 0, st>>>(
       perm_table(f.seed), shade_dev(f, s), cd, w, h, reinterpret_cast<const float4*>(d_hits),
-      d_rgba, ctr, reinterpret_cast<unsigned long long*>(d_evals));
-  RE_CHECK_LAUNCH("re_render_sdf_frame: shade launch");
+      d_rgba);
+  RE_CHECK_LAUNCH("re_render_sdf_frame: finish launch");
   return RE_OK;
 }
 

@@ -837,7 +837,7 @@ class NeuralTerrainSDF:
                              "final_l1_loss": round(self.final_loss, 5)},
                 "trace_params": {"lipschitz": round(self.tp.lipschitz, 4),
                                  "lipschitz_quantile": n.lipschitz_quantile,
-                                 "safety": n.safety, "switch_dist": n.switch_dist,
+                                 "safety": n.cone_safety, "switch_dist": n.switch_dist,
                                  "min_step": n.min_step, "max_network_steps": n.max_network_steps,
                                  "root_steps": n.root_steps, "cone_tile": n.cone_tile,
                                  "cone_lanes": n.cone_lanes, "relax": n.relax,

@@ -418,7 +418,7 @@ typedef struct re_nsdf_trace_params {
   uint32_t normal_taps; /* 0 or 6: central differences; 4: tetrahedral;   */
                         /* 1: the exact field's analytic gradient, in a   */
                         /* second pass over the hits                      */
-  uint32_t cone_lanes;  /* 0 or 1, 2, 4, 8: lanes per cone; above 1 they   */
+  uint32_t cone_lanes;  /* 0 or 1, 2, 4, 8, 16: lanes per cone; above 1   */
                         /* evaluate successive guessed steps in one pass   */
   float root_tol;       /* > 0: the root search ends when its next secant  */
                         /* point moves less than this (scene units)        */

@@ -169,10 +169,13 @@ class NeuralTerrainConfig:
     lipschitz_samples: int = 200000
     lipschitz_h: float = 1e-2
     lipschitz_quantile: float = 0.5
-    # Network phase: one cone per 16x16 pixel tile, 8 lanes per cone
-    # evaluating guessed successive steps in one pass (measured on B200,
-    # 1080p, 20k-step network: cone + exact phase 3.21 ms against 7.62 ms
-    # for the per-ray network march below; the exact tracer 4.17 ms).
+    # Network phase: one cone per 16x16 pixel tile, 16 lanes per cone
+    # evaluating guessed successive steps in one pass, each step safety
+    # `cone_safety` / L (measured on B200, 1080p, 20k-step network: cone +
+    # exact phase 3.21 ms against 7.62 ms for the per-ray network march
+    # below, the exact tracer then 4.17 ms; on the faster field 2.12 ms
+    # with 16 lanes and safety 1.5 against 2.19 ms with 8 lanes and 1.2,
+    # same median error, p95 and silhouettes).
     # Exact phase from the cone's stop: the exact tracer's steps allowed to
     # grow 1.5x along the secant of the last two samples (median hit error
     # 8e-5, ~850 of 2.07M pixels whose hit/miss differs from the exact
@@ -180,13 +183,14 @@ class NeuralTerrainConfig:
     # relax 2.0: 2.94 ms, 2,100 pixels, median error 4e-4); the root search
     # ends when its secant point moves less than 1e-4 (3.23 -> 3.17 ms, same
     # median error).
-    safety: float = 1.2
+    safety: float = 1.2          # the per-ray network march's step safety
+    cone_safety: float = 1.5
     switch_dist: float = 0.3
     min_step: float = 0.05
     max_network_steps: int = 64
     root_steps: int = 4
     cone_tile: int = 16
-    cone_lanes: int = 8
+    cone_lanes: int = 16
     relax: float = 1.5
     root_tol: float = 1e-4
     # the normal: the exact field's analytic gradient at the hit, in a
@@ -229,7 +233,7 @@ class NeuralTerrainConfig:
 
     def trace_params(self, lipschitz):
         """The cone tracer's settings (the default method)."""
-        return api.nsdf_trace_params(lipschitz, self.safety, self.switch_dist, self.min_step,
+        return api.nsdf_trace_params(lipschitz, self.cone_safety, self.switch_dist, self.min_step,
                                      self.max_network_steps, 0, self.root_steps, self.relax,
                                      cone_tile=self.cone_tile, cone_lanes=self.cone_lanes,
                                      normal_taps=self.normal_taps, root_tol=self.root_tol)

@@ -1162,7 +1162,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nsdf_cone(InputMap m,
                                                              unsigned long long* __restrict__ totals,
                                                              float* __restrict__ tile_t,
                                                              int* __restrict__ err) {
-  static_assert(K == 1 || K == 2 || K == 4 || K == 8, "lanes per cone: 1, 2, 4 or 8");
+  static_assert(K == 1 || K == 2 || K == 4 || K == 8 || K == 16,
+                "lanes per cone: 1, 2, 4, 8 or 16");
   extern __shared__ unsigned char smem_raw[];
   TcSmem& s = tc_smem(smem_raw);
   tc_setup(s, pack);
@@ -2166,8 +2167,8 @@ re_status trace_check(re_nsdf* s, const re_sdf_params* field, const re_nsdf_trac
   if (tp->normal_taps != 0 && tp->normal_taps != 1 && tp->normal_taps != 4 &&
       tp->normal_taps != 6)
     return fail(RE_ERR_INVALID_ARG, "%s: normal_taps 0, 1, 4 or 6", fn);
-  if (tp->cone_lanes > 8 || (tp->cone_lanes & (tp->cone_lanes - 1u)))
-    return fail(RE_ERR_INVALID_ARG, "%s: cone_lanes 0, 1, 2, 4 or 8", fn);
+  if (tp->cone_lanes > 16 || (tp->cone_lanes & (tp->cone_lanes - 1u)))
+    return fail(RE_ERR_INVALID_ARG, "%s: cone_lanes 0, 1, 2, 4, 8 or 16", fn);
   return RE_OK;
 }
 }  // namespace
@@ -2222,7 +2223,8 @@ RE_API re_status re_nsdf_trace_network(re_nsdf* s, const re_sdf_params* field,
   }
   if (cone) {
     const uint32_t K = tp->cone_lanes ? tp->cone_lanes : 1u;
-    auto kc = K == 8u   ? re::nsdf::k_nsdf_cone<8>
+    auto kc = K == 16u  ? re::nsdf::k_nsdf_cone<16>
+              : K == 8u ? re::nsdf::k_nsdf_cone<8>
               : K == 4u ? re::nsdf::k_nsdf_cone<4>
               : K == 2u ? re::nsdf::k_nsdf_cone<2>
                         : re::nsdf::k_nsdf_cone<1>;

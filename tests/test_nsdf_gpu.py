@@ -232,7 +232,7 @@ def test_trace_parameter_checks(cuda):
         field, cam = tc.params(), tc.camera()
         bad = [dict(cone_tile=8, cone_coarse=12), dict(cone_tile=8, cone_coarse=8),
                dict(cone_tile=0, cone_coarse=32), dict(cone_tile=300),
-               dict(cone_tile=8, cone_lanes=3), dict(cone_tile=8, cone_lanes=16),
+               dict(cone_tile=8, cone_lanes=3), dict(cone_tile=8, cone_lanes=32),
                dict(normal_taps=5)]
         for kw in bad:
             with pytest.raises(rb.RayEngineError):

@@ -8,7 +8,7 @@ cosine-weighted AO rays (length 1) per primary hit.  Metric: Mrays/s over all
 rays traced in the frame.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config heightfield_ao|soup|soup1m|terrain_sdf|nsdf_terrain|batch32]
+                    [--config heightfield_ao|soup|soup1m|soup1m_2k|terrain_sdf|sdf_frame|nsdf_terrain|batch32]
                     [--tree tuned|configured]
 
 The mesh workloads run over the library's B200-tuned kd-tree; the same
@@ -467,15 +467,16 @@ class HeightfieldAO:
 class SoupPrimary:
     name = "soup"
 
-    def __init__(self, torch, num_tris=65536, tree="tuned", packed=None):
+    def __init__(self, torch, num_tris=65536, tree="tuned", packed=None, size=512):
         import rayengine_b200 as rb
 
         self.rb = rb
         self.tree = tree
         self.num_tris = num_tris
+        self.size = size
         if num_tris == 1 << 20:
-            self.name = "soup1m"
-        self.cfg = cfg = rb.configs.SoupConfig(num_tris=num_tris)
+            self.name = "soup1m" if size == 512 else f"soup1m_{size // 1024}k"
+        self.cfg = cfg = rb.configs.SoupConfig(num_tris=num_tris, width=size, height=size)
         self.packed = cfg.packed() if packed is None else packed
         if tree == "configured":
             self.kd = cfg.kd_params()
@@ -529,7 +530,8 @@ class SoupPrimary:
         if self.tree == "configured" or (self.kd.max_depth, self.kd.leaf_size) == (
                 CONFIGURED_TREE["max_depth"], CONFIGURED_TREE["leaf_size"]):
             return None  # the headline already runs the configured tree
-        return SoupPrimary(torch, self.num_tris, tree="configured", packed=self.packed)
+        return SoupPrimary(torch, self.num_tris, tree="configured", packed=self.packed,
+                           size=self.size)
 
     def parity(self):
         from oracle import pyoracle as po
@@ -1139,6 +1141,8 @@ def reference_workload(name):
                 "rays per hit")
     else:
         cfg = C.SoupConfig(num_tris=(1 << 20) if name.startswith("soup1m") else 65536)
+        if name == "soup1m_2k":
+            cfg.width = cfg.height = 2048
         tri = po.soup(cfg.seed, cfg.num_tris)
         verts = tri.reshape(-1, 3)
         faces = np.arange(verts.shape[0], dtype=np.uint32).reshape(-1, 3)
@@ -1204,12 +1208,15 @@ def reference_workload(name):
     return desc, built_by, "reference", make_step(sah_tree), as_shipped
 
 
-TREE_WORKLOADS = ("heightfield_ao", "soup", "soup1m")
+TREE_WORKLOADS = ("heightfield_ao", "soup", "soup1m", "soup1m_2k")
 
 WORKLOADS = {
     "heightfield_ao": HeightfieldAO,
     "soup": SoupPrimary,
     "soup1m": lambda torch, **kw: SoupPrimary(torch, num_tris=1 << 20, **kw),
+    # the same scene and camera at 2048x2048: a frame with enough rays to
+    # fill the GPU (the 512x512 frame is shorter than its longest walks)
+    "soup1m_2k": lambda torch, **kw: SoupPrimary(torch, num_tris=1 << 20, size=2048, **kw),
     "terrain_sdf": TerrainSDF,
     "sdf_frame": SdfFrame,
     "nsdf_terrain": NeuralTerrainSDF,

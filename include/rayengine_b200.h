@@ -157,6 +157,15 @@ RE_API re_status re_scene_stats_get(const re_scene* s, re_scene_stats* out);
  * be NULL; sizes come from re_scene_stats. */
 RE_API re_status re_scene_export(const re_scene* s, uint32_t* nodes,
                                  uint32_t* leaves, float* tris);
+/* The entry table (for checking): *res = cells per face side; when out is
+ * not NULL it receives 6 * res * res start nodes, entry (k, side, i, j) at
+ * ((k * 2 + side) * res + i) * res + j for the face of axis k (side 0: -k,
+ * 1: +k), cell i along the face's lower other axis and j along the higher.
+ * Each is the deepest node whose region holds the cell grown by 1e-4 x the
+ * scene box's largest extent; primary and caller rays that enter the box
+ * through a cell start their first descent there (the counting calls start
+ * at the root). */
+RE_API re_status re_scene_export_entry(const re_scene* s, uint32_t* out, uint32_t* res);
 RE_API re_status re_scene_destroy(re_scene* s);
 
 /* Primary rays for every pixel of a w x h image (row-major, d_out has w*h

@@ -235,6 +235,7 @@ _SIGS = {
     "re_scene_build_host": (ctypes.c_int, [_P, _U32, ctypes.POINTER(re_kd_params), ctypes.POINTER(_P)]),
     "re_scene_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(re_scene_stats)]),
     "re_scene_export": (ctypes.c_int, [_P, _P, _P, _P]),
+    "re_scene_export_entry": (ctypes.c_int, [_P, _P, _P]),
     "re_scene_destroy": (ctypes.c_int, [_P]),
     "re_trace_primary": (ctypes.c_int, [_P, ctypes.POINTER(re_camera), _U32, _U32, _U32, _P, _P]),
     "re_trace_rays": (ctypes.c_int, [_P, _P, _U32, _U32, _P, _P]),

@@ -228,6 +228,17 @@ class KDScene:
         call("re_scene_export", self._h, nodes.ctypes.data, leaves.ctypes.data, tris.ctypes.data)
         return nodes, leaves, tris
 
+    def export_entry(self):
+        """The entry table: uint32 (3, 2, res, res) start nodes per face
+        (axis k, side 0 = -k / 1 = +k) and cell (i along the face's lower
+        other axis, j along the higher)."""
+        res = ctypes.c_uint32()
+        call("re_scene_export_entry", self._h, None, ctypes.byref(res))
+        r = res.value
+        out = np.empty((3, 2, r, r), np.uint32)
+        call("re_scene_export_entry", self._h, out.ctypes.data, ctypes.byref(res))
+        return out
+
     def trace_primary(self, cam: RCamera, w: int, h: int, flags: int = TRACE_TWO_SIDED,
                       out=None, stream=None):
         """Closest hits for every pixel -> int32 CUDA tensor (h*w, 4) = re_hit."""

@@ -332,6 +332,58 @@ void link_ropes(BNode* n, BNode* const r[6]) {
 
 }  // namespace
 
+// The entry table of FlatTree (kd_build.hpp): per face cell, descend from
+// the root while the cell, grown by the margin, lies strictly on one side of
+// the split (on the face's own axis the cell is the face plane itself).
+void build_entry_table(FlatTree& t) {
+  const uint32_t R = kEntryRes;
+  t.entry.assign(6u * R * R, 0u);
+  double lo_box[3], ext[3], emax = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    lo_box[k] = t.bmin[k];
+    ext[k] = (double)t.bmax[k] - (double)t.bmin[k];
+    emax = std::max(emax, ext[k]);
+  }
+  const double m = 1e-4 * emax;
+  auto split_of = [&](uint32_t n) {
+    float f;
+    std::memcpy(&f, &t.nodes[2 * (size_t)n], 4);
+    return (double)f;
+  };
+#pragma omp parallel for schedule(static)
+  for (int face = 0; face < 6; ++face) {
+    const int k = face >> 1, side = face & 1;
+    const int a = k == 0 ? 1 : 0, b = k == 2 ? 1 : 2;
+    const double f = side ? (double)t.bmax[k] : (double)t.bmin[k];
+    for (uint32_t i = 0; i < R; ++i) {
+      for (uint32_t j = 0; j < R; ++j) {
+        double lo[3], hi[3];
+        lo[a] = lo_box[a] + ext[a] * i / R - m;
+        hi[a] = lo_box[a] + ext[a] * (i + 1) / R + m;
+        lo[b] = lo_box[b] + ext[b] * j / R - m;
+        hi[b] = lo_box[b] + ext[b] * (j + 1) / R + m;
+        lo[k] = f - m;
+        hi[k] = f + m;
+        uint32_t node = 0;
+        for (;;) {
+          const uint32_t meta = t.nodes[2 * (size_t)node + 1];
+          const uint32_t axis = meta & 3u;
+          if (axis == 3u) break;
+          const double s = split_of(node);
+          if (hi[axis] < s) {
+            node = meta >> 2;
+          } else if (lo[axis] > s) {
+            node = (meta >> 2) + 1u;
+          } else {
+            break;
+          }
+        }
+        t.entry[((size_t)face * R + i) * R + j] = node;
+      }
+    }
+  }
+}
+
 bool build_kdtree(const float* tris, uint32_t num_tris, const re_kd_params& params,
                   FlatTree& out, const char** err) {
   auto t0 = std::chrono::steady_clock::now();
@@ -511,6 +563,7 @@ bool build_kdtree(const float* tris, uint32_t num_tris, const re_kd_params& para
   out.max_leaf_size = maxleaf;
   out.bfs_nodes = bfs_nodes;
   free_tree(tree);
+  build_entry_table(out);
   out.build_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return true;

@@ -24,10 +24,22 @@
 
 namespace re {
 
+// Entry table: for each face of the root box (axis k, side 0 = the -k face,
+// 1 = the +k face) a kEntryRes x kEntryRes grid of cells over the face's
+// other two axes (a < b, cell i along a, j along b), each holding the
+// deepest node whose region contains the whole cell grown by a margin of
+// 1e-4 x the box's largest extent.  A ray that enters the root box through
+// that cell of that face starts its first descent there: at every node
+// above, its entry point lies farther from the split plane than rounding
+// can move it, so the root descent takes the same path to that node.
+// Entry (k, side, i, j) is at ((k * 2 + side) * kEntryRes + i) * kEntryRes + j.
+constexpr uint32_t kEntryRes = 128;
+
 struct FlatTree {
   std::vector<uint32_t> nodes;   // 2 words per node
   std::vector<uint32_t> leaves;  // 16 words per leaf
   std::vector<float> tris;       // 12 words per reference
+  std::vector<uint32_t> entry;   // 6 * kEntryRes^2 start nodes
   float bmin[3], bmax[3];
   uint32_t num_tris = 0, num_nodes = 0, num_leaves = 0, num_refs = 0;
   uint32_t max_depth = 0, max_leaf_size = 0, bfs_nodes = 0;

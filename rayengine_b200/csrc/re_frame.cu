@@ -152,6 +152,16 @@ KdDev kd_of_scene(const re_scene* s) {
   kd.max_visits = s->max_visits;
   kd.stage = s->stage;
   kd.trunc = s->d_counters + RE_SCENE_TRUNC_SLOT;
+  if (s->d_entry) {
+    kd.entry = s->d_entry;
+    kd.entry_res = kEntryRes;
+    float sc[3];
+    for (int k = 0; k < 3; ++k) {
+      const float ext = s->host.bmax[k] - s->host.bmin[k];
+      sc[k] = ext > 0.f ? (float)kEntryRes / ext : 0.f;
+    }
+    kd.entry_scale = {sc[0], sc[1], sc[2]};
+  }
   return kd;
 }
 

@@ -30,6 +30,12 @@ struct KdDev {
   // triangle slots in `tris`; lanes that share a ray fetch their first
   // triangle of a leaf before its record only below this bound (0: never)
   uint32_t num_refs = 0;
+  // start nodes of rays entering the root box through a face (the host's
+  // entry table: 6 faces x entry_res^2 cells; null: every walk starts at the
+  // root).  entry_scale = entry_res / extent per axis.
+  const uint32_t* __restrict__ entry = nullptr;
+  uint32_t entry_res = 0;
+  V3 entry_scale = {0.f, 0.f, 0.f};
 };
 
 // Trav::visits of a walk that stopped at the leaf-visit cap.
@@ -124,8 +130,36 @@ __device__ __forceinline__ bool origin_in_leaf(const KdDev& kd, V3 o, uint32_t s
   return o.x >= A.x && o.x <= A.w && o.y >= A.y && o.y <= B.x && o.z >= A.z && o.z <= B.y;
 }
 
+// The node a ray entering the root box at t_entry > 0 starts its first
+// descent from: the entry table's cell of the face it entered through (the
+// axis whose slab it entered last; the -k face when it moves in +k).  The
+// table was built so that every entry point in a cell takes the root
+// descent's path down to the cell's node, so the walk (and every hit) is
+// that of a descent from the root.  0 (the root) without a table or for an
+// origin inside the box.
+__device__ __forceinline__ uint32_t entry_node(const KdDev& kd, V3 o, V3 d, V3 inv,
+                                               float t_entry) {
+  if (kd.entry == nullptr || !(t_entry > 0.0f)) return 0u;
+  const float nx = fminf((kd.bmin.x - o.x) * inv.x, (kd.bmax.x - o.x) * inv.x);
+  const float ny = fminf((kd.bmin.y - o.y) * inv.y, (kd.bmax.y - o.y) * inv.y);
+  const float nz = fminf((kd.bmin.z - o.z) * inv.z, (kd.bmax.z - o.z) * inv.z);
+  const uint32_t k = (nx >= ny && nx >= nz) ? 0u : (ny >= nz ? 1u : 2u);
+  const uint32_t side = comp(d, k) > 0.0f ? 0u : 1u;
+  // the face's axes a < b
+  const uint32_t a = k == 0u ? 1u : 0u, b = k == 2u ? 1u : 2u;
+  const float lim = (float)(kd.entry_res - 1u);
+  const float pa = __fmaf_rn(t_entry, comp(d, a), comp(o, a));
+  const float pb = __fmaf_rn(t_entry, comp(d, b), comp(o, b));
+  const float fa = fminf(fmaxf((pa - comp(kd.bmin, a)) * comp(kd.entry_scale, a), 0.0f), lim);
+  const float fb = fminf(fmaxf((pb - comp(kd.bmin, b)) * comp(kd.entry_scale, b), 0.0f), lim);
+  const uint32_t i = (uint32_t)fa, j = (uint32_t)fb;
+  return __ldg(&kd.entry[((k * 2u + side) * kd.entry_res + i) * kd.entry_res + j]);
+}
+
 // CHECKED false: the caller has already established origin_in_leaf(start)
 // (or passes start 0), so the walk begins at `start` without loading it.
+// CHECKED true: a start leaf the origin is not in, or start 0, begins at the
+// entry table's node (entry_node).
 template <bool CHECKED = true>
 __device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, float tmax,
                                           uint32_t start) {
@@ -146,6 +180,7 @@ __device__ __forceinline__ void trav_init(Trav& s, const KdDev& kd, V3 o, V3 d, 
   s.live = s.t_entry < s.best_t;
   if (CHECKED) {
     if (s.live && start != 0 && origin_in_leaf(kd, o, start)) s.node = start;
+    else if (s.live) s.node = entry_node(kd, o, d, s.inv, s.t_entry);
   } else {
     s.node = start;
   }

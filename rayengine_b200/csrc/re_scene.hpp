@@ -17,6 +17,7 @@ struct re_scene {
   uint2* d_nodes = nullptr;
   float4* d_leaves = nullptr;
   float4* d_tris = nullptr;
+  uint32_t* d_entry = nullptr;  // the host's entry table (FlatTree::entry)
   // [0] tile cursor, [1] queue size, [2] queue cursor, [3] secondary rays,
   // [RE_SCENE_TRUNC_SLOT] rays of the last trace call stopped at the
   // leaf-visit cap; every trace call clears the first RE_SCENE_RESET_BYTES

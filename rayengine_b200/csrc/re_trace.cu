@@ -525,6 +525,16 @@ KdDev kd_view(const re_scene* s) {
   kd.stage = s->stage;
   kd.trunc = s->d_counters + RE_SCENE_TRUNC_SLOT;
   kd.num_refs = s->host.num_refs;
+  if (s->d_entry) {
+    kd.entry = s->d_entry;
+    kd.entry_res = kEntryRes;
+    float sc[3];
+    for (int k = 0; k < 3; ++k) {
+      const float ext = s->host.bmax[k] - s->host.bmin[k];
+      sc[k] = ext > 0.f ? (float)kEntryRes / ext : 0.f;
+    }
+    kd.entry_scale = {sc[0], sc[1], sc[2]};
+  }
   return kd;
 }
 
@@ -566,6 +576,10 @@ re_status upload(re_scene* s) {
   RE_CUDA(cudaMalloc(&s->d_leaves, h.leaves.size() * 4));
   RE_CUDA(cudaMalloc(&s->d_tris, h.tris.size() * 4));
   RE_CUDA(cudaMalloc(&s->d_counters, 64));
+  if (!h.entry.empty()) {
+    RE_CUDA(cudaMalloc(&s->d_entry, h.entry.size() * 4));
+    RE_CUDA(cudaMemcpy(s->d_entry, h.entry.data(), h.entry.size() * 4, cudaMemcpyHostToDevice));
+  }
   RE_CUDA(cudaMemcpy(s->d_nodes, h.nodes.data(), h.nodes.size() * 4, cudaMemcpyHostToDevice));
   RE_CUDA(cudaMemcpy(s->d_leaves, h.leaves.data(), h.leaves.size() * 4, cudaMemcpyHostToDevice));
   RE_CUDA(cudaMemcpy(s->d_tris, h.tris.data(), h.tris.size() * 4, cudaMemcpyHostToDevice));
@@ -589,6 +603,7 @@ void release(re_scene* s) {
   cudaFree(s->d_nodes);
   cudaFree(s->d_leaves);
   cudaFree(s->d_tris);
+  cudaFree(s->d_entry);
   cudaFree(s->d_counters);
   cudaFree(s->d_queue);
   delete s;
@@ -643,6 +658,8 @@ template <int MODE, bool COUNT>
 re_status launch_primary(re_scene* s, const re_camera& cam, uint32_t w, uint32_t h, re_hit* out,
                          uint4* counts, cudaStream_t st) {
   KdDev kd = kd_view(s);
+  // the counting walk descends from the root, as the oracle's does
+  if (COUNT) kd.entry = nullptr;
   CamDev cd = cam_view(cam);
   size_t smem = kd.stage * sizeof(uint2);
   uint32_t refill = s->tune.ray_refill_min, lanes = COUNT ? 1u : s->tune.ray_lanes;
@@ -773,6 +790,13 @@ RE_API re_status re_scene_export(const re_scene* s, uint32_t* nodes, uint32_t* l
   return RE_OK;
 }
 
+RE_API re_status re_scene_export_entry(const re_scene* s, uint32_t* out, uint32_t* res) {
+  if (!s || !res) return re::fail(RE_ERR_INVALID_ARG, "re_scene_export_entry: bad arguments");
+  *res = re::kEntryRes;
+  if (out) std::memcpy(out, s->host.entry.data(), s->host.entry.size() * 4);
+  return RE_OK;
+}
+
 RE_API re_status re_scene_destroy(re_scene* s) {
   re::release(s);
   return RE_OK;
@@ -870,6 +894,8 @@ re_status ao_primary(re_scene* s, const CamDev& cd, const AoDev& ao, uint32_t w,
                      re_hit* d_primary, uint32_t* d_mask, unsigned long long* totals,
                      cudaStream_t st) {
   KdDev kd = kd_view(s);
+  // the counting walk descends from the root, as the oracle's does
+  if (COUNT) kd.entry = nullptr;
   size_t smem = kd.stage * sizeof(uint2);
   RE_CUDA(cudaMemsetAsync(s->d_counters, 0, RE_SCENE_RESET_BYTES, st));
   auto k = k_ao_primary<COUNT>;

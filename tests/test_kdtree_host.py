@@ -189,3 +189,121 @@ def test_leaf_visit_cap_sets_status():
     cam = rb.build_camera((0, 0, 3), (0, 0, 0), (60, 60))
     h, c = po.primary_kd(kd, cam, 64, 64, max_visits=2, counts=True)
     assert c["status"].max() == 1 and c["leaf"].max() <= 2
+
+
+def _first_leaf(nodes, start, o, d, inv, te):
+    """The device's descent (float32): from `start` down to a leaf, split
+    decisions on the ray parameter (re_kd.cuh trav_step)."""
+    split = nodes[:, 0].view(np.float32)
+    meta = nodes[:, 1]
+    node = start.astype(np.int64).copy()
+    act = np.ones(len(node), bool)
+    while act.any():
+        idx = np.nonzero(act)[0]
+        mm = meta[node[idx]]
+        leaf = (mm & 3) == 3
+        act[idx[leaf]] = False
+        idx, mm = idx[~leaf], mm[~leaf]
+        if len(idx) == 0:
+            break
+        k = (mm & 3).astype(np.int64)
+        sp = split[node[idx]]
+        ok, dk, ik = o[idx, k], d[idx, k], inv[idx, k]
+        with np.errstate(invalid="ignore", over="ignore"):
+            ts = ((sp - ok) * ik).astype(np.float32)
+            left = np.where(dk > 0, te[idx] < ts, np.where(dk < 0, te[idx] >= ts, ok < sp))
+        node[idx] = (mm >> 2).astype(np.int64) + np.where(left, 0, 1)
+    return node
+
+
+def _entry_start(table, st, o, d, inv, te):
+    """entry_node (re_kd.cuh) in float32: face of the last-entered slab, the
+    cell of the entry point, the table's node."""
+    res = table.shape[-1]
+    bmin = np.array(st["bmin"], np.float32)
+    bmax = np.array(st["bmax"], np.float32)
+    ext = bmax - bmin
+    scale = np.where(ext > 0, np.float32(res) / ext, 0).astype(np.float32)
+    with np.errstate(invalid="ignore", over="ignore"):
+        near = np.minimum((bmin - o) * inv, (bmax - o) * inv).astype(np.float32)
+    nx, ny, nz = near[:, 0], near[:, 1], near[:, 2]
+    k = np.where((nx >= ny) & (nx >= nz), 0, np.where(ny >= nz, 1, 2))
+    side = np.where(d[np.arange(len(d)), k] > 0, 0, 1)
+    a = np.where(k == 0, 1, 0)
+    b = np.where(k == 2, 1, 2)
+    r = np.arange(len(d))
+    pa = (te.astype(np.float64) * d[r, a] + o[r, a]).astype(np.float32)
+    pb = (te.astype(np.float64) * d[r, b] + o[r, b]).astype(np.float32)
+    fa = np.minimum(np.maximum((pa - bmin[a]) * scale[a], 0), res - 1).astype(np.float32)
+    fb = np.minimum(np.maximum((pb - bmin[b]) * scale[b], 0), res - 1).astype(np.float32)
+    start = table[k, side, fa.astype(np.int64), fb.astype(np.int64)].astype(np.int64)
+    return np.where(te > 0, start, 0)
+
+
+def _rays_into_box(st, nodes, n, seed):
+    """Rays from outside the box toward random points inside it, half of them
+    aimed at a point on a split plane of a node near the top of the tree or
+    on a cell boundary of a face, where the descent is decided by rounding."""
+    rng = np.random.default_rng(seed)
+    bmin = np.array(st["bmin"], np.float64)
+    bmax = np.array(st["bmax"], np.float64)
+    c, ext = (bmin + bmax) / 2, bmax - bmin
+    tgt = bmin + rng.random((n, 3)) * ext
+    split = nodes[:, 0].view(np.float32)
+    inner = np.nonzero((nodes[:64, 1] & 3) != 3)[0]
+    for i in range(0, n // 2, 2):
+        nd = inner[rng.integers(len(inner))]
+        tgt[i, nodes[nd, 1] & 3] = split[nd]
+        k = rng.integers(3)
+        tgt[i + 1, k] = bmin[k] + ext[k] * rng.integers(1, 128) / 128
+    dirn = rng.normal(size=(n, 3))
+    dirn /= np.linalg.norm(dirn, axis=1, keepdims=True)
+    o = (c + dirn * 1.5 * np.linalg.norm(ext) + rng.normal(scale=0.01, size=(n, 3))).astype(np.float32)
+    d = (tgt - o).astype(np.float64)
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return o, d
+
+
+@pytest.mark.parametrize("scene", ["soup", "grid"])
+def test_entry_table_starts_on_the_root_descents_path(scene):
+    """Every ray entering the box starts its first descent at the entry
+    table's node of its face cell and reaches the leaf the root descent
+    reaches (the device's float32 rules), while skipping most of the
+    descent."""
+    if scene == "soup":
+        packed = rb.configs.SoupConfig(num_tris=1 << 14, seed=3).packed()
+        kw = dict(leaf_size=8, max_depth=24)
+    else:
+        verts, faces = po.heightfield(po.perm(2016), 96, -10.0, 10.0, 6, 2.0)
+        tri = verts[faces.reshape(-1)].reshape(-1, 3, 3)
+        packed = np.zeros((tri.shape[0], 12), np.float32)
+        packed[:, 0:3] = tri[:, 0]
+        packed[:, 4:7] = tri[:, 1] - tri[:, 0]
+        packed[:, 8:11] = tri[:, 2] - tri[:, 0]
+        kw = {}
+    sc = rb.KDScene.build_host(packed, rb.kd_params(**kw) if kw else None)
+    st = sc.stats()
+    nodes, _, _ = sc.export()
+    table = sc.export_entry()
+    sc.close()
+    assert table.shape[:2] == (3, 2) and table.shape[2] == table.shape[3] >= 64
+    assert table.max() < st["num_nodes"]
+    o, d = _rays_into_box(st, nodes, 40000, seed=11)
+    with np.errstate(divide="ignore"):
+        inv = (np.float32(1) / d).astype(np.float32)
+    bmin = np.array(st["bmin"], np.float32)
+    bmax = np.array(st["bmax"], np.float32)
+    with np.errstate(invalid="ignore", over="ignore"):
+        t1, t2 = (bmin - o) * inv, (bmax - o) * inv
+    tmin = np.max(np.minimum(t1, t2), 1)
+    tmax = np.min(np.maximum(t1, t2), 1)
+    live = (tmax >= 0) & (tmin <= tmax)
+    o, d, inv = o[live], d[live], inv[live]
+    te = np.maximum(tmin[live], 0).astype(np.float32)
+    assert len(te) > 30000 and np.all(te > 0)
+    start = _entry_start(table, st, o, d, inv, te)
+    root = _first_leaf(nodes, np.zeros(len(te), np.int64), o, d, inv, te)
+    from_table = _first_leaf(nodes, start, o, d, inv, te)
+    assert np.array_equal(root, from_table)
+    # the table's nodes are deep: most of the first descent is skipped
+    assert (start > 0).mean() > 0.9

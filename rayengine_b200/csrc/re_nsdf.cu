@@ -1329,56 +1329,89 @@ __global__ void __launch_bounds__(256) k_sdf_refine(PermTable perm, FieldDev f, 
                                                     unsigned long long* __restrict__ totals,
                                                     float4* __restrict__ out) {
   extern __shared__ uint32_t perm_smem[];
+  // Per-warp ring of set-up rays (64 entries): the warp claims 32 work
+  // indices at a time and all its lanes set those rays up together (pixel,
+  // two divisions and three normalisations for the direction, the cone
+  // tile's start), so the set-up runs with every lane active instead of on
+  // the few lanes that happen to be idle; idle lanes then take entries.
+  // Entry: {d.xyz, t} and {pixel (0xFFFFFFFF: no ray), t_lo bits, base
+  // steps, 0}.
+  __shared__ float4 ring_a[8][64];
+  __shared__ uint4 ring_b[8][64];
   load_perm(perm, perm_smem);
   Perm P = perm_view(perm_smem);
-  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   // direct mode claims pixels in 8x4 tiles (claim i = lane i & 31 of tile
   // i >> 5), so a warp's rays start close together
   const uint32_t dtiles_x = (w + 7) / 8;
   const uint32_t total = direct ? dtiles_x * ((h + 3) / 4) * 32u : counters[1];
-  bool live = false, exhausted = false, have_lo = false, restarted = false;
+  bool live = false, claimed_all = false, have_lo = false, restarted = false;
+  uint32_t head = 0, tail = 0;  // ring positions (warp-uniform)
   uint32_t pix = 0, steps = 0, base_steps = 0, mode = kMarch, tap = 0, iters = 0;
   int side = 0;
-  V3 o = {0, 0, 0}, d = {0, 0, 1}, p = {0, 0, 0};
+  V3 o = cam.campos, d = {0, 0, 1}, p = {0, 0, 0};
   float t = 0.f, t_lo = 0.f, a = 0.f, va = 0.f, b = 0.f, vb = 0.f, delta = 0.f;
   float nx = 0.f, ny = 0.f, nz = 0.f, plus = 0.f;
   uint32_t n_exact = 0, n_normal = 0;  // evaluations: march/probe/root, normal taps
   for (;;) {
     uint32_t idle = __ballot_sync(0xFFFFFFFFu, !live);
     uint32_t nidle = __popc(idle);
-    if (!exhausted && nidle >= 4u) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(&counters[2], nidle);
-      base = __shfl_sync(0xFFFFFFFFu, base, 0);
-      if (base + nidle >= total) exhausted = true;
-      if (!live) {
-        uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+    if (nidle >= 4u && (!claimed_all || head != tail)) {
+      if (tail - head < nidle && !claimed_all) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&counters[2], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base + 32u >= total) claimed_all = true;
+        const uint32_t i = base + lane;
         uint32_t dx = 0, dy = 0;
         if (direct) {
           dx = ((i >> 5) % dtiles_x) * 8 + (i & 7u);
           dy = ((i >> 5) / dtiles_x) * 4 + ((i >> 3) & 3u);
         }
+        float4 ea = make_float4(0.f, 0.f, 1.f, 0.f);
+        uint4 eb = make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
         if (i < total && (!direct || (dx < w && dy < h))) {
           uint4 e = direct ? make_uint4(dy * w + dx, 0u, 0u, 0u) : queue[i];
-          pix = e.x;
-          generate_ray(cam, w, h, pix % w, pix / w, o, d);
-          t = __uint_as_float(e.y);
-          t_lo = __uint_as_float(e.z);
+          V3 ro, rd3;
+          generate_ray(cam, w, h, e.x % w, e.x / w, ro, rd3);
+          float t0 = __uint_as_float(e.y), tl = __uint_as_float(e.z);
           if (direct && rd.tile_t) {
-            t = rd.tile_t[((pix / w) / rd.cone_tile) * rd.cone_tiles_x + (pix % w) / rd.cone_tile];
-            t_lo = t;
+            t0 = rd.tile_t[((e.x / w) / rd.cone_tile) * rd.cone_tiles_x + (e.x % w) / rd.cone_tile];
+            tl = t0;
           }
-          base_steps = e.w;
-          steps = 0;
-          mode = kMarch;
-          have_lo = false;
-          restarted = false;
-          live = true;
+          ea = make_float4(rd3.x, rd3.y, rd3.z, t0);
+          eb = make_uint4(e.x, __float_as_uint(tl), e.w, 0u);
+        }
+        ring_a[warp][(tail + lane) & 63u] = ea;
+        ring_b[warp][(tail + lane) & 63u] = eb;
+        __syncwarp();
+        tail += 32u;
+      }
+      const uint32_t avail = tail - head;
+      if (!live) {
+        const uint32_t r = __popc(idle & ((1u << lane) - 1u));
+        if (r < avail) {
+          const float4 ea = ring_a[warp][(head + r) & 63u];
+          const uint4 eb = ring_b[warp][(head + r) & 63u];
+          if (eb.x != 0xFFFFFFFFu) {
+            pix = eb.x;
+            d = v3(ea.x, ea.y, ea.z);
+            t = ea.w;
+            t_lo = __uint_as_float(eb.y);
+            base_steps = eb.z;
+            steps = 0;
+            mode = kMarch;
+            have_lo = false;
+            restarted = false;
+            live = true;
+          }
         }
       }
+      head += min(nidle, avail);
+      __syncwarp();
     }
     if (__ballot_sync(0xFFFFFFFFu, live) == 0u) {
-      if (exhausted) break;
+      if (claimed_all && head == tail) break;
       continue;
     }
     if (!live) continue;

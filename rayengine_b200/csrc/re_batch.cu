@@ -93,6 +93,10 @@ struct __align__(16) SceneDev {
   CamDev cam;
   uint32_t w, h, kind, pix_off;
   float albedo;
+  // the mesh's entry table (re_kd.cuh entry_node) for its camera rays
+  const uint32_t* entry;
+  float entry_scale[3];
+  uint32_t entry_res;
 };
 // Shared memory holds SceneDev[num_scenes], then the noise tables (multiples
 // of 512 bytes), then the staged nodes (uint2): the nodes stay 8-byte
@@ -150,6 +154,17 @@ __device__ __forceinline__ KdDev kd_of(const SceneDev& s) {
   kd.max_visits = s.max_visits;
   kd.stage = s.stage;
   kd.trunc = nullptr;
+  return kd;
+}
+
+// kd_of with the mesh's entry table, for camera rays (which enter the scene
+// box from outside); the counting kernel descends from the root, as the
+// oracle does.
+__device__ __forceinline__ KdDev kd_entry_of(const SceneDev& s) {
+  KdDev kd = kd_of(s);
+  kd.entry = s.entry;
+  kd.entry_res = s.entry_res;
+  kd.entry_scale = v3(s.entry_scale[0], s.entry_scale[1], s.entry_scale[2]);
   return kd;
 }
 
@@ -399,7 +414,7 @@ __global__ void __launch_bounds__(RE_BATCH_MAX_THREADS, RE_BATCH_MIN_BLOCKS) k_b
           V3 o, d;
           generate_ray(S.cam, S.w, S.h, lp % S.w, lp / S.w, o, d);
           if (kind == kMesh) {
-            trav_init(tr, kd_of(S), o, d, K_INF, 0u);
+            trav_init(tr, COUNT ? kd_of(S) : kd_entry_of(S), o, d, K_INF, 0u);
           } else {
             tr.o = o;
             tr.d = d;
@@ -821,6 +836,12 @@ RE_API re_status re_batch_create(const re_batch_scene* scenes, uint32_t n, const
         d.bmax[k] = m->host.bmax[k];
       }
       d.max_visits = m->max_visits;
+      d.entry = m->d_entry;
+      d.entry_res = m->d_entry ? re::kEntryRes : 0u;
+      for (int k = 0; k < 3; ++k) {
+        const float ext = m->host.bmax[k] - m->host.bmin[k];
+        d.entry_scale[k] = ext > 0.f ? (float)re::kEntryRes / ext : 0.f;
+      }
       b->cap[0] += (uint64_t)s.width * s.height;
     } else if (s.kind == RE_BATCH_TERRAIN) {
       const re_sdf_params& f = s.field;

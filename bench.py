@@ -230,7 +230,7 @@ def hbm_roofline(wl, phase_ms, peaks):
     return out
 
 
-def survey_bytes(rays, inner, leaf, tests, stored=0):
+def traversal_bytes(rays, inner, leaf, tests, stored=0):
     """Algorithmic bytes of a traversal launch: 16 (hit out) per ray, 16 per
     inner-node visit, 48 per leaf visit (24-byte box + 24-byte ropes), 4 per
     triangle reference read and 48 per triangle test, plus 32 per stored ray
@@ -376,12 +376,12 @@ class HeightfieldAO:
         ]
 
     def alg_bytes(self):
-        """Algorithmic bytes per launch (survey_bytes): the primary pass also
+        """Algorithmic bytes per launch (traversal_bytes): the primary pass also
         stores the five secondary rays of every hit, the secondary pass reads
         them."""
         p, s = self.counts["primary"], self.counts["secondary"]
-        return {"ao_primary": survey_bytes(p["rays"], p["inner"], p["leaf"], p["tests"], s["rays"]),
-                "ao_secondary": survey_bytes(s["rays"], s["inner"], s["leaf"], s["tests"], s["rays"])}
+        return {"ao_primary": traversal_bytes(p["rays"], p["inner"], p["leaf"], p["tests"], s["rays"]),
+                "ao_secondary": traversal_bytes(s["rays"], s["inner"], s["leaf"], s["tests"], s["rays"])}
 
     def layout_bytes(self):
         p, s = self.counts["primary"], self.counts["secondary"]
@@ -520,7 +520,7 @@ class SoupPrimary:
 
     def alg_bytes(self):
         t = self.tot
-        return {"primary": survey_bytes(t["rays"], t["inner"], t["leaf"], t["tests"])}
+        return {"primary": traversal_bytes(t["rays"], t["inner"], t["leaf"], t["tests"])}
 
     def layout_bytes(self):
         t = self.tot
@@ -974,7 +974,7 @@ class BatchWavefront:
     def alg_bytes(self):
         w = self.work
         cont = int(self.rays[1:].sum())
-        return {"batch": survey_bytes(int(self.rays.sum()), w["inner"], w["leaf"], w["tests"], cont)}
+        return {"batch": traversal_bytes(int(self.rays.sum()), w["inner"], w["leaf"], w["tests"], cont)}
 
     def layout_bytes(self):
         w = self.work

@@ -840,7 +840,7 @@ class NeuralTerrainSDF:
                 "trace_params": {"lipschitz": round(self.tp.lipschitz, 4),
                                  "lipschitz_quantile": n.lipschitz_quantile,
                                  "safety": n.cone_safety, "switch_dist": n.switch_dist,
-                                 "min_step": n.min_step, "max_network_steps": n.max_network_steps,
+                                 "min_step": n.min_step, "cone_max_passes": n.cone_max_passes,
                                  "root_steps": n.root_steps, "cone_tile": n.cone_tile,
                                  "cone_lanes": n.cone_lanes, "relax": n.relax,
                                  "root_tol": n.root_tol, "normal_taps": n.normal_taps},

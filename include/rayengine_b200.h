@@ -411,7 +411,9 @@ typedef struct re_nsdf_trace_params {
   float safety;         /* step = safety * distance / lipschitz            */
   float switch_dist;    /* hand over to the exact field below this         */
   float min_step;       /* smallest network step                           */
-  uint32_t max_network_steps; /* 0 = 256                                   */
+  uint32_t max_network_steps; /* 0 = 256; with cones: passes per cone      */
+                              /* (a tile that reaches it starts its exact  */
+                              /* phase where its cone is)                  */
   uint32_t max_exact_steps;   /* exact evaluations per ray; 0 = max_steps  */
   uint32_t root_steps;  /* regula-falsi steps on a bracketed crossing; 0=4 */
   float relax;          /* exact steps may grow along the secant up to     */

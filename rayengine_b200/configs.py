@@ -187,7 +187,13 @@ class NeuralTerrainConfig:
     cone_safety: float = 1.5
     switch_dist: float = 0.3
     min_step: float = 0.05
-    max_network_steps: int = 64
+    max_network_steps: int = 64  # per-ray march steps
+    # passes of a cone (16 steps guessed per pass): the cone phase lasts as
+    # long as its longest chains of passes; capped at 12 the far tiles hand
+    # over earlier (measured on B200: 2.10 -> 2.01 ms per frame, cone phase
+    # 0.27 -> 0.20 ms, exact evaluations 14.41 -> 14.59 per ray, the same
+    # median error and p95; 8 passes: 2.05 ms)
+    cone_max_passes: int = 12
     root_steps: int = 4
     cone_tile: int = 16
     cone_lanes: int = 16
@@ -234,7 +240,7 @@ class NeuralTerrainConfig:
     def trace_params(self, lipschitz):
         """The cone tracer's settings (the default method)."""
         return api.nsdf_trace_params(lipschitz, self.cone_safety, self.switch_dist, self.min_step,
-                                     self.max_network_steps, 0, self.root_steps, self.relax,
+                                     self.cone_max_passes, 0, self.root_steps, self.relax,
                                      cone_tile=self.cone_tile, cone_lanes=self.cone_lanes,
                                      normal_taps=self.normal_taps, root_tol=self.root_tol)
 
